@@ -1,0 +1,81 @@
+/*
+ * op2b.h -- extensions of the B200 OP2 library beyond the reference C API.
+ *
+ * Nothing here is needed by the reference apps; op_lib.h alone is the
+ * drop-in.  These calls choose how the loops run, expose the device stream
+ * and timers to benchmark drivers, and return errors instead of exiting.
+ * All have C linkage.
+ */
+#ifndef OP2B_H
+#define OP2B_H
+
+#include "op_lib_core.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* How loops with OP_INC through a map are executed.
+ *  GATHER   : owner-computes.  Each target element sums its contributions
+ *             in ascending (element, argument) order, which is exactly the
+ *             order of the reference's sequential op_seq.h back-end, so the
+ *             results are bit-identical to it.  No colouring, no atomics.
+ *  COLOURED : the two-level colouring of op_plan (blocks staged in shared
+ *             memory, increments applied in thread-colour order, blocks
+ *             launched colour by colour).  Deterministic; summation order
+ *             differs from op_seq.h, as in the reference's CUDA/OpenMP code.
+ *  AUTO     : per loop, the faster of the two as measured by the tuner. */
+enum { OP2B_STRATEGY_AUTO = 0, OP2B_STRATEGY_GATHER = 1, OP2B_STRATEGY_COLOURED = 2 };
+
+/* How global OP_INC reductions (op_arg_gbl ... OP_INC) are summed.
+ *  TREE : fixed-shape tree (per-thread, warp shuffle, per-block, one final
+ *         block); deterministic run to run.
+ *  SEQ  : element order, one addition at a time, exactly as op_seq.h does;
+ *         bit-identical to the reference, at the cost of a serial pass. */
+enum { OP2B_REDUCE_TREE = 0, OP2B_REDUCE_SEQ = 1 };
+
+/* Errors: EXIT (default, like the reference: print and exit) or RETURN
+ * (print, remember the message, return NULL / do nothing). */
+enum { OP2B_ERRORS_EXIT = 0, OP2B_ERRORS_RETURN = 1 };
+
+int         op2b_set_strategy(int strategy);   /* returns the previous value */
+int         op2b_set_reduction(int mode);      /* returns the previous value */
+int         op2b_set_error_mode(int mode);     /* returns the previous value */
+const char *op2b_last_error(void);             /* "" when none               */
+void        op2b_clear_error(void);
+
+/* The CUDA stream all loops are issued on (a cudaStream_t).  Setting it lets
+ * a caller capture the loops into a CUDA graph or order them with its own
+ * work. */
+void *op2b_get_stream(void);
+void  op2b_set_stream(void *stream);
+/* Wait for all issued loops; returns 0 or a CUDA error code. */
+int   op2b_sync(void);
+
+/* Global reductions normally complete inside the loop call (the reference
+ * semantics: the host variable holds the result on return).  With deferred
+ * mode on, a loop with OP_INC/OP_MIN/OP_MAX global arguments only issues
+ * device work; the results reach the host variables at the next
+ * op2b_sync(), op_fetch_data() or op2b_set_gbl_deferred(0).  Deferred mode is
+ * what makes an outer iteration capturable as one CUDA graph. */
+int   op2b_set_gbl_deferred(int on);
+
+/* Per-loop device time in seconds and call count, by loop name (CUDA events
+ * around each loop; summed lazily).  Returns -1 if the name is unknown. */
+double op2b_loop_time(char const *name, int *count);
+/* Turn per-loop event timing on (default) or off; returns the old value. */
+int    op2b_set_timing(int on);
+
+/* Plan validation on the device: the reference's op_plan_check plus the
+ * colouring checks it lacks.  Returns the number of violations found. */
+long op2b_plan_validate(char const *name, op_set set, int part_size, int nargs, op_arg *args,
+                        int ninds, int *inds);
+
+/* Library build string (arch, flags). */
+char const *op2b_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,577 @@
+// airfoil.cu -- the five parallel loops of the airfoil app, as hand-written
+// sm_100a kernels (FP32 and FP64), replacing the generated
+// airfoil/{save_soln,adt_calc,res_calc,bres_calc,update}_kernel.cu.
+//
+// The user-kernel arithmetic (airfoil/*.h) is restated term for term in the
+// reference's evaluation order; the library is compiled with -fmad=false and
+// IEEE division / square root, so every per-element value is bit-identical
+// to the reference's x86 build.
+//
+// Indirect loops with OP_INC (res_calc, bres_calc) have two executions:
+//  GATHER   one thread per incremented cell walks that cell's contributions
+//           in ascending (edge, argument) order -- op_seq.h's order -- and
+//           writes the cell once: bit-identical to the sequential reference,
+//           no colouring, no atomics, one launch.
+//  COLOURED the reference's two-level scheme on the device plan: a CTA per
+//           block stages x, q, adt of its distinct targets in shared memory,
+//           applies increments in thread-colour order, and adds its block
+//           increment to res once; block colours are separate launches.
+
+#include <string.h>
+
+#include "loops.h"
+#include "reduce.cuh"
+
+namespace op2b {
+
+// ---------------------------------------------------------- vector I/O ----
+__device__ __forceinline__ void ld2(const float *p, float v[2]) {
+  float2 t = __ldg(reinterpret_cast<const float2 *>(p));
+  v[0] = t.x; v[1] = t.y;
+}
+__device__ __forceinline__ void ld2(const double *p, double v[2]) {
+  double2 t = __ldg(reinterpret_cast<const double2 *>(p));
+  v[0] = t.x; v[1] = t.y;
+}
+__device__ __forceinline__ void ld4(const float *p, float v[4]) {
+  float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+  v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void ld4(const double *p, double v[4]) {
+  double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+  double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+// plain (coherent) loads for data the kernel also writes
+__device__ __forceinline__ void ldw4(const float *p, float v[4]) {
+  float4 t = *reinterpret_cast<const float4 *>(p);
+  v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void ldw4(const double *p, double v[4]) {
+  double2 a = reinterpret_cast<const double2 *>(p)[0], b = reinterpret_cast<const double2 *>(p)[1];
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void st4(float *p, const float v[4]) {
+  *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double *p, const double v[4]) {
+  reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+  reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+}
+
+__device__ __forceinline__ int at(const IdxMap &m, int e) {
+  return m.map ? __ldg(m.map + m.idx + (size_t)e * m.dim) : e;
+}
+
+template <class T>
+struct AirConsts {
+  T gam, gm1, cfl, eps, qinf[4];
+};
+
+// --------------------------------------------------------- user kernels ---
+// airfoil/adt_calc.h:1-26
+template <class T>
+__device__ __forceinline__ T adt_calc(const T x1[2], const T x2[2], const T x3[2], const T x4[2],
+                                      const T q[4], const AirConsts<T> &K) {
+  T dx, dy, ri, u, v, c, adt;
+  ri = T(1.0f) / q[0];
+  u = ri * q[1];
+  v = ri * q[2];
+  c = sqrt(K.gam * K.gm1 * (ri * q[3] - T(0.5f) * (u * u + v * v)));
+  dx = x2[0] - x1[0];
+  dy = x2[1] - x1[1];
+  adt = fabs(u * dy - v * dx) + c * sqrt(dx * dx + dy * dy);
+  dx = x3[0] - x2[0];
+  dy = x3[1] - x2[1];
+  adt += fabs(u * dy - v * dx) + c * sqrt(dx * dx + dy * dy);
+  dx = x4[0] - x3[0];
+  dy = x4[1] - x3[1];
+  adt += fabs(u * dy - v * dx) + c * sqrt(dx * dx + dy * dy);
+  dx = x1[0] - x4[0];
+  dy = x1[1] - x4[1];
+  adt += fabs(u * dy - v * dx) + c * sqrt(dx * dx + dy * dy);
+  return adt / K.cfl;
+}
+
+// airfoil/res_calc.h:1-30; f is the flux added to res1 and taken from res2
+template <class T>
+__device__ __forceinline__ void res_flux(const T x1[2], const T x2[2], const T q1[4],
+                                         const T q2[4], T adt1, T adt2, T gm1, T eps, T f[4]) {
+  T dx = x1[0] - x2[0];
+  T dy = x1[1] - x2[1];
+  T ri = T(1.0f) / q1[0];
+  T p1 = gm1 * (q1[3] - T(0.5f) * ri * (q1[1] * q1[1] + q1[2] * q1[2]));
+  T vol1 = ri * (q1[1] * dy - q1[2] * dx);
+  ri = T(1.0f) / q2[0];
+  T p2 = gm1 * (q2[3] - T(0.5f) * ri * (q2[1] * q2[1] + q2[2] * q2[2]));
+  T vol2 = ri * (q2[1] * dy - q2[2] * dx);
+  T mu = T(0.5f) * (adt1 + adt2) * eps;
+  f[0] = T(0.5f) * (vol1 * q1[0] + vol2 * q2[0]) + mu * (q1[0] - q2[0]);
+  f[1] = T(0.5f) * (vol1 * q1[1] + p1 * dy + vol2 * q2[1] + p2 * dy) + mu * (q1[1] - q2[1]);
+  f[2] = T(0.5f) * (vol1 * q1[2] - p1 * dx + vol2 * q2[2] - p2 * dx) + mu * (q1[2] - q2[2]);
+  f[3] = T(0.5f) * (vol1 * (q1[3] + p1) + vol2 * (q2[3] + p2)) + mu * (q1[3] - q2[3]);
+}
+
+// airfoil/bres_calc.h:1-33, applied to the running value r of res1
+template <class T>
+__device__ __forceinline__ void bres_apply(const T x1[2], const T x2[2], const T q1[4], T adt1,
+                                           int bound, const AirConsts<T> &K, T r[4]) {
+  T dx = x1[0] - x2[0];
+  T dy = x1[1] - x2[1];
+  T ri = T(1.0f) / q1[0];
+  T p1 = K.gm1 * (q1[3] - T(0.5f) * ri * (q1[1] * q1[1] + q1[2] * q1[2]));
+  if (bound == 1) {
+    r[1] += +p1 * dy;
+    r[2] += -p1 * dx;
+  } else {
+    const T *qinf = K.qinf;
+    T vol1 = ri * (q1[1] * dy - q1[2] * dx);
+    ri = T(1.0f) / qinf[0];
+    T p2 = K.gm1 * (qinf[3] - T(0.5f) * ri * (qinf[1] * qinf[1] + qinf[2] * qinf[2]));
+    T vol2 = ri * (qinf[1] * dy - qinf[2] * dx);
+    T mu = adt1 * K.eps;
+    T f;
+    f = T(0.5f) * (vol1 * q1[0] + vol2 * qinf[0]) + mu * (q1[0] - qinf[0]);
+    r[0] += f;
+    f = T(0.5f) * (vol1 * q1[1] + p1 * dy + vol2 * qinf[1] + p2 * dy) + mu * (q1[1] - qinf[1]);
+    r[1] += f;
+    f = T(0.5f) * (vol1 * q1[2] - p1 * dx + vol2 * qinf[2] - p2 * dx) + mu * (q1[2] - qinf[2]);
+    r[2] += f;
+    f = T(0.5f) * (vol1 * (q1[3] + p1) + vol2 * (qinf[3] + p2)) + mu * (q1[3] - qinf[3]);
+    r[3] += f;
+  }
+}
+
+// ------------------------------------------------------------- kernels ----
+
+// save_soln: qold = q, one element per thread, 16-byte vectors
+template <class T>
+__global__ void k_save_soln(int n, const T *__restrict__ q, T *__restrict__ qold) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    T v[4];
+    ld4(q + 4 * (size_t)c, v);
+    st4(qold + 4 * (size_t)c, v);
+  }
+}
+
+// adt_calc: direct over cells, x gathered through pcell
+template <class T>
+__global__ void k_adt_calc(int n, IdxMap m0, IdxMap m1, IdxMap m2, IdxMap m3, IdxMap mq,
+                           const T *__restrict__ x0, const T *__restrict__ x1,
+                           const T *__restrict__ x2, const T *__restrict__ x3,
+                           const T *__restrict__ q, T *__restrict__ adt, AirConsts<T> K) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    T a[2], b[2], d[2], e[2], qq[4];
+    ld2(x0 + 2 * (size_t)at(m0, c), a);
+    ld2(x1 + 2 * (size_t)at(m1, c), b);
+    ld2(x2 + 2 * (size_t)at(m2, c), d);
+    ld2(x3 + 2 * (size_t)at(m3, c), e);
+    ld4(q + 4 * (size_t)at(mq, c), qq);
+    adt[c] = adt_calc(a, b, d, e, qq, K);
+  }
+}
+
+// res_calc, GATHER: one thread per incremented cell
+template <class T>
+__global__ void k_res_calc_gather(int nrows, const int *__restrict__ active,
+                                  const int *__restrict__ row, const int *__restrict__ keys,
+                                  IdxMap mx1, IdxMap mx2, IdxMap mq1, IdxMap mq2, IdxMap ma1,
+                                  IdxMap ma2, const T *__restrict__ xa, const T *__restrict__ xb,
+                                  const T *__restrict__ qa, const T *__restrict__ qb,
+                                  const T *__restrict__ adta, const T *__restrict__ adtb,
+                                  T *__restrict__ res, T gm1, T eps) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nrows) return;
+  int c = active ? active[t] : t;
+  T r[4];
+  ldw4(res + 4 * (size_t)c, r);
+  int k1 = row[t + 1];
+  for (int k = row[t]; k < k1; k++) {
+    int key = __ldg(keys + k);
+    int e = key >> 1;
+    T p[2], s[2], q1[4], q2[4], f[4];
+    ld2(xa + 2 * (size_t)at(mx1, e), p);
+    ld2(xb + 2 * (size_t)at(mx2, e), s);
+    ld4(qa + 4 * (size_t)at(mq1, e), q1);
+    ld4(qb + 4 * (size_t)at(mq2, e), q2);
+    T a1 = __ldg(adta + at(ma1, e)), a2 = __ldg(adtb + at(ma2, e));
+    res_flux(p, s, q1, q2, a1, a2, gm1, eps, f);
+    if ((key & 1) == 0) {
+      r[0] += f[0]; r[1] += f[1]; r[2] += f[2]; r[3] += f[3];
+    } else {
+      r[0] -= f[0]; r[1] -= f[1]; r[2] -= f[2]; r[3] -= f[3];
+    }
+  }
+  st4(res + 4 * (size_t)c, r);
+}
+
+// bres_calc, GATHER: one thread per cell that has boundary edges
+template <class T>
+__global__ void k_bres_calc_gather(int nrows, const int *__restrict__ active,
+                                   const int *__restrict__ row, const int *__restrict__ keys,
+                                   IdxMap mx1, IdxMap mx2, IdxMap mq, IdxMap ma, IdxMap mb,
+                                   const T *__restrict__ xa, const T *__restrict__ xb,
+                                   const T *__restrict__ q, const T *__restrict__ adt,
+                                   const int *__restrict__ bound, T *__restrict__ res,
+                                   AirConsts<T> K) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nrows) return;
+  int c = active ? active[t] : t;
+  T r[4];
+  ldw4(res + 4 * (size_t)c, r);
+  int k1 = row[t + 1];
+  for (int k = row[t]; k < k1; k++) {
+    int e = __ldg(keys + k);
+    T p[2], s[2], q1[4];
+    ld2(xa + 2 * (size_t)at(mx1, e), p);
+    ld2(xb + 2 * (size_t)at(mx2, e), s);
+    ld4(q + 4 * (size_t)at(mq, e), q1);
+    T a1 = __ldg(adt + at(ma, e));
+    bres_apply(p, s, q1, a1, __ldg(bound + at(mb, e)), K, r);
+  }
+  st4(res + 4 * (size_t)c, r);
+}
+
+// The plan arrays one coloured launch needs
+struct PlanView {
+  const int *blkmap, *offset, *nelems, *nthrcol, *thrcol, *ind_offs, *ind_sizes;
+  const int *ind_maps[4];
+  const short *loc_maps[8];
+  int ninds;
+};
+
+// res_calc, COLOURED (inds {0,0,1,1,2,2,3,3}: x, q, adt read; res incremented)
+template <class T>
+__global__ void k_res_calc_coloured(PlanView P, int block_offset, const T *__restrict__ x,
+                                    const T *__restrict__ q, const T *__restrict__ adt,
+                                    T *__restrict__ res, T gm1, T eps) {
+  extern __shared__ __align__(16) char smem[];
+  const int b = P.blkmap[blockIdx.x + block_offset];
+  const int nelem = P.nelems[b], off = P.offset[b], ncol = P.nthrcol[b];
+  int sz[4], io[4];
+  for (int m = 0; m < 4; m++) {
+    sz[m] = P.ind_sizes[m + b * 4];
+    io[m] = P.ind_offs[m + b * 4];
+  }
+  T *xs = (T *)smem;
+  T *qs = (T *)(smem + ROUND_UP(sz[0] * 2 * (int)sizeof(T)));
+  T *as = (T *)((char *)qs + ROUND_UP(sz[1] * 4 * (int)sizeof(T)));
+  T *rs = (T *)((char *)as + ROUND_UP(sz[2] * (int)sizeof(T)));
+  for (int u = threadIdx.x; u < sz[0]; u += blockDim.x) {
+    T v[2];
+    ld2(x + 2 * (size_t)P.ind_maps[0][io[0] + u], v);
+    xs[2 * u] = v[0]; xs[2 * u + 1] = v[1];
+  }
+  for (int u = threadIdx.x; u < sz[1]; u += blockDim.x) {
+    T v[4];
+    ld4(q + 4 * (size_t)P.ind_maps[1][io[1] + u], v);
+    st4(qs + 4 * u, v);
+  }
+  for (int u = threadIdx.x; u < sz[2]; u += blockDim.x) as[u] = __ldg(adt + P.ind_maps[2][io[2] + u]);
+  for (int u = threadIdx.x; u < sz[3] * 4; u += blockDim.x) rs[u] = T(0);
+  __syncthreads();
+  const int nelems2 = blockDim.x * (1 + (nelem - 1) / blockDim.x);
+  for (int n = threadIdx.x; n < nelems2; n += blockDim.x) {
+    int col2 = -1;
+    T l6[4], l7[4];
+    int m6 = 0, m7 = 0;
+    if (n < nelem) {
+      const int e = n + off;
+      T f[4];
+      res_flux(xs + 2 * P.loc_maps[0][e], xs + 2 * P.loc_maps[1][e], qs + 4 * P.loc_maps[2][e],
+               qs + 4 * P.loc_maps[3][e], as[P.loc_maps[4][e]], as[P.loc_maps[5][e]], gm1, eps, f);
+      for (int d = 0; d < 4; d++) {
+        l6[d] = T(0) + f[d];
+        l7[d] = T(0) - f[d];
+      }
+      m6 = P.loc_maps[6][e];
+      m7 = P.loc_maps[7][e];
+      col2 = P.thrcol[e];
+    }
+    for (int col = 0; col < ncol; col++) {
+      if (col2 == col) {
+        for (int d = 0; d < 4; d++) rs[d + m6 * 4] += l6[d];
+        for (int d = 0; d < 4; d++) rs[d + m7 * 4] += l7[d];
+      }
+      __syncthreads();
+    }
+  }
+  for (int u = threadIdx.x; u < sz[3]; u += blockDim.x) {
+    T *dst = res + 4 * (size_t)P.ind_maps[3][io[3] + u];
+    T v[4];
+    ldw4(dst, v);
+    for (int d = 0; d < 4; d++) v[d] += rs[4 * u + d];
+    st4(dst, v);
+  }
+}
+
+// bres_calc, COLOURED (inds {0,0,1,2,3,-1}; bound is direct)
+template <class T>
+__global__ void k_bres_calc_coloured(PlanView P, int block_offset, const T *__restrict__ x,
+                                     const T *__restrict__ q, const T *__restrict__ adt,
+                                     const int *__restrict__ bound, T *__restrict__ res,
+                                     AirConsts<T> K) {
+  extern __shared__ __align__(16) char smem[];
+  const int b = P.blkmap[blockIdx.x + block_offset];
+  const int nelem = P.nelems[b], off = P.offset[b], ncol = P.nthrcol[b];
+  int sz[4], io[4];
+  for (int m = 0; m < 4; m++) {
+    sz[m] = P.ind_sizes[m + b * 4];
+    io[m] = P.ind_offs[m + b * 4];
+  }
+  T *xs = (T *)smem;
+  T *qs = (T *)(smem + ROUND_UP(sz[0] * 2 * (int)sizeof(T)));
+  T *as = (T *)((char *)qs + ROUND_UP(sz[1] * 4 * (int)sizeof(T)));
+  T *rs = (T *)((char *)as + ROUND_UP(sz[2] * (int)sizeof(T)));
+  for (int u = threadIdx.x; u < sz[0]; u += blockDim.x) {
+    T v[2];
+    ld2(x + 2 * (size_t)P.ind_maps[0][io[0] + u], v);
+    xs[2 * u] = v[0]; xs[2 * u + 1] = v[1];
+  }
+  for (int u = threadIdx.x; u < sz[1]; u += blockDim.x) {
+    T v[4];
+    ld4(q + 4 * (size_t)P.ind_maps[1][io[1] + u], v);
+    st4(qs + 4 * u, v);
+  }
+  for (int u = threadIdx.x; u < sz[2]; u += blockDim.x) as[u] = __ldg(adt + P.ind_maps[2][io[2] + u]);
+  for (int u = threadIdx.x; u < sz[3] * 4; u += blockDim.x) rs[u] = T(0);
+  __syncthreads();
+  const int nelems2 = blockDim.x * (1 + (nelem - 1) / blockDim.x);
+  for (int n = threadIdx.x; n < nelems2; n += blockDim.x) {
+    int col2 = -1, m4 = 0;
+    T l4[4] = {T(0), T(0), T(0), T(0)};
+    if (n < nelem) {
+      const int e = n + off;
+      bres_apply(xs + 2 * P.loc_maps[0][e], xs + 2 * P.loc_maps[1][e], qs + 4 * P.loc_maps[2][e],
+                 as[P.loc_maps[3][e]], __ldg(bound + e), K, l4);
+      m4 = P.loc_maps[4][e];
+      col2 = P.thrcol[e];
+    }
+    for (int col = 0; col < ncol; col++) {
+      if (col2 == col)
+        for (int d = 0; d < 4; d++) rs[d + m4 * 4] += l4[d];
+      __syncthreads();
+    }
+  }
+  for (int u = threadIdx.x; u < sz[3]; u += blockDim.x) {
+    T *dst = res + 4 * (size_t)P.ind_maps[3][io[3] + u];
+    T v[4];
+    ldw4(dst, v);
+    for (int d = 0; d < 4; d++) v[d] += rs[4 * u + d];
+    st4(dst, v);
+  }
+}
+
+// update: q = qold - res/adt, res = 0, rms += del^2 (airfoil/update.h:1-12).
+// SEQ != nullptr: store each del^2 in element order for the serial fold.
+template <class T>
+__global__ void k_update(int n, const T *__restrict__ qold, T *__restrict__ q,
+                         T *__restrict__ res, const T *__restrict__ adt, T *seq,
+                         RedSlot<T> slot, unsigned *ticket) {
+  T rms = T(0);
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    T qo[4], r[4], qn[4];
+    ld4(qold + 4 * (size_t)c, qo);
+    ldw4(res + 4 * (size_t)c, r);
+    T adti = T(1.0f) / __ldg(adt + c);
+    T sq[4];
+    for (int d = 0; d < 4; d++) {
+      T del = adti * r[d];
+      qn[d] = qo[d] - del;
+      sq[d] = del * del;
+      rms += sq[d];
+    }
+    st4(q + 4 * (size_t)c, qn);
+    const T z[4] = {T(0), T(0), T(0), T(0)};
+    st4(res + 4 * (size_t)c, z);
+    if (seq) st4(seq + 4 * (size_t)c, sq);
+  }
+  if (seq) return;
+  const T v[1] = {rms}, id[1] = {T(0)};
+  RedSlot<T> sl[1] = {slot};
+  grid_finish<T, OpSum, OpSum, 1>(v, id, OpSum(), OpSum(), sl, ticket);
+}
+
+// ------------------------------------------------------------ host side ---
+
+template <class T>
+static AirConsts<T> air_consts() {
+  AirConsts<T> K;
+  memset(&K, 0, sizeof K);
+  T v[4];
+  auto get = [&](const char *nm, int dim) -> bool {
+    int got = sizeof(T) == 4 ? const_get_f32(nm, (float *)v, dim) : const_get_f64(nm, (double *)v, dim);
+    if (got < dim) {
+      fail(-1, "op2b error -- constant \"%s\" (dim %d) not declared with op_decl_const2\n", nm, dim);
+      return false;
+    }
+    return true;
+  };
+  if (get("gam", 1)) K.gam = v[0];
+  if (get("gm1", 1)) K.gm1 = v[0];
+  if (get("cfl", 1)) K.cfl = v[0];
+  if (get("eps", 1)) K.eps = v[0];
+  if (get("qinf", 4))
+    for (int i = 0; i < 4; i++) K.qinf[i] = v[i];
+  return K;
+}
+
+static bool is_double(const op_arg &a) { return a.dat && strcmp(a.dat->type, "double") == 0; }
+
+static int grid_for(long long n, int threads) {
+  long long g = (n + threads - 1) / threads;
+  long long cap = (long long)rt().num_sms * 16;
+  if (g < 1) g = 1;
+  return (int)(g < cap ? g : cap);
+}
+
+static PlanView plan_view(const DevPlan &p) {
+  PlanView v;
+  memset(&v, 0, sizeof v);
+  v.blkmap = p.d_blkmap; v.offset = p.d_offset; v.nelems = p.d_nelems; v.nthrcol = p.d_nthrcol;
+  v.thrcol = p.d_thrcol; v.ind_offs = p.d_ind_offs; v.ind_sizes = p.d_ind_sizes;
+  v.ninds = p.ninds;
+  for (int m = 0; m < p.ninds && m < 4; m++) v.ind_maps[m] = p.d_ind_maps[m];
+  for (int a = 0; a < p.nargs && a < 8; a++) v.loc_maps[a] = p.d_loc_maps[a];
+  return v;
+}
+
+template <class T>
+static void save_soln_t(char const *name, op_set set, const op_arg *args) {
+  LoopScope ls(name, compulsory_bytes(set, 2, args), 0);
+  int n = set->size;
+  k_save_soln<T><<<grid_for(n, 256), 256, 0, rt().stream>>>(n, (const T *)args[0].dat->data_d,
+                                                             (T *)args[1].dat->data_d);
+}
+void run_save_soln(char const *name, op_set set, const op_arg *args) {
+  if (is_double(args[0])) save_soln_t<double>(name, set, args);
+  else save_soln_t<float>(name, set, args);
+}
+
+template <class T>
+static void adt_calc_t(char const *name, op_set set, const op_arg *args) {
+  AirConsts<T> K = air_consts<T>();
+  if (error_pending()) return;
+  LoopScope ls(name, compulsory_bytes(set, 6, args), 0);
+  int n = set->size;
+  k_adt_calc<T><<<grid_for(n, 256), 256, 0, rt().stream>>>(
+      n, idx_map(args[0]), idx_map(args[1]), idx_map(args[2]), idx_map(args[3]), idx_map(args[4]),
+      (const T *)args[0].dat->data_d, (const T *)args[1].dat->data_d,
+      (const T *)args[2].dat->data_d, (const T *)args[3].dat->data_d,
+      (const T *)args[4].dat->data_d, (T *)args[5].dat->data_d, K);
+}
+void run_adt_calc(char const *name, op_set set, const op_arg *args) {
+  if (is_double(args[0])) adt_calc_t<double>(name, set, args);
+  else adt_calc_t<float>(name, set, args);
+}
+
+static const int kResInds[8] = {0, 0, 1, 1, 2, 2, 3, 3};
+static const int kBresInds[6] = {0, 0, 1, 2, 3, -1};
+
+template <class T>
+static void res_calc_t(char const *name, op_set set, const op_arg *args) {
+  AirConsts<T> K = air_consts<T>();
+  if (error_pending()) return;
+  cudaStream_t s = rt().stream;
+  if (effective_strategy(name) == OP2B_STRATEGY_COLOURED) {
+    int part = OP_part_size;
+    DevPlan *p = get_plan(name, set, part, 8, args, 4, kResInds);
+    if (!p) return;
+    LoopScope ls(name, p->transfer, p->transfer2);
+    PlanView v = plan_view(*p);
+    int nthread = OP_block_size > 0 ? OP_block_size : 512;
+    if (p->nshared > 48 * 1024)
+      OP2B_CUDA(cudaFuncSetAttribute(k_res_calc_coloured<T>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, p->nshared));
+    for (int c = 0, off = 0; c < p->ncolors; off += p->ncolblk[c], c++)
+      if (p->ncolblk[c] > 0)
+        k_res_calc_coloured<T><<<p->ncolblk[c], nthread, p->nshared, s>>>(
+            v, off, (const T *)args[0].dat->data_d, (const T *)args[2].dat->data_d,
+            (const T *)args[4].dat->data_d, (T *)args[6].dat->data_d, K.gm1, K.eps);
+    return;
+  }
+  GatherPlan *g = get_gather_plan(set, args, {6, 7});
+  if (!g) return;
+  LoopScope ls(name, compulsory_bytes(set, 8, args), 0);
+  if (g->nactive == 0) return;
+  k_res_calc_gather<T><<<(g->nactive + 255) / 256, 256, 0, s>>>(
+      g->nactive, g->d_active, g->d_row, g->d_keys, idx_map(args[0]), idx_map(args[1]),
+      idx_map(args[2]), idx_map(args[3]), idx_map(args[4]), idx_map(args[5]),
+      (const T *)args[0].dat->data_d, (const T *)args[1].dat->data_d,
+      (const T *)args[2].dat->data_d, (const T *)args[3].dat->data_d,
+      (const T *)args[4].dat->data_d, (const T *)args[5].dat->data_d, (T *)args[6].dat->data_d,
+      K.gm1, K.eps);
+}
+void run_res_calc(char const *name, op_set set, const op_arg *args) {
+  if (is_double(args[0])) res_calc_t<double>(name, set, args);
+  else res_calc_t<float>(name, set, args);
+}
+
+template <class T>
+static void bres_calc_t(char const *name, op_set set, const op_arg *args) {
+  AirConsts<T> K = air_consts<T>();
+  if (error_pending()) return;
+  cudaStream_t s = rt().stream;
+  if (effective_strategy(name) == OP2B_STRATEGY_COLOURED) {
+    DevPlan *p = get_plan(name, set, OP_part_size, 6, args, 4, kBresInds);
+    if (!p) return;
+    LoopScope ls(name, p->transfer, p->transfer2);
+    PlanView v = plan_view(*p);
+    int nthread = OP_block_size > 0 ? OP_block_size : 512;
+    if (p->nshared > 48 * 1024)
+      OP2B_CUDA(cudaFuncSetAttribute(k_bres_calc_coloured<T>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, p->nshared));
+    for (int c = 0, off = 0; c < p->ncolors; off += p->ncolblk[c], c++)
+      if (p->ncolblk[c] > 0)
+        k_bres_calc_coloured<T><<<p->ncolblk[c], nthread, p->nshared, s>>>(
+            v, off, (const T *)args[0].dat->data_d, (const T *)args[2].dat->data_d,
+            (const T *)args[3].dat->data_d, (const int *)args[5].dat->data_d,
+            (T *)args[4].dat->data_d, K);
+    return;
+  }
+  GatherPlan *g = get_gather_plan(set, args, {4});
+  if (!g) return;
+  LoopScope ls(name, compulsory_bytes(set, 6, args), 0);
+  if (g->nactive == 0) return;
+  k_bres_calc_gather<T><<<(g->nactive + 255) / 256, 256, 0, s>>>(
+      g->nactive, g->d_active, g->d_row, g->d_keys, idx_map(args[0]), idx_map(args[1]),
+      idx_map(args[2]), idx_map(args[3]), idx_map(args[5]), (const T *)args[0].dat->data_d,
+      (const T *)args[1].dat->data_d, (const T *)args[2].dat->data_d,
+      (const T *)args[3].dat->data_d, (const int *)args[5].dat->data_d, (T *)args[4].dat->data_d,
+      K);
+}
+void run_bres_calc(char const *name, op_set set, const op_arg *args) {
+  if (is_double(args[0])) bres_calc_t<double>(name, set, args);
+  else bres_calc_t<float>(name, set, args);
+}
+
+template <class T>
+static void update_t(char const *name, op_set set, const op_arg *args) {
+  cudaStream_t s = rt().stream;
+  const int n = set->size;
+  const bool seq = rt().reduction == OP2B_REDUCE_SEQ;
+  int slot = red_new_slot();
+  T *result = (T *)red_slot_ptr(slot);
+  {
+    LoopScope ls(name, compulsory_bytes(set, 5, args), 0);
+    T *seqbuf = seq ? (T *)red_seq_buffer(sizeof(T) * 4 * (size_t)n) : nullptr;
+    const int threads = 256;
+    const int grid = seq ? grid_for(n, threads) : red_grid(n, threads);
+    RedSlot<T> rslot{(T *)red_partials(0), result};
+    k_update<T><<<grid, threads, 0, s>>>(n, (const T *)args[0].dat->data_d,
+                                         (T *)args[1].dat->data_d, (T *)args[2].dat->data_d,
+                                         (const T *)args[3].dat->data_d, seqbuf, rslot,
+                                         red_ticket());
+    if (seq) {
+      T init = *(const T *)args[4].data;
+      k_seq_sum<T><<<1, 32, 0, s>>>(seqbuf, 4LL * n, init, result);
+    }
+  }
+  red_finish({GblRequest{args[4].data, slot, OP_INC, sizeof(T) == 8 ? GBL_F64 : GBL_F32, seq}});
+}
+void run_airfoil_update(char const *name, op_set set, const op_arg *args) {
+  if (is_double(args[0])) update_t<double>(name, set, args);
+  else update_t<float>(name, set, args);
+}
+
+}  // namespace op2b

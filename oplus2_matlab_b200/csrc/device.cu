@@ -1,0 +1,262 @@
+// device.cu -- device set-up and data movement: op_init, op_decl_dat_char,
+// op_decl_const_char, op_fetch_data, op_exit (the CUDA half of the
+// reference's common/op_lib.cu:82-209), the library stream and loop timers.
+//
+// Layout in HBM: each op_dat lives in one allocation in the app's own
+// element-major order (element e, component d at e*dim+d).  Components of one
+// element are contiguous, so a thread reads a whole element with one
+// 8/16-byte vector load (float2 x, float4 q, 2 x double2 for FP64 q); the
+// direct loops stream 16-byte vectors per thread, which coalesces fully.
+
+#include <stdio.h>
+
+#include "internal.h"
+
+namespace op2b {
+
+void ensure_cuda() {
+  Runtime &R = rt();
+  if (R.cuda_ready) return;
+  int n = 0;
+  cudaError_t err = cudaGetDeviceCount(&n);
+  if (err != cudaSuccess || n == 0) {
+    fail(-1, "op2b error: no CUDA device available (%s)\n",
+         err == cudaSuccess ? "0 devices" : cudaGetErrorString(err));
+    return;
+  }
+  OP2B_CUDA(cudaGetDevice(&R.device));
+  cudaDeviceProp prop;
+  OP2B_CUDA(cudaGetDeviceProperties(&prop, R.device));
+  R.num_sms = prop.multiProcessorCount;
+  if (prop.major < 10)
+    fail(-1, "op2b error: device %s is sm_%d%d; this library is built for sm_100a\n", prop.name,
+         prop.major, prop.minor);
+  if (!R.stream) {
+    OP2B_CUDA(cudaStreamCreateWithFlags(&R.stream, cudaStreamNonBlocking));
+    R.own_stream = true;
+  }
+  R.cuda_ready = true;
+}
+
+void *dev_alloc(size_t bytes) {
+  void *p = nullptr;
+  if (bytes == 0) bytes = 16;
+  cudaError_t err = cudaMalloc(&p, bytes);
+  if (err != cudaSuccess) {
+    fail(-1, "op2b error: cudaMalloc of %zu bytes failed: %s\n", bytes, cudaGetErrorString(err));
+    return nullptr;
+  }
+  return p;
+}
+
+void dev_free(void *p) {
+  if (p) cudaFree(p);
+}
+
+static bool capturing() {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  if (rt().stream) cudaStreamIsCapturing(rt().stream, &st);
+  return st != cudaStreamCaptureStatusNone;
+}
+
+LoopScope::LoopScope(char const *name, double transfer, double transfer2) {
+  Runtime &R = rt();
+  LoopTimer &T = R.timers[name];
+  if (T.kernel_index < 0) {
+    T.name = name;
+    T.kernel_index = (int)R.timers.size() - 1;
+  }
+  t = &T;
+  T.count++;
+  op_timing_realloc(T.kernel_index);
+  op_kernel &k = OP_kernels[T.kernel_index];
+  k.name = T.name.c_str();
+  k.count += 1;
+  k.transfer += (float)transfer;
+  k.transfer2 += (float)transfer2;
+  if (!R.timing || capturing()) return;
+  if (T.pending.size() > 512) flush_timers();
+  if (T.free_pairs.empty()) {
+    cudaEvent_t a, b;
+    OP2B_CUDA(cudaEventCreate(&a));
+    OP2B_CUDA(cudaEventCreate(&b));
+    T.free_pairs.push_back({a, b});
+  }
+  ev = T.free_pairs.back();
+  T.free_pairs.pop_back();
+  OP2B_CUDA(cudaEventRecord(ev.first, R.stream));
+}
+
+LoopScope::~LoopScope() {
+  if (!ev.first) return;
+  cudaEventRecord(ev.second, rt().stream);
+  t->pending.push_back(ev);
+}
+
+void flush_timers() {
+  Runtime &R = rt();
+  for (auto &kv : R.timers) {
+    LoopTimer &T = kv.second;
+    for (auto &p : T.pending) {
+      float ms = 0.f;
+      if (cudaEventSynchronize(p.second) == cudaSuccess &&
+          cudaEventElapsedTime(&ms, p.first, p.second) == cudaSuccess) {
+        T.seconds += ms * 1e-3;
+        if (T.kernel_index >= 0 && T.kernel_index < OP_kern_max)
+          OP_kernels[T.kernel_index].time += ms * 1e-3f;
+      }
+      T.free_pairs.push_back(p);
+    }
+    T.pending.clear();
+  }
+}
+
+int const_get_f32(char const *name, float *out, int n) {
+  auto it = rt().consts.find(name);
+  if (it == rt().consts.end()) return 0;
+  const Runtime::Const &c = it->second;
+  int k = c.dim < n ? c.dim : n;
+  for (int i = 0; i < k; i++) {
+    if (c.type == "double") out[i] = (float)((const double *)c.bytes.data())[i];
+    else if (c.type == "float") out[i] = ((const float *)c.bytes.data())[i];
+    else if (c.type == "int") out[i] = (float)((const int *)c.bytes.data())[i];
+    else return 0;
+  }
+  return k;
+}
+
+int const_get_f64(char const *name, double *out, int n) {
+  auto it = rt().consts.find(name);
+  if (it == rt().consts.end()) return 0;
+  const Runtime::Const &c = it->second;
+  int k = c.dim < n ? c.dim : n;
+  for (int i = 0; i < k; i++) {
+    if (c.type == "double") out[i] = ((const double *)c.bytes.data())[i];
+    else if (c.type == "float") out[i] = (double)((const float *)c.bytes.data())[i];
+    else if (c.type == "int") out[i] = (double)((const int *)c.bytes.data())[i];
+    else return 0;
+  }
+  return k;
+}
+
+}  // namespace op2b
+
+using namespace op2b;
+
+extern void op2b_release_plans();  // plan.cu
+
+extern "C" {
+
+// common/op_lib.cu:128-143
+void op_init(int argc, char **argv, int diags) {
+  op_init_core(argc, argv, diags);
+  ensure_cuda();
+  if (!rt().cuda_ready) return;
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, rt().device);
+  printf("\n Using CUDA device: %s\n", prop.name);
+}
+
+// common/op_lib.cu:145-153: registry entry + device copy (synchronous, so
+// the caller may reuse its array on return)
+op_dat op_decl_dat_char(op_set set, int dim, char const *type, int size, char *data,
+                        char const *name) {
+  op_dat dat = op_decl_dat_core(set, dim, type, size, data, name);
+  if (!dat) return nullptr;
+  Runtime &R = rt();
+  ensure_cuda();
+  if (R.dats.size() <= (size_t)dat->index) R.dats.resize(dat->index + 1);
+  size_t bytes = (size_t)dat->size * set->size;
+  R.dats[dat->index].bytes = bytes;
+  dat->data_d = (char *)dev_alloc(bytes);
+  if (!dat->data_d) return dat;
+  if (data) OP2B_CUDA(cudaMemcpyAsync(dat->data_d, data, bytes, cudaMemcpyHostToDevice, R.stream));
+  else OP2B_CUDA(cudaMemsetAsync(dat->data_d, 0, bytes, R.stream));
+  OP2B_CUDA(cudaStreamSynchronize(R.stream));
+  return dat;
+}
+
+// airfoil/airfoil_kernels.cu:23-26 copied constants to __constant__ symbols
+// by name; here they are kept by name and handed to the loops as kernel
+// parameters (the parameter bank is constant memory too).  A later
+// declaration of the same name replaces the earlier one (jac2/jac.cpp:137-140).
+void op_decl_const_char(int dim, char const *type, int size, char *dat, char const *name) {
+  if (dim <= 0 || size <= 0 || dat == nullptr) {
+    fail(-1, "op_decl_const error -- invalid constant %s\n", name ? name : "(null)");
+    return;
+  }
+  Runtime::Const c;
+  c.type = type ? type : "";
+  c.dim = dim;
+  c.size = size;
+  c.bytes.assign(dat, dat + (size_t)dim * size);
+  rt().consts[name] = c;
+  rt().consts_version++;
+}
+
+// common/op_lib.cu:116-121: device -> the caller's original array
+void op_fetch_data(op_dat dat) {
+  if (!dat || !dat->data_d) return;
+  Runtime &R = rt();
+  deliver_deferred();
+  OP2B_CUDA(cudaMemcpyAsync(dat->data, dat->data_d, (size_t)dat->size * dat->set->size,
+                            cudaMemcpyDeviceToHost, R.stream));
+  OP2B_CUDA(cudaStreamSynchronize(R.stream));
+}
+
+// common/op_lib.cu:186-209
+void op_exit(void) {
+  Runtime &R = rt();
+  if (R.cuda_ready) {
+    deliver_deferred();
+    cudaStreamSynchronize(R.stream);
+    flush_timers();
+  }
+  op2b_release_plans();
+  for (auto &m : R.maps) dev_free(m.d);
+  R.maps.clear();
+  for (int i = 0; i < OP_dat_index; i++) dev_free(OP_dat_list[i]->data_d);
+  R.dats.clear();
+  for (auto &kv : R.timers) {
+    for (auto &p : kv.second.free_pairs) {
+      cudaEventDestroy(p.first);
+      cudaEventDestroy(p.second);
+    }
+  }
+  R.timers.clear();
+  R.consts.clear();
+  op_exit_core();
+}
+
+void *op2b_get_stream(void) {
+  ensure_cuda();
+  return (void *)rt().stream;
+}
+
+void op2b_set_stream(void *s) {
+  ensure_cuda();
+  Runtime &R = rt();
+  if (R.stream && R.stream != (cudaStream_t)s) cudaStreamSynchronize(R.stream);
+  R.stream = (cudaStream_t)s;
+  R.own_stream = false;
+}
+
+int op2b_sync(void) {
+  ensure_cuda();
+  deliver_deferred();
+  return (int)cudaStreamSynchronize(rt().stream);
+}
+
+double op2b_loop_time(char const *name, int *count) {
+  flush_timers();
+  auto it = rt().timers.find(name);
+  if (it == rt().timers.end()) return -1.0;
+  if (count) *count = it->second.count;
+  return it->second.seconds;
+}
+
+char const *op2b_version(void) {
+  return "libop2b200 (sm_100a; -fmad=false, IEEE div/sqrt)";
+}
+
+}  // extern "C"

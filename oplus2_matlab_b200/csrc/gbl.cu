@@ -1,0 +1,144 @@
+// gbl.cu -- host side of global reductions: device scratch, result slots,
+// and delivery into the caller's variables.
+//
+// Semantics kept from the reference CUDA back-end (airfoil/update_kernel.cu:
+// 116-169, jac1/update_kernel.cu:94-141): OP_INC adds the device sum to the
+// host value, OP_MAX / OP_MIN combine with it; the variable holds the result
+// when the loop call returns.  In deferred mode the device results wait in
+// slots until op2b_sync / op_fetch_data, so no call blocks.
+
+#include "loops.h"
+
+namespace op2b {
+
+namespace {
+constexpr int kSlots = 4096;
+struct RedState {
+  char *dev = nullptr;  // [2 x kMaxRedBlocks x 8] partials | ticket (256 B) | slots
+  char *host = nullptr; // pinned mirror of the slots
+  int next_slot = 0;
+  void *seq = nullptr;
+  size_t seq_bytes = 0;
+};
+RedState &rs() {
+  static RedState s;
+  return s;
+}
+size_t off_ticket() { return 2 * (size_t)kMaxRedBlocks * 8; }
+size_t off_slots() { return off_ticket() + 256; }
+
+void ensure_red() {
+  RedState &S = rs();
+  if (S.dev) return;
+  size_t bytes = off_slots() + (size_t)kSlots * 8;
+  S.dev = (char *)dev_alloc(bytes);
+  OP2B_CUDA(cudaMemset(S.dev, 0, bytes));
+  OP2B_CUDA(cudaMallocHost((void **)&S.host, (size_t)kSlots * 8));
+}
+
+template <class T>
+void combine(char *host, const T v, op_access acc, bool assign) {
+  T *h = (T *)host;
+  switch (acc) {
+    case OP_INC: *h = assign ? v : (T)(*h + v); break;
+    case OP_MAX: *h = (*h > v) ? *h : v; break;
+    case OP_MIN: *h = (*h < v) ? *h : v; break;
+    default: break;
+  }
+}
+
+void deliver(const std::vector<GblRequest> &reqs) {
+  RedState &S = rs();
+  if (reqs.empty()) return;
+  int lo = kSlots, hi = -1;
+  for (auto &r : reqs) {
+    lo = std::min(lo, r.slot);
+    hi = std::max(hi, r.slot);
+  }
+  OP2B_CUDA(cudaMemcpyAsync(S.host + (size_t)lo * 8, S.dev + off_slots() + (size_t)lo * 8,
+                            (size_t)(hi - lo + 1) * 8, cudaMemcpyDeviceToHost, rt().stream));
+  OP2B_CUDA(cudaStreamSynchronize(rt().stream));
+  for (auto &r : reqs) {
+    const char *p = S.host + (size_t)r.slot * 8;
+    if (r.type == GBL_F64) combine<double>(r.host, *(const double *)p, r.acc, r.assign);
+    else combine<float>(r.host, *(const float *)p, r.acc, r.assign);
+  }
+}
+
+std::vector<GblRequest> &pending() {
+  static std::vector<GblRequest> v;
+  return v;
+}
+}  // namespace
+
+void *red_partials(int i) {
+  ensure_red();
+  return rs().dev + (size_t)i * kMaxRedBlocks * 8;
+}
+
+unsigned *red_ticket() {
+  ensure_red();
+  return (unsigned *)(rs().dev + off_ticket());
+}
+
+void *red_slot_ptr(int slot) {
+  ensure_red();
+  return rs().dev + off_slots() + (size_t)slot * 8;
+}
+
+int red_new_slot() {
+  ensure_red();
+  RedState &S = rs();
+  if (S.next_slot >= kSlots) {
+    deliver_deferred();  // frees every slot
+    S.next_slot = 0;
+  }
+  return S.next_slot++;
+}
+
+void *red_seq_buffer(size_t bytes) {
+  RedState &S = rs();
+  if (bytes > S.seq_bytes) {
+    OP2B_CUDA(cudaStreamSynchronize(rt().stream));
+    dev_free(S.seq);
+    S.seq = dev_alloc(bytes);
+    S.seq_bytes = bytes;
+  }
+  return S.seq;
+}
+
+int red_grid(long long n, int threads) {
+  long long want = (n + threads - 1) / threads;
+  long long cap = (long long)rt().num_sms * 4;
+  if (cap > kMaxRedBlocks) cap = kMaxRedBlocks;
+  if (want < 1) want = 1;
+  return (int)(want < cap ? want : cap);
+}
+
+void red_finish(const std::vector<GblRequest> &reqs) {
+  if (reqs.empty()) return;
+  if (rt().gbl_deferred) {
+    for (auto &r : reqs) pending().push_back(r);
+    return;
+  }
+  deliver(reqs);
+  if (pending().empty()) rs().next_slot = 0;
+}
+
+void deliver_deferred() {
+  if (pending().empty()) return;
+  std::vector<GblRequest> v;
+  v.swap(pending());
+  deliver(v);
+  rs().next_slot = 0;
+}
+
+}  // namespace op2b
+
+extern "C" int op2b_set_gbl_deferred(int on) {
+  op2b::Runtime &R = op2b::rt();
+  int old = R.gbl_deferred;
+  if (old && !on) op2b::deliver_deferred();
+  R.gbl_deferred = on != 0;
+  return old;
+}

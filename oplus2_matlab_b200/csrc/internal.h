@@ -1,0 +1,117 @@
+// internal.h -- shared declarations of libop2b200 (not installed).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "op2b.h"
+#include "op_lib.h"
+
+extern "C" int OP_cache_line_size;  // common/op_lib_core.c:43, not in op_lib.h
+
+namespace op2b {
+
+// ---------------------------------------------------------------- errors --
+// Print like the reference (printf + exit) in EXIT mode; in RETURN mode print,
+// remember the message and let the caller return a neutral value.
+void fail(int exit_code, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
+bool error_pending();  // a fail() happened since the last clear (RETURN mode)
+
+void cuda_fail(cudaError_t err, const char *what, const char *file, int line);
+#define OP2B_CUDA(call)                                                    \
+  do {                                                                     \
+    cudaError_t e_ = (call);                                               \
+    if (e_ != cudaSuccess) ::op2b::cuda_fail(e_, #call, __FILE__, __LINE__); \
+  } while (0)
+
+// ------------------------------------------------------------ device data --
+struct MapDev {
+  int *d = nullptr;  // device copy of map->map, same layout (from-major, dim-minor)
+};
+
+struct DatDev {
+  size_t bytes = 0;  // set->size * dat->size
+};
+
+// per-loop timing record (op_kernel of the reference plus device events)
+struct LoopTimer {
+  std::string name;
+  int kernel_index = -1;  // slot in OP_kernels
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> free_pairs;
+  double seconds = 0.0;
+  int count = 0;
+};
+
+struct Runtime {
+  bool cuda_ready = false;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int strategy = OP2B_STRATEGY_AUTO;
+  int reduction = OP2B_REDUCE_TREE;
+  int error_mode = OP2B_ERRORS_EXIT;
+  bool gbl_deferred = false;
+  bool timing = true;
+  int num_sms = 148;
+
+  std::vector<MapDev> maps;  // by op_map index
+  std::vector<DatDev> dats;  // by op_dat index
+
+  // constants declared by op_decl_const_char, by name (raw bytes + type)
+  struct Const {
+    std::string type;
+    int dim = 0, size = 0;
+    std::vector<char> bytes;
+  };
+  std::map<std::string, Const> consts;
+  unsigned consts_version = 0;
+
+  std::map<std::string, LoopTimer> timers;
+
+  // device scratch for global reductions: partials + final slots
+  void *red_scratch = nullptr;
+  size_t red_scratch_bytes = 0;
+  void *red_host = nullptr;  // pinned mirror of the final slots
+  size_t red_host_bytes = 0;
+
+  // deferred global reductions waiting for the next sync
+  struct DeferredGbl {
+    char *host;        // user variable
+    int bytes_offset;  // offset of the result in red_host
+    int dim;
+    op_access acc;
+    int is_double;
+  };
+  std::vector<DeferredGbl> deferred;
+};
+
+Runtime &rt();
+
+// device memory helpers (long-lived allocations)
+void *dev_alloc(size_t bytes);
+void dev_free(void *p);
+void ensure_cuda();  // op_init's device part, also run lazily
+
+// timing around one loop call
+struct LoopScope {
+  LoopTimer *t = nullptr;
+  std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+  LoopScope(char const *name, double transfer, double transfer2);
+  ~LoopScope();
+};
+void flush_timers();  // harvest finished event pairs into OP_kernels
+
+// constants lookup: copies up to n values of the named constant into out,
+// converted to T; returns the number found (0 if never declared)
+int const_get_f32(char const *name, float *out, int n);
+int const_get_f64(char const *name, double *out, int n);
+
+// global reductions: device slot management (reduce.cu)
+void deliver_deferred();
+
+}  // namespace op2b

@@ -1,0 +1,210 @@
+// jac.cu -- the two loops of the jac1 / jac2 Jacobi apps as sm_100a kernels,
+// replacing the generated jac*/res_kernel.cu and jac*/update_kernel.cu.
+//
+//   res    (jac1/res.h:1-3)    du[p0] += beta * A * u[p1], p = edge->node map
+//   update (jac1/update.h:1-6) u += du + alpha*r; du = 0;
+//                              u_sum += u*u; u_max = MAX(u_max, u)
+// jac2 stores A as double[3], u as float[2], du as float[3], r as float[2]
+// and uses component 0 only (jac2/res.h, jac2/update.h); beta * A * u is
+// evaluated in double there, and so it is here.
+
+#include <math.h>
+#include <string.h>
+
+#include "loops.h"
+#include "reduce.cuh"
+
+namespace op2b {
+
+__device__ __forceinline__ int jat(const IdxMap &m, int e) {
+  return m.map ? __ldg(m.map + m.idx + (size_t)e * m.dim) : e;
+}
+
+// V = 1: A float[1], u float[1], du float[1];  V = 2: A double[3], u float[2], du float[3]
+template <int V>
+struct JacLayout;
+template <>
+struct JacLayout<1> {
+  typedef float AT;
+  static constexpr int A = 1, U = 1, DU = 1, R = 1;
+};
+template <>
+struct JacLayout<2> {
+  typedef double AT;
+  static constexpr int A = 3, U = 2, DU = 3, R = 2;
+};
+
+// du += beta * A * u, with jac2's double product
+template <int V>
+__device__ __forceinline__ float jac_inc(float du, float beta, typename JacLayout<V>::AT a, float u) {
+  if (V == 1) return du + beta * (float)a * u;
+  return (float)((double)du + (double)beta * (double)a * (double)u);
+}
+
+// res, GATHER: one thread per node with incoming contributions
+template <int V>
+__global__ void k_jac_res_gather(int nrows, const int *__restrict__ active,
+                                 const int *__restrict__ row, const int *__restrict__ keys,
+                                 IdxMap mA, IdxMap mu,
+                                 const typename JacLayout<V>::AT *__restrict__ A,
+                                 const float *__restrict__ u, float *__restrict__ du, float beta) {
+  typedef JacLayout<V> L;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nrows) return;
+  int n = active ? active[t] : t;
+  float d = du[(size_t)n * L::DU];
+  int k1 = row[t + 1];
+  for (int k = row[t]; k < k1; k++) {
+    int e = __ldg(keys + k);
+    typename L::AT a = __ldg(A + (size_t)jat(mA, e) * L::A);
+    float uu = __ldg(u + (size_t)jat(mu, e) * L::U);
+    d = jac_inc<V>(d, beta, a, uu);
+  }
+  du[(size_t)n * L::DU] = d;
+}
+
+struct JacPlanView {
+  const int *blkmap, *offset, *nelems, *nthrcol, *thrcol, *ind_offs, *ind_sizes;
+  const int *ind_u, *ind_du;
+  const short *loc_u, *loc_du;
+};
+
+// res, COLOURED (inds {-1, 0, 1, -1}: u read, du incremented)
+template <int V>
+__global__ void k_jac_res_coloured(JacPlanView P, int block_offset, IdxMap mA,
+                                   const typename JacLayout<V>::AT *__restrict__ A,
+                                   const float *__restrict__ u, float *__restrict__ du,
+                                   float beta) {
+  typedef JacLayout<V> L;
+  extern __shared__ __align__(16) char smem[];
+  const int b = P.blkmap[blockIdx.x + block_offset];
+  const int nelem = P.nelems[b], off = P.offset[b], ncol = P.nthrcol[b];
+  const int su = P.ind_sizes[0 + b * 2], sd = P.ind_sizes[1 + b * 2];
+  const int ou = P.ind_offs[0 + b * 2], od = P.ind_offs[1 + b * 2];
+  float *us = (float *)smem;
+  float *ds = (float *)(smem + ROUND_UP(su * L::U * (int)sizeof(float)));
+  for (int i = threadIdx.x; i < su * L::U; i += blockDim.x)
+    us[i] = u[(size_t)P.ind_u[ou + i / L::U] * L::U + i % L::U];
+  for (int i = threadIdx.x; i < sd * L::DU; i += blockDim.x) ds[i] = 0.0f;
+  __syncthreads();
+  const int nelems2 = blockDim.x * (1 + (nelem - 1) / blockDim.x);
+  for (int n = threadIdx.x; n < nelems2; n += blockDim.x) {
+    int col2 = -1, md = 0;
+    float l[L::DU];
+    for (int j = 0; j < L::DU; j++) l[j] = 0.0f;
+    if (n < nelem) {
+      const int e = n + off;
+      typename L::AT a = __ldg(A + (size_t)jat(mA, e) * L::A);
+      l[0] = jac_inc<V>(l[0], beta, a, us[P.loc_u[e] * L::U]);
+      md = P.loc_du[e];
+      col2 = P.thrcol[e];
+    }
+    for (int col = 0; col < ncol; col++) {
+      if (col2 == col)
+        for (int j = 0; j < L::DU; j++) ds[j + md * L::DU] += l[j];
+      __syncthreads();
+    }
+  }
+  for (int i = threadIdx.x; i < sd * L::DU; i += blockDim.x)
+    du[(size_t)P.ind_du[od + i / L::DU] * L::DU + i % L::DU] += ds[i];
+}
+
+// update (direct): SEQ != nullptr stores u*u in element order for the serial
+// fold; the maximum is order independent and always folded as a tree
+template <int V>
+__global__ void k_jac_update(int n, const float *__restrict__ r, float *__restrict__ du,
+                             float *__restrict__ u, float alpha, float *seq,
+                             RedSlot<float> s_sum, RedSlot<float> s_max, unsigned *ticket) {
+  typedef JacLayout<V> L;
+  float sum = 0.0f, mx = -INFINITY;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float *up = u + (size_t)i * L::U;
+    float *dp = du + (size_t)i * L::DU;
+    float uu = *up + (*dp + alpha * __ldg(r + (size_t)i * L::R));
+    *up = uu;
+    *dp = 0.0f;
+    float sq = uu * uu;
+    sum += sq;
+    mx = (mx > uu) ? mx : uu;
+    if (seq) seq[i] = sq;
+  }
+  const float v[2] = {sum, mx}, id[2] = {0.0f, -INFINITY};
+  RedSlot<float> sl[2] = {s_sum, s_max};
+  grid_finish<float, OpSum, OpMax, 2>(v, id, OpSum(), OpMax(), sl, ticket);
+}
+
+static const int kJacResInds[4] = {-1, 0, 1, -1};
+
+template <int V>
+static void jac_res_t(char const *name, op_set set, const op_arg *args) {
+  typedef JacLayout<V> L;
+  cudaStream_t s = rt().stream;
+  const float beta = *(const float *)args[3].data;  // gbl OP_READ, passed by value
+  if (effective_strategy(name) == OP2B_STRATEGY_COLOURED) {
+    DevPlan *p = get_plan(name, set, OP_part_size, 4, args, 2, kJacResInds);
+    if (!p) return;
+    LoopScope ls(name, p->transfer, p->transfer2);
+    JacPlanView v;
+    v.blkmap = p->d_blkmap; v.offset = p->d_offset; v.nelems = p->d_nelems;
+    v.nthrcol = p->d_nthrcol; v.thrcol = p->d_thrcol; v.ind_offs = p->d_ind_offs;
+    v.ind_sizes = p->d_ind_sizes; v.ind_u = p->d_ind_maps[0]; v.ind_du = p->d_ind_maps[1];
+    v.loc_u = p->d_loc_maps[1]; v.loc_du = p->d_loc_maps[2];
+    int nthread = OP_block_size > 0 ? OP_block_size : 512;
+    if (p->nshared > 48 * 1024)
+      OP2B_CUDA(cudaFuncSetAttribute(k_jac_res_coloured<V>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, p->nshared));
+    for (int c = 0, off = 0; c < p->ncolors; off += p->ncolblk[c], c++)
+      if (p->ncolblk[c] > 0)
+        k_jac_res_coloured<V><<<p->ncolblk[c], nthread, p->nshared, s>>>(
+            v, off, idx_map(args[0]), (const typename L::AT *)args[0].dat->data_d,
+            (const float *)args[1].dat->data_d, (float *)args[2].dat->data_d, beta);
+    return;
+  }
+  GatherPlan *g = get_gather_plan(set, args, {2});
+  if (!g) return;
+  LoopScope ls(name, compulsory_bytes(set, 4, args), 0);
+  if (g->nactive == 0) return;
+  k_jac_res_gather<V><<<(g->nactive + 255) / 256, 256, 0, s>>>(
+      g->nactive, g->d_active, g->d_row, g->d_keys, idx_map(args[0]), idx_map(args[1]),
+      (const typename L::AT *)args[0].dat->data_d, (const float *)args[1].dat->data_d,
+      (float *)args[2].dat->data_d, beta);
+}
+
+void run_jac_res(char const *name, op_set set, const op_arg *args, int variant) {
+  if (variant == 2) jac_res_t<2>(name, set, args);
+  else jac_res_t<1>(name, set, args);
+}
+
+template <int V>
+static void jac_update_t(char const *name, op_set set, const op_arg *args) {
+  cudaStream_t s = rt().stream;
+  float alpha = 0.f;
+  if (const_get_f32("alpha", &alpha, 1) < 1) {
+    fail(-1, "op2b error -- constant \"alpha\" not declared with op_decl_const2\n");
+    return;
+  }
+  const int n = set->size;
+  const bool seq = rt().reduction == OP2B_REDUCE_SEQ;
+  int slot_sum = red_new_slot(), slot_max = red_new_slot();
+  float *r_sum = (float *)red_slot_ptr(slot_sum), *r_max = (float *)red_slot_ptr(slot_max);
+  {
+    LoopScope ls(name, compulsory_bytes(set, 5, args), 0);
+    float *seqbuf = seq ? (float *)red_seq_buffer(sizeof(float) * (size_t)n) : nullptr;
+    const int threads = 256, grid = red_grid(n, threads);
+    RedSlot<float> ss{(float *)red_partials(0), r_sum}, sm{(float *)red_partials(1), r_max};
+    k_jac_update<V><<<grid, threads, 0, s>>>(n, (const float *)args[0].dat->data_d,
+                                             (float *)args[1].dat->data_d,
+                                             (float *)args[2].dat->data_d, alpha, seqbuf, ss, sm,
+                                             red_ticket());
+    if (seq) k_seq_sum<float><<<1, 32, 0, s>>>(seqbuf, n, *(const float *)args[3].data, r_sum);
+  }
+  red_finish({GblRequest{args[3].data, slot_sum, OP_INC, GBL_F32, seq},
+              GblRequest{args[4].data, slot_max, OP_MAX, GBL_F32, false}});
+}
+
+void run_jac_update(char const *name, op_set set, const op_arg *args, int variant) {
+  if (variant == 2) jac_update_t<2>(name, set, args);
+  else jac_update_t<1>(name, set, args);
+}
+
+}  // namespace op2b

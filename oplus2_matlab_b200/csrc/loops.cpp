@@ -1,0 +1,205 @@
+// loops.cpp -- op_par_loop entry points and their dispatch.
+//
+// The reference generates one host stub per loop (op2.m; e.g.
+// airfoil/res_calc_kernel.cu:158-245).  Here every op_par_loop_<name> entry
+// point, and the generic op2b_par_loop, check their arguments the way
+// op_arg_check does (common/op_lib_core.c:266-305) and then match the
+// argument signature (access, dims, types, direct or indirect) against the
+// loops this library implements on the device.  A call that matches none is
+// an error, never a host fallback.
+
+#include <stdarg.h>
+#include <string.h>
+
+#include <set>
+
+#include "loops.h"
+
+namespace op2b {
+
+int effective_strategy(char const *loop_name) {
+  (void)loop_name;
+  int s = rt().strategy;
+  return s == OP2B_STRATEGY_COLOURED ? OP2B_STRATEGY_COLOURED : OP2B_STRATEGY_GATHER;
+}
+
+double compulsory_bytes(op_set set, int nargs, const op_arg *args) {
+  std::set<const void *> maps_seen;
+  std::set<const void *> dats_seen;
+  double bytes = 0;
+  for (int m = 0; m < nargs; m++) {
+    const op_arg &a = args[m];
+    if (a.argtype != OP_ARG_DAT || !a.dat) continue;
+    if (a.map && maps_seen.insert(a.map).second)
+      bytes += 4.0 * a.map->dim * (double)set->size;
+    if (dats_seen.insert(a.dat).second) {
+      double fac = (a.acc == OP_READ || a.acc == OP_WRITE) ? 1.0 : 2.0;
+      bytes += fac * a.dat->size * (double)a.dat->set->size;
+    }
+  }
+  return bytes;
+}
+
+}  // namespace op2b
+
+using namespace op2b;
+
+namespace {
+
+bool dat_arg(const op_arg &a, int dim, op_access acc, bool indirect, const char *type = nullptr) {
+  if (a.argtype != OP_ARG_DAT || !a.dat || a.dim != dim || a.acc != acc) return false;
+  if (indirect != (a.map != nullptr)) return false;
+  if (type && strcmp(a.dat->type, type) != 0) return false;
+  return true;
+}
+
+bool gbl_arg(const op_arg &a, int dim, op_access acc, const char *type) {
+  return a.argtype == OP_ARG_GBL && a.dim == dim && a.acc == acc && a.type &&
+         strcmp(a.type, type) == 0 && a.data != nullptr;
+}
+
+bool real_type(const op_arg &a, const char *&t) {
+  if (!a.dat) return false;
+  if (strcmp(a.dat->type, "float") == 0 || strcmp(a.dat->type, "double") == 0) {
+    if (!t) t = a.dat->type;
+    return strcmp(a.dat->type, t) == 0;
+  }
+  return false;
+}
+
+bool same_types(const op_arg *args, std::initializer_list<int> which) {
+  const char *t = nullptr;
+  for (int i : which)
+    if (!real_type(args[i], t)) return false;
+  return true;
+}
+
+// airfoil/airfoil_op.cpp:245-292 argument lists
+bool is_save_soln(int n, const op_arg *a) {
+  return n == 2 && dat_arg(a[0], 4, OP_READ, false) && dat_arg(a[1], 4, OP_WRITE, false) &&
+         same_types(a, {0, 1});
+}
+bool is_adt_calc(int n, const op_arg *a) {
+  return n == 6 && dat_arg(a[0], 2, OP_READ, true) && dat_arg(a[1], 2, OP_READ, true) &&
+         dat_arg(a[2], 2, OP_READ, true) && dat_arg(a[3], 2, OP_READ, true) &&
+         dat_arg(a[4], 4, OP_READ, false) && dat_arg(a[5], 1, OP_WRITE, false) &&
+         same_types(a, {0, 1, 2, 3, 4, 5});
+}
+bool is_res_calc(int n, const op_arg *a) {
+  return n == 8 && dat_arg(a[0], 2, OP_READ, true) && dat_arg(a[1], 2, OP_READ, true) &&
+         dat_arg(a[2], 4, OP_READ, true) && dat_arg(a[3], 4, OP_READ, true) &&
+         dat_arg(a[4], 1, OP_READ, true) && dat_arg(a[5], 1, OP_READ, true) &&
+         dat_arg(a[6], 4, OP_INC, true) && dat_arg(a[7], 4, OP_INC, true) &&
+         a[6].dat == a[7].dat && a[0].dat == a[1].dat && a[2].dat == a[3].dat &&
+         a[4].dat == a[5].dat && same_types(a, {0, 1, 2, 3, 4, 5, 6, 7});
+}
+bool is_bres_calc(int n, const op_arg *a) {
+  return n == 6 && dat_arg(a[0], 2, OP_READ, true) && dat_arg(a[1], 2, OP_READ, true) &&
+         dat_arg(a[2], 4, OP_READ, true) && dat_arg(a[3], 1, OP_READ, true) &&
+         dat_arg(a[4], 4, OP_INC, true) && dat_arg(a[5], 1, OP_READ, false, "int") &&
+         a[0].dat == a[1].dat && same_types(a, {0, 1, 2, 3, 4});
+}
+bool is_airfoil_update(int n, const op_arg *a) {
+  if (n != 5 || !dat_arg(a[0], 4, OP_READ, false) || !dat_arg(a[1], 4, OP_WRITE, false) ||
+      !dat_arg(a[2], 4, OP_RW, false) || !dat_arg(a[3], 1, OP_READ, false) ||
+      !same_types(a, {0, 1, 2, 3}))
+    return false;
+  return gbl_arg(a[4], 1, OP_INC, a[0].dat->type);
+}
+// jac1/jac_op.cpp:168-181, jac2/jac_op.cpp likewise
+int jac_res_variant(int n, const op_arg *a) {
+  if (n != 4 || !gbl_arg(a[3], 1, OP_READ, "float")) return 0;
+  if (dat_arg(a[0], 1, OP_READ, false, "float") && dat_arg(a[1], 1, OP_READ, true, "float") &&
+      dat_arg(a[2], 1, OP_INC, true, "float"))
+    return 1;
+  if (dat_arg(a[0], 3, OP_READ, false, "double") && dat_arg(a[1], 2, OP_READ, true, "float") &&
+      dat_arg(a[2], 3, OP_INC, true, "float"))
+    return 2;
+  return 0;
+}
+int jac_update_variant(int n, const op_arg *a) {
+  if (n != 5 || !gbl_arg(a[3], 1, OP_INC, "float") || !gbl_arg(a[4], 1, OP_MAX, "float"))
+    return 0;
+  if (dat_arg(a[0], 1, OP_READ, false, "float") && dat_arg(a[1], 1, OP_RW, false, "float") &&
+      dat_arg(a[2], 1, OP_INC, false, "float"))
+    return 1;
+  if (dat_arg(a[0], 2, OP_READ, false, "float") && dat_arg(a[1], 3, OP_RW, false, "float") &&
+      dat_arg(a[2], 2, OP_INC, false, "float"))
+    return 2;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+void op2b_par_loop(char const *name, op_set set, int nargs, const op_arg *args) {
+  if (set == nullptr) {
+    fail(1, "error: invalid set in kernel \"%s\"\n", name ? name : "(null)");
+    return;
+  }
+  if (!rt().cuda_ready) {
+    ensure_cuda();
+    if (error_pending()) return;
+  }
+  // the checks op_seq.h runs when OP_diags > 0 (common/op_seq.h:37-39); a
+  // device loop always runs them, since bad arguments would fault the GPU
+  int ninds = 0;
+  for (int m = 0; m < nargs; m++) {
+    op_arg_check(set, m, args[m], &ninds, name);
+    if (error_pending()) return;
+    if (args[m].argtype == OP_ARG_DAT && (!args[m].dat || !args[m].dat->data_d)) {
+      fail(1, "error: arg %d in kernel \"%s\"\ndataset has no device copy \n", m, name);
+      return;
+    }
+  }
+  if (OP_diags > 2) {
+    if (ninds == 0) printf(" kernel routine w/o indirection:  %s \n", name);
+    else printf(" kernel routine with indirection: %s \n", name);
+  }
+  int v;
+  if (is_res_calc(nargs, args)) return run_res_calc(name, set, args);
+  if (is_adt_calc(nargs, args)) return run_adt_calc(name, set, args);
+  if (is_bres_calc(nargs, args)) return run_bres_calc(name, set, args);
+  if (is_save_soln(nargs, args)) return run_save_soln(name, set, args);
+  if (is_airfoil_update(nargs, args)) return run_airfoil_update(name, set, args);
+  if ((v = jac_res_variant(nargs, args))) return run_jac_res(name, set, args, v);
+  if ((v = jac_update_variant(nargs, args))) return run_jac_update(name, set, args, v);
+  fail(1,
+       "op2b error: no device implementation of loop \"%s\" with this argument signature "
+       "(%d args)\n",
+       name, nargs);
+}
+
+// the per-loop entry points of the generated app mains
+// (airfoil/airfoil_op.cpp:64-99, jac1/jac_op.cpp:58-73)
+void op_par_loop_save_soln(char const *name, op_set set, op_arg a0, op_arg a1) {
+  op_arg args[2] = {a0, a1};
+  op2b_par_loop(name, set, 2, args);
+}
+void op_par_loop_adt_calc(char const *name, op_set set, op_arg a0, op_arg a1, op_arg a2,
+                          op_arg a3, op_arg a4, op_arg a5) {
+  op_arg args[6] = {a0, a1, a2, a3, a4, a5};
+  op2b_par_loop(name, set, 6, args);
+}
+void op_par_loop_res_calc(char const *name, op_set set, op_arg a0, op_arg a1, op_arg a2,
+                          op_arg a3, op_arg a4, op_arg a5, op_arg a6, op_arg a7) {
+  op_arg args[8] = {a0, a1, a2, a3, a4, a5, a6, a7};
+  op2b_par_loop(name, set, 8, args);
+}
+void op_par_loop_bres_calc(char const *name, op_set set, op_arg a0, op_arg a1, op_arg a2,
+                           op_arg a3, op_arg a4, op_arg a5) {
+  op_arg args[6] = {a0, a1, a2, a3, a4, a5};
+  op2b_par_loop(name, set, 6, args);
+}
+void op_par_loop_update(char const *name, op_set set, op_arg a0, op_arg a1, op_arg a2,
+                        op_arg a3, op_arg a4) {
+  op_arg args[5] = {a0, a1, a2, a3, a4};
+  op2b_par_loop(name, set, 5, args);
+}
+void op_par_loop_res(char const *name, op_set set, op_arg a0, op_arg a1, op_arg a2, op_arg a3) {
+  op_arg args[4] = {a0, a1, a2, a3};
+  op2b_par_loop(name, set, 4, args);
+}
+
+}  // extern "C"

@@ -1,0 +1,62 @@
+// loops.h -- host-side pieces shared by the loop implementations.
+#pragma once
+
+#include <vector>
+
+#include "internal.h"
+#include "plan.h"
+
+namespace op2b {
+
+// device view of one argument's indirection: element e -> map[idx + e*dim],
+// or e itself when map == nullptr (OP_ID)
+struct IdxMap {
+  const int *map;
+  int dim, idx;
+};
+
+inline IdxMap idx_map(const op_arg &a) {
+  IdxMap m{nullptr, 0, 0};
+  if (a.map) {
+    m.map = rt().maps[a.map->index].d;
+    m.dim = a.map->dim;
+    m.idx = a.idx;
+  }
+  return m;
+}
+
+// strategy actually used for a loop with OP_INC through a map
+int effective_strategy(char const *loop_name);
+
+// algorithmic (compulsory) bytes of one loop call: every distinct map array
+// once, every distinct dataset once, read-write and increment data twice
+double compulsory_bytes(op_set set, int nargs, const op_arg *args);
+
+// -------------------------------------------------- global reductions -----
+enum GblType { GBL_F32 = 0, GBL_F64 = 1 };
+struct GblRequest {
+  char *host;      // caller's variable (op_arg.data)
+  int slot;        // result slot in the device ring
+  op_access acc;
+  int type;        // GblType
+  bool assign;     // SEQ-mode sum: device value already includes the seed
+};
+constexpr int kMaxRedBlocks = 4096;
+void *red_partials(int i);       // [kMaxRedBlocks] of 8-byte entries, i in {0,1}
+unsigned *red_ticket();
+void *red_slot_ptr(int slot);    // 8-byte device slot
+int red_new_slot();
+void *red_seq_buffer(size_t bytes);  // scratch for SEQ-mode contributions
+void red_finish(const std::vector<GblRequest> &reqs);
+int red_grid(long long n, int threads);  // fixed grid for a set size
+
+// loop implementations (airfoil.cu, jac.cu)
+void run_save_soln(char const *name, op_set set, const op_arg *args);
+void run_adt_calc(char const *name, op_set set, const op_arg *args);
+void run_res_calc(char const *name, op_set set, const op_arg *args);
+void run_bres_calc(char const *name, op_set set, const op_arg *args);
+void run_airfoil_update(char const *name, op_set set, const op_arg *args);
+void run_jac_res(char const *name, op_set set, const op_arg *args, int variant);
+void run_jac_update(char const *name, op_set set, const op_arg *args, int variant);
+
+}  // namespace op2b

@@ -1,0 +1,72 @@
+// plan.h -- device execution plans (not installed).
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "internal.h"
+
+namespace op2b {
+
+// The reference's execution plan (common/op_lib_core.h:122-150), built on the
+// device by build_plan() and kept there.  Arrays follow the reference's
+// definitions exactly; `pub` is the op_plan view handed to callers of
+// op_plan_get (device pointers except ncolblk and nindirect).
+struct DevPlan {
+  // cache key (common/op_lib_core.c:632-659)
+  std::string name;
+  op_set set = nullptr;
+  int part_size = 0, nargs = 0, ninds = 0;
+  std::vector<op_dat> dats;
+  std::vector<op_map> maps;
+  std::vector<int> idxs, inds;
+  std::vector<op_access> accs;
+
+  int bsize = 0, nblocks = 0, ncolors = 0, nshared = 0;
+  int *d_nthrcol = nullptr, *d_thrcol = nullptr, *d_offset = nullptr, *d_nelems = nullptr;
+  int *d_ind_offs = nullptr, *d_ind_sizes = nullptr, *d_blkmap = nullptr;
+  std::vector<int *> d_ind_maps;
+  std::vector<short *> d_loc_maps;
+  std::vector<int> nindirect, ncolblk, colstart;  // host
+  std::vector<int> nthrcol_h;                     // host copy (for diagnostics)
+  double transfer = 0, transfer2 = 0, transfer3 = 0;
+  float avg_thread_colours = 0;
+  int max_thread_colours = 0;
+  op_plan pub;
+  std::vector<int *> pub_ind_maps;
+  std::vector<short *> pub_loc_maps;
+  int count = 0;
+};
+
+// Owner-computes ("gather") plan for one group of OP_INC arguments that
+// increment the same dataset: for every target element, the list of
+// (element, slot) contributions in ascending order, slot = position of the
+// argument inside the group.  This is the order of the sequential back-end
+// (common/op_seq.h:26-57, element loop outermost, arguments in kernel order).
+struct GatherPlan {
+  op_set set = nullptr;           // loop set
+  op_dat dat = nullptr;           // incremented dataset
+  std::vector<op_map> maps;       // per slot
+  std::vector<int> idxs;          // per slot
+  int nslots = 0;
+  int ntarget = 0;                // size of dat->set
+  int nactive = 0;                // targets with at least one contribution
+  int *d_row = nullptr;           // [nactive + 1] offsets into d_keys
+  int *d_keys = nullptr;          // [set->size * nslots] element * nslots + slot
+  int *d_active = nullptr;        // [nactive] target ids, nullptr when all active
+  int max_row = 0;
+};
+
+// Find or build the reference-compatible plan (device resident).
+DevPlan *get_plan(char const *name, op_set set, int part_size, int nargs, const op_arg *args,
+                  int ninds, const int *inds);
+// Find or build the gather plan for the INC args listed in slots (all on
+// the same dat).
+GatherPlan *get_gather_plan(op_set set, const op_arg *args, const std::vector<int> &slots);
+// Device validation of a plan; returns the number of violations.
+long validate_plan(const DevPlan &p);
+
+// device-wide exclusive scan of n ints (in place allowed); returns the total
+long long exclusive_scan(const int *d_in, int *d_out, int n, cudaStream_t s);
+
+}  // namespace op2b
