@@ -1,0 +1,470 @@
+#!/usr/bin/env python
+"""Benchmark: airfoil 720k-cell outer iterations per second on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the reference's airfoil app at the 720k-cell mesh, I=400, J=600,
+FP32): one step = one outer iteration = save_soln + 2 x (adt_calc, res_calc,
+bres_calc, update with the rms reduction).  Synthetic input: the NACA0012
+C-mesh of airfoil/naca0012.m restated in csrc/meshgen.cpp, flow at free
+stream (Mach 0.4) -- the reference ships no mesh, so this is its generator.
+
+value   device throughput: W untimed warm-up iterations build the plans, then
+        one iteration is captured as a CUDA graph (op2b_capture_*) and K
+        launches are timed with CUDA events on the library stream; L2 is
+        flushed (512 MiB memset, untimed) before every step.
+e2e     a complete solve through the C API (libop2b200_apps.so ->
+        op_decl_* from host arrays, 1000 iterations with the rms returned to
+        the host after every update, op_fetch_data of q), wall-clock timed.
+roofline  res_calc: algorithmic bytes per launch (every map and dataset
+        entry it touches once, res read and written) over its average
+        launch time inside the timed graph launches.
+cpu_baseline / --impl reference  the reference's own OpenMP build
+        (oracle/_ref/airfoil_op_f32, compiled from its sources) on this
+        host's cores, timed by its own op_timing_output.
+With N > 1 (torchrun), every rank runs an independent replica (the path
+does not shard: "replicas only") and value = N*K iterations / max rank time.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "720k-cell airfoil iters/s"
+UNIT = "iters/s"
+I_MESH, J_MESH = 400, 600
+FLUSH_BYTES = 512 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--strategy", default="gather", choices=["gather", "coloured"])
+    ap.add_argument("--fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-iters", type=int, default=1000)
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------- plumbing ----
+
+class Dist:
+    """One process per GPU under torchrun; torch.distributed only for the
+    barrier and the max over ranks."""
+
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.dist = None
+        if self.world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            self.torch, self.dist = torch, dist
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def max(self, v):
+        if not self.dist:
+            return v
+        t = self.torch.tensor([float(v)], device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+def cudart():
+    for name in ("libcudart.so.12", "libcudart.so"):
+        try:
+            lib = C.CDLL(name)
+            break
+        except OSError:
+            continue
+    lib.cudaEventElapsedTime.argtypes = [C.POINTER(C.c_float), C.c_void_p, C.c_void_p]
+    lib.cudaEventRecord.argtypes = [C.c_void_p, C.c_void_p]
+    lib.cudaMemsetAsync.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.c_void_p]
+    lib.cudaStreamSynchronize.argtypes = [C.c_void_p]
+    lib.cudaMalloc.argtypes = [C.POINTER(C.c_void_p), C.c_size_t]
+    lib.cudaFree.argtypes = [C.c_void_p]
+    lib.cudaEventCreate.argtypes = [C.POINTER(C.c_void_p)]
+    lib.cudaMallocHost.argtypes = [C.POINTER(C.c_void_p), C.c_size_t]
+    lib.cudaFreeHost.argtypes = [C.c_void_p]
+    return lib
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False,
+                                               dir=ROOT if os.access(ROOT, os.W_OK) else None)
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        self.index = vis.split(",")[device] if vis and vis.split(",")[device].isdigit() else str(device)
+        if shutil.which("nvidia-smi"):
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.index, "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        self.out.flush()
+        rows = [l.split(", ") for l in open(self.out.name).read().strip().splitlines() if l.strip()]
+        os.unlink(self.out.name)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, mx, reasons = [], None, set()
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip() == "Active":
+                        reasons.add(nm)
+            except (IndexError, ValueError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        v = json.load(open(p))["hbm_gbs"]
+        return float(v), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """dram bytes per res_calc launch from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "res_calc_airfoil_720k.md")
+    try:
+        m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+def res_calc_bytes(m, s=4):
+    """Algorithmic bytes of one res_calc call: pedge + pecell (16 B / edge),
+    x of every node, q and adt of every cell read once, res read and written."""
+    return 16.0 * m.nedge + 2 * s * m.nnode + 4 * s * m.ncell + s * m.ncell + 8 * s * m.ncell
+
+
+def iteration_bytes(m, s=4):
+    save = 8 * s * m.ncell
+    adt = 16 * m.ncell + 2 * s * m.nnode + 4 * s * m.ncell + s * m.ncell
+    res = res_calc_bytes(m, s)
+    bres = 16 * m.nbedge + (2 * s + 4 * s + s + 8 * s) * m.nbedge
+    update = 17 * s * m.ncell
+    return save + 2 * (adt + res + bres + update)
+
+
+# ------------------------------------------------------------ reference ----
+
+def run_reference_openmp(mesh, niter, fp64=False, threads=None):
+    """The reference's OpenMP airfoil (oracle/_ref/airfoil_op_f32) on this
+    host; returns (iters/s from its own op_timing_output, seconds, cores)."""
+    binary = os.path.join(ROOT, "oracle", "_ref", "airfoil_op_f64" if fp64 else "airfoil_op_f32")
+    if not os.path.exists(binary):
+        return None
+    from oplus2_matlab_b200 import mesh as M
+    d = tempfile.mkdtemp(dir=os.path.join(ROOT, "oracle", "_ref"))
+    try:
+        M.write_grid(mesh, os.path.join(d, "new_grid.dat"))
+        cores = threads or os.cpu_count()
+        env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_PROC_BIND="close",
+                   OP2REF_NITER=str(niter), OP2REF_PRINT=str(max(niter, 1)))
+        r = subprocess.run([binary], cwd=d, env=env, capture_output=True, text=True, timeout=1800)
+        if r.returncode != 0:
+            return None
+        tot = 0.0
+        for line in r.stdout.splitlines():
+            f = line.split()
+            if len(f) >= 4 and f[0].isdigit() and f[-1] in ("save_soln", "adt_calc", "res_calc",
+                                                          "bres_calc", "update"):
+                tot += float(f[1])
+        return (niter / tot if tot > 0 else None), tot, cores
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def impl_reference(args, dist):
+    """--impl reference: rank 0 times the reference's OpenMP airfoil; other
+    ranks exit without work."""
+    if dist.rank != 0:
+        return
+    from oplus2_matlab_b200 import mesh as M
+    mesh = M.naca0012(I_MESH, J_MESH)
+    niter = max(1, args.steps + args.warmup)
+    res = run_reference_openmp(mesh, niter, fp64=args.fp64)
+    base = {"impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup}
+    if res is None or res[0] is None:
+        print(json.dumps(dict(base, unavailable="reference OpenMP build oracle/_ref/airfoil_op_f32 missing or failed")))
+        return
+    v, secs, cores = res
+    line = dict(base, value=v, ms_per_step=1e3 / v, scaling="weak", vs_baseline=None,
+                dtype="f64" if args.fp64 else "f32", data="synthetic",
+                config={"workload": "airfoil NACA0012 C-mesh 1200x600 cells (720,000), %s, "
+                                    "reference OpenMP airfoil_op on host cores" % ("FP64" if args.fp64 else "FP32"),
+                        "cells": mesh.ncell, "edges": mesh.nedge, "iterations": niter},
+                cpu_baseline={"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                              "sample": "%d iterations of the 720k mesh, sum of op_timing_output" % niter},
+                e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------ ours ----
+
+def impl_ours(args, dist):
+    from oplus2_matlab_b200 import api, apps
+    from oplus2_matlab_b200 import mesh as M
+    lib = api.lib()
+    cr = cudart()
+    dt = np.float64 if args.fp64 else np.float32
+    s = 8 if args.fp64 else 4
+
+    mesh = M.naca0012(I_MESH, J_MESH)
+    api.set_error_mode(api.ERRORS_RETURN)
+    api.op_init([], 0)
+    api.set_strategy(api.STRATEGY_GATHER if args.strategy == "gather" else api.STRATEGY_COLOURED)
+    api.set_reduction(api.REDUCE_TREE)
+    A = apps.Airfoil(mesh, dt)
+    stream = lib.op2b_get_stream()
+
+    # warm-up: builds the plans, uploads the maps
+    for _ in range(max(3, args.warmup)):
+        A.iteration()
+    api.sync()
+    assert api.last_error() == "", api.last_error()
+
+    # one outer iteration as a profiled CUDA graph (event nodes around loops)
+    rms_dev = A.rms
+    assert lib.op2b_capture_begin(1) == 1, api.last_error()
+    A.loop("save_soln")
+    for _ in range(2):
+        A.loop("adt_calc")
+        A.loop("res_calc")
+        A.loop("bres_calc")
+        rms_dev[0] = 0
+        A.loop("update")
+    g = lib.op2b_capture_end()
+    assert g, api.last_error()
+    nloops = lib.op2b_graph_nloops(g)
+    nkern = lib.op2b_graph_nkernels(g)
+    names = [lib.op2b_graph_loop_name(g, i).decode() for i in range(nloops)]
+
+    flush = C.c_void_p()
+    assert cr.cudaMalloc(C.byref(flush), FLUSH_BYTES) == 0
+    ev = []
+    for _ in range(2 * args.steps):
+        e = C.c_void_p()
+        cr.cudaEventCreate(C.byref(e))
+        ev.append(e)
+    lt = (C.c_double * nloops)()
+    loop_tot = {n: 0.0 for n in names}
+    loop_cnt = {n: 0 for n in names}
+
+    clocks = Clocks(dist.local)
+    dist.barrier()
+    cr.cudaStreamSynchronize(stream)
+    step_ms = []
+    for k in range(args.steps):
+        cr.cudaMemsetAsync(flush, k & 0xFF, FLUSH_BYTES, stream)   # L2 flush, untimed
+        cr.cudaEventRecord(ev[2 * k], stream)
+        rc = lib.op2b_graph_launch(g)
+        cr.cudaEventRecord(ev[2 * k + 1], stream)
+        assert rc == 0, rc
+        cr.cudaStreamSynchronize(stream)
+        got = lib.op2b_graph_loop_times(g, lt, nloops)
+        for i in range(got):
+            loop_tot[names[i]] += lt[i]
+            loop_cnt[names[i]] += 1
+    cr.cudaStreamSynchronize(stream)
+    dist.barrier()
+    clk = clocks.stop()
+    for k in range(args.steps):
+        ms = C.c_float()
+        cr.cudaEventElapsedTime(C.byref(ms), ev[2 * k], ev[2 * k + 1])
+        step_ms.append(ms.value)
+    total_s = dist.max(sum(step_ms) * 1e-3)
+    api.sync()  # delivers the last launch's rms
+    rms_last = float(np.sqrt(A.rms[0] / dt(mesh.ncell)))
+    value = dist.world * args.steps / total_s
+
+    res_launch_s = loop_tot["res_calc"] / max(1, loop_cnt["res_calc"])
+    algo = res_calc_bytes(mesh, s)
+    peak, peak_kind = measured_peak()
+    achieved = algo / res_launch_s / 1e9
+    per_loop_us = {n: 1e6 * loop_tot[n] / max(1, loop_cnt[n]) for n in names}
+    iter_bytes = iteration_bytes(mesh, s)
+
+    lib.op2b_graph_destroy(g)
+    cr.cudaFree(flush)
+    st = A.fetch()
+    ok = bool(np.isfinite(st["q"]).all()) and np.isfinite(rms_last) and rms_last > 0
+    api.op_exit()
+
+    # end to end: a whole solve through the C API from host arrays
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(mesh, args.fp64, args.e2e_iters, args.strategy, dist)
+
+    cpu = None
+    if not args.no_cpu_baseline and dist.rank == 0 and dist.world == 1:
+        cpu = cpu_baseline(mesh, args.fp64)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.fp64 else "f32",
+        "data": "synthetic: NACA0012 C-mesh from the reference's generator, free-stream start",
+        "config": {"workload": "airfoil 720k cells (I=400, J=600: 720,000 cells, 1,438,600 edges, "
+                               "721,801 nodes, 2,800 bedges), one outer iteration per step",
+                   "cells": mesh.ncell, "edges": mesh.nedge, "strategy": args.strategy,
+                   "reduction": "tree", "l2": "flushed before every step (512 MiB memset, untimed)",
+                   "timing": "CUDA events around each graph launch on the library stream",
+                   "parallelism": "replicas" if dist.world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "kernel": "res_calc", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": ncu_traffic(),
+                     "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": algo, "avg_launch_us": res_launch_s * 1e6},
+        "iteration_roofline": {"algorithmic_bytes": iter_bytes,
+                               "achieved_gbs": iter_bytes * value / dist.world / 1e9,
+                               "frac": iter_bytes * value / dist.world / 1e9 / peak},
+        "per_loop_us": per_loop_us,
+        "gpu_launches": nkern * args.steps,
+        "kernels_per_step": nkern,
+        "rms_last": rms_last, "finite": ok,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    }
+    if dist.rank == 0:
+        print(json.dumps(line))
+
+
+class AppTiming(C.Structure):
+    _fields_ = [("t_declare", C.c_double), ("t_iterate", C.c_double), ("t_fetch", C.c_double),
+                ("t_total", C.c_double), ("h2d_bytes", C.c_longlong), ("d2h_bytes", C.c_longlong)]
+
+
+def run_e2e(mesh, fp64, niter, strategy, dist):
+    """A complete solve through the C API (oplus2_matlab_b200/apps/airfoil_app.cpp):
+    declarations from pinned host arrays, niter iterations with the rms read
+    back after every update, q fetched to the host.  Wall-clock timed."""
+    from oplus2_matlab_b200 import _lib
+    from oplus2_matlab_b200 import api
+    cr = cudart()
+    lib = _lib.load()
+    app = C.CDLL(os.path.join(ROOT, "oplus2_matlab_b200", "lib", "libop2b200_apps.so"))
+    app.op2b_airfoil_app.argtypes = [C.POINTER(_lib.op2b_mesh), C.c_int, C.c_int, C.c_void_p,
+                                     C.c_void_p, C.c_int, C.POINTER(AppTiming)]
+    dt = np.float64 if fp64 else np.float32
+    # pinned host copies of every input
+    keep = []
+
+    def pinned(a):
+        a = np.ascontiguousarray(a)
+        p = C.c_void_p()
+        assert cr.cudaMallocHost(C.byref(p), max(1, a.nbytes)) == 0
+        buf = np.frombuffer((C.c_char * a.nbytes).from_address(p.value), dtype=a.dtype).reshape(a.shape)
+        buf[...] = a
+        keep.append(p)
+        return buf
+
+    m = _lib.op2b_mesh()
+    arrs = {k: pinned(getattr(mesh, k)) for k in ("cell", "edge", "ecell", "bedge", "becell", "bound",
+                                                  "x64", "x32")}
+    m.nnode, m.ncell, m.nedge, m.nbedge = mesh.nnode, mesh.ncell, mesh.nedge, mesh.nbedge
+    for k in ("cell", "edge", "ecell", "bedge", "becell", "bound"):
+        setattr(m, k, arrs[k].ctypes.data_as(C.POINTER(C.c_int)))
+    m.x64 = arrs["x64"].ctypes.data_as(C.POINTER(C.c_double))
+    m.x32 = arrs["x32"].ctypes.data_as(C.POINTER(C.c_float))
+    from oplus2_matlab_b200.apps import airfoil_consts
+    qinf = np.asarray(airfoil_consts(dt)["qinf"], dt)
+    q = pinned(np.tile(qinf, (mesh.ncell, 1)))
+    rms = np.zeros(niter, np.float64)
+    t = AppTiming()
+    api.set_error_mode(api.ERRORS_RETURN)
+    dist.barrier()
+    rc = app.op2b_airfoil_app(C.byref(m), 1 if fp64 else 0, niter, q.ctypes.data,
+                              rms.ctypes.data, 1 if strategy == "gather" else 2, C.byref(t))
+    total = dist.max(t.t_total)
+    for p in keep:
+        cr.cudaFreeHost(p)
+    if rc != 0:
+        return None
+    return {"value": dist.world * niter / total, "unit": UNIT,
+            "h2d_bytes_per_step": t.h2d_bytes / niter, "d2h_bytes_per_step": t.d2h_bytes / niter,
+            "iterations": niter, "seconds": total,
+            "phases_s": {"declare_h2d": t.t_declare, "iterate": t.t_iterate, "fetch_d2h": t.t_fetch},
+            "rms_final": float(rms[-1]),
+            "path": "C API (libop2b200_apps.so: op_decl_* from pinned host arrays, op_par_loop_* "
+                    "with rms to the host every update, op_fetch_data)"}
+
+
+def cpu_baseline(mesh, fp64):
+    """The reference OpenMP build on a bounded sample (about 10-30 s)."""
+    probe = run_reference_openmp(mesh, 3, fp64=fp64)
+    if probe is None or probe[0] is None:
+        return None
+    rate = probe[0]
+    niter = int(min(400, max(5, 15.0 * rate)))
+    res = run_reference_openmp(mesh, niter, fp64=fp64)
+    if res is None or res[0] is None:
+        return None
+    return {"value": res[0], "unit": UNIT, "cores": res[2], "kind": "reference",
+            "sample": "%d iterations of the 720k mesh (reference airfoil_op, OpenMP, "
+                      "sum of its op_timing_output)" % niter}
+
+
+def main():
+    args = parse()
+    dist = Dist()
+    try:
+        if args.impl == "reference":
+            impl_reference(args, dist)
+        else:
+            impl_ours(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -66,6 +66,25 @@ double op2b_loop_time(char const *name, int *count);
 /* Turn per-loop event timing on (default) or off; returns the old value. */
 int    op2b_set_timing(int on);
 
+/* CUDA graphs.  op2b_capture_begin() starts capturing the library stream;
+ * the op_par_loop calls that follow are recorded, not run, with their global
+ * reductions deferred; op2b_capture_end() instantiates them as one graph.
+ * Plans must already exist (run the loops once before capturing).  Each
+ * op2b_graph_launch() re-arms the graph's reductions: the results of the
+ * latest launch reach the host variables at the next op2b_sync().  With
+ * profile != 0 each loop is bracketed by event nodes so that
+ * op2b_graph_loop_times() reports per-loop device time of the most recent
+ * launch.  Handles are opaque; 0 / NULL means failure. */
+int   op2b_capture_begin(int profile);
+void *op2b_capture_end(void);
+int   op2b_graph_launch(void *graph);
+int   op2b_graph_nloops(void *graph);
+int   op2b_graph_nkernels(void *graph);
+char const *op2b_graph_loop_name(void *graph, int i);
+/* seconds of each recorded loop in the last launch (waits for it) */
+int   op2b_graph_loop_times(void *graph, double *seconds, int n);
+void  op2b_graph_destroy(void *graph);
+
 /* Plan validation on the device: the reference's op_plan_check plus the
  * colouring checks it lacks.  Returns the number of violations found. */
 long op2b_plan_validate(char const *name, op_set set, int part_size, int nargs, op_arg *args,

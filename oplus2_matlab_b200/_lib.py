@@ -125,6 +125,14 @@ PROTOTYPES = [
     ("op2b_plan_validate", C.c_long,
      [C.c_char_p, op_set, C.c_int, C.c_int, C.POINTER(op_arg), C.c_int, C.POINTER(C.c_int)]),
     ("op2b_version", C.c_char_p, []),
+    ("op2b_capture_begin", C.c_int, [C.c_int]),
+    ("op2b_capture_end", _P, []),
+    ("op2b_graph_launch", C.c_int, [_P]),
+    ("op2b_graph_nloops", C.c_int, [_P]),
+    ("op2b_graph_nkernels", C.c_int, [_P]),
+    ("op2b_graph_loop_name", C.c_char_p, [_P, C.c_int]),
+    ("op2b_graph_loop_times", C.c_int, [_P, C.POINTER(C.c_double), C.c_int]),
+    ("op2b_graph_destroy", None, [_P]),
     # op2b_mesh.h
     ("op2b_mesh_naca0012", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(op2b_mesh)]),
     ("op2b_mesh_free", None, [C.POINTER(op2b_mesh)]),

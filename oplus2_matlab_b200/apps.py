@@ -44,7 +44,7 @@ def airfoil_consts(dtype):
 class Airfoil:
     """airfoil_op.cpp with the library: declare, then iterate()."""
 
-    def __init__(self, mesh, dtype=np.float32, consts=None, q0=None):
+    def __init__(self, mesh, dtype=np.float32, consts=None, q0=None, state=None):
         self.dtype = t = np.dtype(dtype)
         tn = "float" if t == np.float32 else "double"
         self.tn = tn
@@ -57,6 +57,9 @@ class Airfoil:
         self.qold = np.zeros((nc, 4), t)
         self.res = np.zeros((nc, 4), t)
         self.adt = np.zeros((nc, 1), t)
+        if state is not None:  # start from a given flow state instead
+            for k in ("q", "qold", "res", "adt"):
+                getattr(self, k)[...] = np.asarray(state[k], t).reshape(getattr(self, k).shape)
         self.x = np.ascontiguousarray(mesh.x(t))
         self.bound = np.ascontiguousarray(mesh.bound.reshape(-1, 1))
 

@@ -20,6 +20,8 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libop2b200.so")
+APPS = os.path.join(HERE, "apps")
+APPS_LIB = os.path.join(LIBDIR, "libop2b200_apps.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
@@ -75,6 +77,17 @@ def build(force=False, verbose=True):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (" ".join(cmd), r.stderr))
+    # the apps (C++ over the public C API only) link against the library
+    app_srcs = sorted(os.path.join(APPS, f) for f in os.listdir(APPS) if f.endswith(".cpp"))
+    newest_app = max([os.path.getmtime(s) for s in app_srcs] + [os.path.getmtime(LIB)] +
+                     [os.path.getmtime(h) for h in headers()])
+    if force or not os.path.exists(APPS_LIB) or os.path.getmtime(APPS_LIB) < newest_app:
+        cmd = [nvcc(), "-O2", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared",
+               "-I" + os.path.join(ROOT, "include"), "-o", APPS_LIB] + app_srcs + \
+              ["-L" + LIBDIR, "-lop2b200", "-lcudart", "-Xlinker", "-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("apps build failed:\n%s\n%s" % (" ".join(cmd), r.stderr))
     return LIB
 
 

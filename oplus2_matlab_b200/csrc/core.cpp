@@ -136,7 +136,7 @@ op_set op_decl_set(int size, char const *name) {
   return set;
 }
 
-// common/op_lib_core.c:121-169, plus the device copy of the map
+// common/op_lib_core.c:121-169
 op_map op_decl_map(op_set from, op_set to, int dim, int *imap, char const *name) {
   if (from == nullptr) {
     fail(-1, " op_decl_map error -- invalid 'from' set for map %s\n", name);
@@ -173,15 +173,8 @@ op_map op_decl_map(op_set from, op_set to, int dim, int *imap, char const *name)
   map->map = imap;
   map->name = name;
   OP_map_list[OP_map_index++] = map;
-
-  Runtime &R = rt();
-  ensure_cuda();
-  if (R.maps.size() <= (size_t)map->index) R.maps.resize(map->index + 1);
-  size_t bytes = sizeof(int) * (size_t)dim * from->size;
-  R.maps[map->index].d = (int *)dev_alloc(bytes);
-  if (R.maps[map->index].d)
-    OP2B_CUDA(cudaMemcpyAsync(R.maps[map->index].d, imap, bytes, cudaMemcpyHostToDevice,
-                              R.stream));
+  // the device copy is made on first use by a loop (map_dev), so declaring
+  // maps needs no GPU, as in the reference
   return map;
 }
 

@@ -53,6 +53,23 @@ void dev_free(void *p) {
   if (p) cudaFree(p);
 }
 
+const int *map_dev(op_map m) {
+  Runtime &R = rt();
+  if (!m) return nullptr;
+  if (R.maps.size() <= (size_t)m->index) R.maps.resize(m->index + 1);
+  MapDev &md = R.maps[m->index];
+  if (!md.d) {
+    ensure_cuda();
+    size_t bytes = sizeof(int) * (size_t)m->dim * m->from->size;
+    md.d = (int *)dev_alloc(bytes);
+    if (md.d) {
+      OP2B_CUDA(cudaMemcpyAsync(md.d, m->map, bytes, cudaMemcpyHostToDevice, R.stream));
+      OP2B_CUDA(cudaStreamSynchronize(R.stream));
+    }
+  }
+  return md.d;
+}
+
 static bool capturing() {
   cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
   if (rt().stream) cudaStreamIsCapturing(rt().stream, &st);
@@ -74,7 +91,19 @@ LoopScope::LoopScope(char const *name, double transfer, double transfer2) {
   k.count += 1;
   k.transfer += (float)transfer;
   k.transfer2 += (float)transfer2;
-  if (!R.timing || capturing()) return;
+  if (capturing()) {
+    // inside a graph capture: bracket the loop with event nodes of its own
+    // (profiled graphs), or record nothing
+    if (!R.capture_profile) return;
+    OP2B_CUDA(cudaEventCreate(&ev.first));
+    OP2B_CUDA(cudaEventCreate(&ev.second));
+    // "external" records become event-record nodes of the graph (a plain
+    // record inside a capture only expresses a dependency)
+    OP2B_CUDA(cudaEventRecordWithFlags(ev.first, R.stream, cudaEventRecordExternal));
+    captured = true;
+    return;
+  }
+  if (!R.timing) return;
   if (T.pending.size() > 512) flush_timers();
   if (T.free_pairs.empty()) {
     cudaEvent_t a, b;
@@ -89,8 +118,10 @@ LoopScope::LoopScope(char const *name, double transfer, double transfer2) {
 
 LoopScope::~LoopScope() {
   if (!ev.first) return;
-  cudaEventRecord(ev.second, rt().stream);
-  t->pending.push_back(ev);
+  if (captured) cudaEventRecordWithFlags(ev.second, rt().stream, cudaEventRecordExternal);
+  else cudaEventRecord(ev.second, rt().stream);
+  if (captured) rt().capture_events.push_back({t->name, ev.first, ev.second});
+  else t->pending.push_back(ev);
 }
 
 void flush_timers() {

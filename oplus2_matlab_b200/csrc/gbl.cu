@@ -7,6 +7,8 @@
 // when the loop call returns.  In deferred mode the device results wait in
 // slots until op2b_sync / op_fetch_data, so no call blocks.
 
+#include <algorithm>
+
 #include "loops.h"
 
 namespace op2b {
@@ -17,6 +19,7 @@ struct RedState {
   char *dev = nullptr;  // [2 x kMaxRedBlocks x 8] partials | ticket (256 B) | slots
   char *host = nullptr; // pinned mirror of the slots
   int next_slot = 0;
+  int graph_slots = 0;  // slots baked into captured graphs stay reserved
   void *seq = nullptr;
   size_t seq_bytes = 0;
 };
@@ -90,8 +93,12 @@ int red_new_slot() {
   ensure_red();
   RedState &S = rs();
   if (S.next_slot >= kSlots) {
-    deliver_deferred();  // frees every slot
-    S.next_slot = 0;
+    deliver_deferred();  // frees every slot not held by a captured graph
+    S.next_slot = S.graph_slots ? S.graph_slots : 0;
+    if (S.next_slot >= kSlots) {
+      fail(-1, "op2b error: global reduction slots exhausted by captured graphs\n");
+      S.next_slot = 0;
+    }
   }
   return S.next_slot++;
 }
@@ -122,7 +129,31 @@ void red_finish(const std::vector<GblRequest> &reqs) {
     return;
   }
   deliver(reqs);
-  if (pending().empty()) rs().next_slot = 0;
+  if (pending().empty() && rs().graph_slots == 0) rs().next_slot = 0;
+}
+
+size_t red_pending_count() { return pending().size(); }
+
+std::vector<GblRequest> red_take_pending_since(size_t mark) {
+  std::vector<GblRequest> &p = pending();
+  std::vector<GblRequest> out;
+  if (mark < p.size()) {
+    out.assign(p.begin() + mark, p.end());
+    p.resize(mark);
+  }
+  return out;
+}
+
+void red_replace_pending(const std::vector<GblRequest> &reqs) {
+  std::vector<GblRequest> &p = pending();
+  std::vector<GblRequest> keep;
+  for (auto &r : p) {
+    bool same = false;
+    for (auto &q : reqs) same = same || (q.slot == r.slot);
+    if (!same) keep.push_back(r);
+  }
+  keep.insert(keep.end(), reqs.begin(), reqs.end());
+  p.swap(keep);
 }
 
 void deliver_deferred() {
@@ -130,8 +161,10 @@ void deliver_deferred() {
   std::vector<GblRequest> v;
   v.swap(pending());
   deliver(v);
-  rs().next_slot = 0;
+  if (rs().graph_slots == 0) rs().next_slot = 0;
 }
+
+void red_reserve_for_graph() { rs().graph_slots = std::max(rs().graph_slots, rs().next_slot); }
 
 }  // namespace op2b
 

@@ -1,0 +1,133 @@
+// graph.cu -- capture a sequence of op_par_loop calls as one CUDA graph.
+//
+// The reference launches every loop from the host and synchronises after
+// each block colour and each reduction (airfoil/res_calc_kernel.cu:230,
+// update_kernel.cu:162-165): about 15 host round trips per airfoil
+// iteration.  Captured, a whole outer iteration (save_soln + 2 x (adt_calc,
+// res_calc, bres_calc, update)) becomes one graph launch; reductions stay on
+// the device in their result slots (deferred mode) until op2b_sync().
+
+#include <string>
+#include <vector>
+
+#include "loops.h"
+
+namespace op2b {
+
+struct Graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int nkernels = 0;
+  std::vector<Runtime::CapturedLoop> loops;
+  std::vector<GblRequest> reductions;  // deferred results each launch refreshes
+};
+
+static bool g_prev_deferred = false;
+
+}  // namespace op2b
+
+using namespace op2b;
+
+extern "C" {
+
+static size_t g_pending_mark = 0;
+
+int op2b_capture_begin(int profile) {
+  ensure_cuda();
+  if (error_pending()) return 0;
+  Runtime &R = rt();
+  deliver_deferred();
+  g_pending_mark = red_pending_count();
+  R.capture_events.clear();
+  R.capture_profile = profile != 0;
+  g_prev_deferred = R.gbl_deferred;
+  R.gbl_deferred = true;
+  cudaError_t e = cudaStreamBeginCapture(R.stream, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) {
+    R.gbl_deferred = g_prev_deferred;
+    R.capture_profile = false;
+    fail(-1, "op2b error: cannot start graph capture: %s\n", cudaGetErrorString(e));
+    return 0;
+  }
+  return 1;
+}
+
+void *op2b_capture_end(void) {
+  Runtime &R = rt();
+  Graph *g = new Graph();
+  cudaError_t e = cudaStreamEndCapture(R.stream, &g->graph);
+  R.capture_profile = false;
+  R.gbl_deferred = g_prev_deferred;
+  g->reductions = red_take_pending_since(g_pending_mark);
+  red_reserve_for_graph();
+  if (e != cudaSuccess) {
+    delete g;
+    fail(-1, "op2b error: graph capture failed: %s\n", cudaGetErrorString(e));
+    return nullptr;
+  }
+  g->loops.swap(R.capture_events);
+  size_t n = 0;
+  OP2B_CUDA(cudaGraphGetNodes(g->graph, nullptr, &n));
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (n) OP2B_CUDA(cudaGraphGetNodes(g->graph, nodes.data(), &n));
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    OP2B_CUDA(cudaGraphNodeGetType(nd, &t));
+    g->nkernels += (t == cudaGraphNodeTypeKernel);
+  }
+  e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g->graph);
+    delete g;
+    fail(-1, "op2b error: graph instantiation failed: %s\n", cudaGetErrorString(e));
+    return nullptr;
+  }
+  return g;
+}
+
+int op2b_graph_launch(void *h) {
+  Graph *g = (Graph *)h;
+  if (!g) return (int)cudaErrorInvalidValue;
+  red_replace_pending(g->reductions);
+  return (int)cudaGraphLaunch(g->exec, rt().stream);
+}
+
+int op2b_graph_nloops(void *h) { return h ? (int)((Graph *)h)->loops.size() : -1; }
+
+int op2b_graph_nkernels(void *h) { return h ? ((Graph *)h)->nkernels : -1; }
+
+char const *op2b_graph_loop_name(void *h, int i) {
+  Graph *g = (Graph *)h;
+  if (!g || i < 0 || i >= (int)g->loops.size()) return "";
+  return g->loops[i].name.c_str();
+}
+
+int op2b_graph_loop_times(void *h, double *seconds, int n) {
+  Graph *g = (Graph *)h;
+  if (!g) return -1;
+  int k = 0;
+  for (auto &l : g->loops) {
+    if (k >= n) break;
+    float ms = 0.f;
+    cudaError_t e = cudaEventSynchronize(l.stop);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, l.start, l.stop);
+    if (e != cudaSuccess) return -(int)e;
+    seconds[k++] = ms * 1e-3;
+  }
+  return k;
+}
+
+void op2b_graph_destroy(void *h) {
+  Graph *g = (Graph *)h;
+  if (!g) return;
+  cudaStreamSynchronize(rt().stream);
+  for (auto &l : g->loops) {
+    cudaEventDestroy(l.start);
+    cudaEventDestroy(l.stop);
+  }
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
+}
+
+}  // extern "C"

@@ -73,6 +73,15 @@ struct Runtime {
 
   std::map<std::string, LoopTimer> timers;
 
+  // stream capture in progress (graph.cu): per-loop event pairs recorded
+  // into the graph when profiling
+  bool capture_profile = false;
+  struct CapturedLoop {
+    std::string name;
+    cudaEvent_t start, stop;
+  };
+  std::vector<CapturedLoop> capture_events;
+
   // device scratch for global reductions: partials + final slots
   void *red_scratch = nullptr;
   size_t red_scratch_bytes = 0;
@@ -92,6 +101,9 @@ struct Runtime {
 
 Runtime &rt();
 
+// device copy of a map, uploaded on first use
+const int *map_dev(op_map m);
+
 // device memory helpers (long-lived allocations)
 void *dev_alloc(size_t bytes);
 void dev_free(void *p);
@@ -101,6 +113,7 @@ void ensure_cuda();  // op_init's device part, also run lazily
 struct LoopScope {
   LoopTimer *t = nullptr;
   std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+  bool captured = false;
   LoopScope(char const *name, double transfer, double transfer2);
   ~LoopScope();
 };

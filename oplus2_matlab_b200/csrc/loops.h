@@ -18,7 +18,7 @@ struct IdxMap {
 inline IdxMap idx_map(const op_arg &a) {
   IdxMap m{nullptr, 0, 0};
   if (a.map) {
-    m.map = rt().maps[a.map->index].d;
+    m.map = map_dev(a.map);
     m.dim = a.map->dim;
     m.idx = a.idx;
   }
@@ -48,6 +48,13 @@ void *red_slot_ptr(int slot);    // 8-byte device slot
 int red_new_slot();
 void *red_seq_buffer(size_t bytes);  // scratch for SEQ-mode contributions
 void red_finish(const std::vector<GblRequest> &reqs);
+// deferred requests (graph capture): count, take those added since a mark,
+// and re-arm a set (replacing any pending request on the same slots)
+size_t red_pending_count();
+std::vector<GblRequest> red_take_pending_since(size_t mark);
+void red_replace_pending(const std::vector<GblRequest> &reqs);
+// keep every slot handed out so far out of reuse (they are baked into a graph)
+void red_reserve_for_graph();
 int red_grid(long long n, int threads);  // fixed grid for a set size
 
 // loop implementations (airfoil.cu, jac.cu)

@@ -511,7 +511,7 @@ static bool fill_params(PlanParams &pp, const DevPlan &p, std::vector<int> &to_s
   for (int a = 0; a < p.nargs; a++) {
     pp.arg_ind[a] = p.inds[a];
     if (p.maps[a]) {
-      pp.am.map[a] = rt().maps[p.maps[a]->index].d;
+      pp.am.map[a] = map_dev(p.maps[a]);
       pp.am.dim[a] = p.maps[a]->dim;
       pp.am.idx[a] = p.idxs[a];
     }
@@ -1068,7 +1068,7 @@ GatherPlan *get_gather_plan(op_set set, const op_arg *args, const std::vector<in
     const op_arg &a = args[slots[k]];
     g.maps.push_back(a.map);
     g.idxs.push_back(a.idx);
-    sm.map[k] = R.maps[a.map->index].d;
+    sm.map[k] = map_dev(a.map);
     sm.dim[k] = a.map->dim;
     sm.idx[k] = a.idx;
   }
