@@ -34,6 +34,16 @@ enum { OP2B_STRATEGY_AUTO = 0, OP2B_STRATEGY_GATHER = 1, OP2B_STRATEGY_COLOURED 
  *         bit-identical to the reference, at the cost of a serial pass. */
 enum { OP2B_REDUCE_TREE = 0, OP2B_REDUCE_SEQ = 1 };
 
+/* Kernel-variant knobs, used by the tuner and by experiments; returns the
+ * previous value or -1.  Keys:
+ *   "gather_tiled"  0: one thread per incremented element, contributions
+ *                   loaded in batches (default); 1: one thread per
+ *                   contribution in CTA tiles, folded in shared memory
+ *   "gather_batch"  contributions whose loads are issued together per
+ *                   thread in the per-element GATHER kernel (1, 2, 4)
+ *   "unroll"        elements per thread in the direct loops (1, 2, 4) */
+int op2b_set_tuning(const char *key, int value);
+
 /* Errors: EXIT (default, like the reference: print and exit) or RETURN
  * (print, remember the message, return NULL / do nothing). */
 enum { OP2B_ERRORS_EXIT = 0, OP2B_ERRORS_RETURN = 1 };
@@ -89,6 +99,10 @@ void  op2b_graph_destroy(void *graph);
  * colouring checks it lacks.  Returns the number of violations found. */
 long op2b_plan_validate(char const *name, op_set set, int part_size, int nargs, op_arg *args,
                         int ninds, int *inds);
+
+/* Evict L2 on the library stream by reading (not writing) a buffer three
+ * times its size; benchmark drivers call it between timed steps. */
+int op2b_l2_flush(void);
 
 /* Library build string (arch, flags). */
 char const *op2b_version(void);

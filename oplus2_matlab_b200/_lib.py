@@ -125,6 +125,8 @@ PROTOTYPES = [
     ("op2b_plan_validate", C.c_long,
      [C.c_char_p, op_set, C.c_int, C.c_int, C.POINTER(op_arg), C.c_int, C.POINTER(C.c_int)]),
     ("op2b_version", C.c_char_p, []),
+    ("op2b_l2_flush", C.c_int, []),
+    ("op2b_set_tuning", C.c_int, [C.c_char_p, C.c_int]),
     ("op2b_capture_begin", C.c_int, [C.c_int]),
     ("op2b_capture_end", _P, []),
     ("op2b_graph_launch", C.c_int, [_P]),

@@ -144,35 +144,131 @@ __device__ __forceinline__ void bres_apply(const T x1[2], const T x2[2], const T
 
 // ------------------------------------------------------------- kernels ----
 
-// save_soln: qold = q, one element per thread, 16-byte vectors
-template <class T>
-__global__ void k_save_soln(int n, const T *__restrict__ q, T *__restrict__ qold) {
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-    T v[4];
-    ld4(q + 4 * (size_t)c, v);
-    st4(qold + 4 * (size_t)c, v);
+// Two map entries of one element.  When both args use one map of dim 2 with
+// idx 0 and 1 (pedge, pecell, pbedge) this is a single 8-byte load.
+__device__ __forceinline__ void at2(const IdxMap &a, const IdxMap &b, int e, int &i, int &j) {
+  if (a.map && a.map == b.map && a.dim == 2 && a.idx == 0 && b.idx == 1) {
+    int2 v = __ldg(reinterpret_cast<const int2 *>(a.map) + e);
+    i = v.x;
+    j = v.y;
+  } else {
+    i = at(a, e);
+    j = at(b, e);
   }
 }
 
-// adt_calc: direct over cells, x gathered through pcell
+// save_soln: qold = q, U elements per thread issued before any store
+template <class T, int U>
+__global__ void k_save_soln(int n, const T *__restrict__ q, T *__restrict__ qold) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x + threadIdx.x; base < n; base += stride * U) {
+    T v[U][4];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      int c = base + u * stride;
+      if (c < n) ld4(q + 4 * (size_t)c, v[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      int c = base + u * stride;
+      if (c < n) st4(qold + 4 * (size_t)c, v[u]);
+    }
+  }
+}
+
+// adt_calc: direct over cells, x gathered through pcell (one 16-byte load
+// of the 4 node indices when the four args share a dim-4 map in order)
 template <class T>
 __global__ void k_adt_calc(int n, IdxMap m0, IdxMap m1, IdxMap m2, IdxMap m3, IdxMap mq,
                            const T *__restrict__ x0, const T *__restrict__ x1,
                            const T *__restrict__ x2, const T *__restrict__ x3,
                            const T *__restrict__ q, T *__restrict__ adt, AirConsts<T> K) {
+  const bool quad = m0.map && m0.map == m1.map && m0.map == m2.map && m0.map == m3.map &&
+                    m0.dim == 4 && m0.idx == 0 && m1.idx == 1 && m2.idx == 2 && m3.idx == 3;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    int n0, n1, n2, n3;
+    if (quad) {
+      int4 v = __ldg(reinterpret_cast<const int4 *>(m0.map) + c);
+      n0 = v.x; n1 = v.y; n2 = v.z; n3 = v.w;
+    } else {
+      n0 = at(m0, c); n1 = at(m1, c); n2 = at(m2, c); n3 = at(m3, c);
+    }
     T a[2], b[2], d[2], e[2], qq[4];
-    ld2(x0 + 2 * (size_t)at(m0, c), a);
-    ld2(x1 + 2 * (size_t)at(m1, c), b);
-    ld2(x2 + 2 * (size_t)at(m2, c), d);
-    ld2(x3 + 2 * (size_t)at(m3, c), e);
     ld4(q + 4 * (size_t)at(mq, c), qq);
+    ld2(x0 + 2 * (size_t)n0, a);
+    ld2(x1 + 2 * (size_t)n1, b);
+    ld2(x2 + 2 * (size_t)n2, d);
+    ld2(x3 + 2 * (size_t)n3, e);
     adt[c] = adt_calc(a, b, d, e, qq, K);
   }
 }
 
-// res_calc, GATHER: one thread per incremented cell
+// res_calc, GATHER, contribution-parallel: CTA b owns the cells whose first
+// contribution lies in [kTile*b, kTile*(b+1)).  Each thread computes the
+// flux of one (edge, side) contribution into shared memory (negated for the
+// second cell of the edge); then one thread per owned cell folds its
+// contributions in ascending order -- op_seq.h's order -- onto res.
+constexpr int kTileExtra = 64;  // contributions past the tile end (max row - 1)
+
 template <class T>
+__global__ void __launch_bounds__(kTile) k_res_calc_tiled(
+    const int *__restrict__ tile_first, const int *__restrict__ active,
+    const int *__restrict__ row, const int *__restrict__ keys, IdxMap mx1, IdxMap mx2,
+    IdxMap mq1, IdxMap mq2, IdxMap ma1, IdxMap ma2, const T *__restrict__ xa,
+    const T *__restrict__ xb, const T *__restrict__ qa, const T *__restrict__ qb,
+    const T *__restrict__ adta, const T *__restrict__ adtb, T *__restrict__ res, T gm1, T eps) {
+  __shared__ __align__(16) T fl[(kTile + kTileExtra) * 4];
+  const int t0 = tile_first[blockIdx.x], t1 = tile_first[blockIdx.x + 1];
+  if (t0 == t1) return;
+  const int e0 = row[t0], e1 = row[t1];
+  const int j = threadIdx.x;
+  const bool owner = j < t1 - t0;
+  int c = 0, k0 = 0, k1 = 0;
+  T r[4];
+  if (owner) {  // start the owner's reads early
+    c = active ? active[t0 + j] : t0 + j;
+    k0 = row[t0 + j];
+    k1 = row[t0 + j + 1];
+    ldw4(res + 4 * (size_t)c, r);
+  }
+  const bool same_cells = mq1.map == ma1.map && mq1.idx == ma1.idx && mq2.map == ma2.map &&
+                          mq2.idx == ma2.idx && mq1.dim == ma1.dim && mq2.dim == ma2.dim;
+  for (int i = e0 + j; i < e1; i += kTile) {
+    const int key = __ldg(keys + i);
+    const int e = key >> 1;
+    int n1, n2, c1, c2, a1, a2;
+    at2(mx1, mx2, e, n1, n2);
+    at2(mq1, mq2, e, c1, c2);
+    if (same_cells) {
+      a1 = c1;
+      a2 = c2;
+    } else {
+      at2(ma1, ma2, e, a1, a2);
+    }
+    T p[2], s[2], q1[4], q2[4], f[4];
+    ld4(qa + 4 * (size_t)c1, q1);
+    ld4(qb + 4 * (size_t)c2, q2);
+    ld2(xa + 2 * (size_t)n1, p);
+    ld2(xb + 2 * (size_t)n2, s);
+    const T ad1 = __ldg(adta + a1), ad2 = __ldg(adtb + a2);
+    res_flux(p, s, q1, q2, ad1, ad2, gm1, eps, f);
+    if (key & 1) {
+      f[0] = -f[0]; f[1] = -f[1]; f[2] = -f[2]; f[3] = -f[3];
+    }
+    st4(fl + 4 * (i - e0), f);
+  }
+  __syncthreads();
+  if (owner) {
+    for (int k = k0; k < k1; k++) {
+      const T *g = fl + 4 * (k - e0);
+      r[0] += g[0]; r[1] += g[1]; r[2] += g[2]; r[3] += g[3];
+    }
+    st4(res + 4 * (size_t)c, r);
+  }
+}
+
+// res_calc, GATHER: one thread per incremented cell
+template <class T, int BATCH>
 __global__ void k_res_calc_gather(int nrows, const int *__restrict__ active,
                                   const int *__restrict__ row, const int *__restrict__ keys,
                                   IdxMap mx1, IdxMap mx2, IdxMap mq1, IdxMap mq2, IdxMap ma1,
@@ -185,21 +281,52 @@ __global__ void k_res_calc_gather(int nrows, const int *__restrict__ active,
   int c = active ? active[t] : t;
   T r[4];
   ldw4(res + 4 * (size_t)c, r);
-  int k1 = row[t + 1];
-  for (int k = row[t]; k < k1; k++) {
-    int key = __ldg(keys + k);
-    int e = key >> 1;
-    T p[2], s[2], q1[4], q2[4], f[4];
-    ld2(xa + 2 * (size_t)at(mx1, e), p);
-    ld2(xb + 2 * (size_t)at(mx2, e), s);
-    ld4(qa + 4 * (size_t)at(mq1, e), q1);
-    ld4(qb + 4 * (size_t)at(mq2, e), q2);
-    T a1 = __ldg(adta + at(ma1, e)), a2 = __ldg(adtb + at(ma2, e));
-    res_flux(p, s, q1, q2, a1, a2, gm1, eps, f);
-    if ((key & 1) == 0) {
-      r[0] += f[0]; r[1] += f[1]; r[2] += f[2]; r[3] += f[3];
-    } else {
-      r[0] -= f[0]; r[1] -= f[1]; r[2] -= f[2]; r[3] -= f[3];
+  const int k1 = row[t + 1];
+  const bool same_cells = mq1.map == ma1.map && mq1.idx == ma1.idx && mq2.map == ma2.map &&
+                          mq2.idx == ma2.idx && mq1.dim == ma1.dim && mq2.dim == ma2.dim;
+  // contributions in batches of B: every load of a batch is issued before
+  // any flux is computed (B = 1: one edge at a time, fewest registers --
+  // the fastest on the 720k airfoil mesh; B = 4: one chain of dependent
+  // loads per cell instead of per edge, at the cost of occupancy)
+  constexpr int B = BATCH;
+  for (int kb = row[t]; kb < k1; kb += B) {
+    int key[B], n1[B], n2[B], c1[B], c2[B], a1[B], a2[B];
+#pragma unroll
+    for (int b = 0; b < B; b++) key[b] = kb + b < k1 ? __ldg(keys + kb + b) : -2;
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+      if (key[b] < 0) continue;
+      const int e = key[b] >> 1;
+      at2(mx1, mx2, e, n1[b], n2[b]);
+      at2(mq1, mq2, e, c1[b], c2[b]);
+      if (same_cells) {
+        a1[b] = c1[b];
+        a2[b] = c2[b];
+      } else {
+        at2(ma1, ma2, e, a1[b], a2[b]);
+      }
+    }
+    T p[B][2], s[B][2], q1[B][4], q2[B][4], d1[B], d2[B];
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+      if (key[b] < 0) continue;
+      ld4(qa + 4 * (size_t)c1[b], q1[b]);
+      ld4(qb + 4 * (size_t)c2[b], q2[b]);
+      ld2(xa + 2 * (size_t)n1[b], p[b]);
+      ld2(xb + 2 * (size_t)n2[b], s[b]);
+      d1[b] = __ldg(adta + a1[b]);
+      d2[b] = __ldg(adtb + a2[b]);
+    }
+#pragma unroll
+    for (int b = 0; b < B; b++) {  // ascending order: op_seq.h's order
+      if (key[b] < 0) continue;
+      T f[4];
+      res_flux(p[b], s[b], q1[b], q2[b], d1[b], d2[b], gm1, eps, f);
+      if ((key[b] & 1) == 0) {
+        r[0] += f[0]; r[1] += f[1]; r[2] += f[2]; r[3] += f[3];
+      } else {
+        r[0] -= f[0]; r[1] -= f[1]; r[2] -= f[2]; r[3] -= f[3];
+      }
     }
   }
   st4(res + 4 * (size_t)c, r);
@@ -364,27 +491,40 @@ __global__ void k_bres_calc_coloured(PlanView P, int block_offset, const T *__re
 
 // update: q = qold - res/adt, res = 0, rms += del^2 (airfoil/update.h:1-12).
 // SEQ != nullptr: store each del^2 in element order for the serial fold.
-template <class T>
+template <class T, int U>
 __global__ void k_update(int n, const T *__restrict__ qold, T *__restrict__ q,
                          T *__restrict__ res, const T *__restrict__ adt, T *seq,
                          RedSlot<T> slot, unsigned *ticket) {
   T rms = T(0);
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-    T qo[4], r[4], qn[4];
-    ld4(qold + 4 * (size_t)c, qo);
-    ldw4(res + 4 * (size_t)c, r);
-    T adti = T(1.0f) / __ldg(adt + c);
-    T sq[4];
-    for (int d = 0; d < 4; d++) {
-      T del = adti * r[d];
-      qn[d] = qo[d] - del;
-      sq[d] = del * del;
-      rms += sq[d];
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x + threadIdx.x; base < n; base += stride * U) {
+    T qo[U][4], r[U][4], ad[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {  // all loads of the U cells first
+      int c = base + u * stride;
+      if (c < n) {
+        ld4(qold + 4 * (size_t)c, qo[u]);
+        ldw4(res + 4 * (size_t)c, r[u]);
+        ad[u] = __ldg(adt + c);
+      }
     }
-    st4(q + 4 * (size_t)c, qn);
-    const T z[4] = {T(0), T(0), T(0), T(0)};
-    st4(res + 4 * (size_t)c, z);
-    if (seq) st4(seq + 4 * (size_t)c, sq);
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      int c = base + u * stride;
+      if (c >= n) continue;
+      T adti = T(1.0f) / ad[u];
+      T qn[4], sq[4];
+      for (int d = 0; d < 4; d++) {
+        T del = adti * r[u][d];
+        qn[d] = qo[u][d] - del;
+        sq[d] = del * del;
+        rms += sq[d];
+      }
+      st4(q + 4 * (size_t)c, qn);
+      const T z[4] = {T(0), T(0), T(0), T(0)};
+      st4(res + 4 * (size_t)c, z);
+      if (seq) st4(seq + 4 * (size_t)c, sq);
+    }
   }
   if (seq) return;
   const T v[1] = {rms}, id[1] = {T(0)};
@@ -425,6 +565,20 @@ static int grid_for(long long n, int threads) {
   return (int)(g < cap ? g : cap);
 }
 
+// direct loops: U elements per thread, at most 8 CTAs of 256 per SM (full
+// occupancy), so one pass covers the 720k-cell set
+constexpr int kUnroll = 4;
+static int unroll() {
+  int u = tuning("unroll", kUnroll);
+  return u == 1 || u == 2 ? u : 4;
+}
+static int grid_direct(long long n, int U) {
+  long long g = (n + 256LL * U - 1) / (256LL * U);
+  long long cap = (long long)rt().num_sms * 8;
+  if (g < 1) g = 1;
+  return (int)(g < cap ? g : cap);
+}
+
 static PlanView plan_view(const DevPlan &p) {
   PlanView v;
   memset(&v, 0, sizeof v);
@@ -440,8 +594,13 @@ template <class T>
 static void save_soln_t(char const *name, op_set set, const op_arg *args) {
   LoopScope ls(name, compulsory_bytes(set, 2, args), 0);
   int n = set->size;
-  k_save_soln<T><<<grid_for(n, 256), 256, 0, rt().stream>>>(n, (const T *)args[0].dat->data_d,
-                                                             (T *)args[1].dat->data_d);
+  const int U = unroll();
+  const T *q = (const T *)args[0].dat->data_d;
+  T *qold = (T *)args[1].dat->data_d;
+  cudaStream_t s = rt().stream;
+  if (U == 1) k_save_soln<T, 1><<<grid_direct(n, 1), 256, 0, s>>>(n, q, qold);
+  else if (U == 2) k_save_soln<T, 2><<<grid_direct(n, 2), 256, 0, s>>>(n, q, qold);
+  else k_save_soln<T, 4><<<grid_direct(n, 4), 256, 0, s>>>(n, q, qold);
 }
 void run_save_soln(char const *name, op_set set, const op_arg *args) {
   if (is_double(args[0])) save_soln_t<double>(name, set, args);
@@ -494,13 +653,29 @@ static void res_calc_t(char const *name, op_set set, const op_arg *args) {
   if (!g) return;
   LoopScope ls(name, compulsory_bytes(set, 8, args), 0);
   if (g->nactive == 0) return;
-  k_res_calc_gather<T><<<(g->nactive + 255) / 256, 256, 0, s>>>(
-      g->nactive, g->d_active, g->d_row, g->d_keys, idx_map(args[0]), idx_map(args[1]),
-      idx_map(args[2]), idx_map(args[3]), idx_map(args[4]), idx_map(args[5]),
-      (const T *)args[0].dat->data_d, (const T *)args[1].dat->data_d,
-      (const T *)args[2].dat->data_d, (const T *)args[3].dat->data_d,
-      (const T *)args[4].dat->data_d, (const T *)args[5].dat->data_d, (T *)args[6].dat->data_d,
-      K.gm1, K.eps);
+  if (tuning("gather_tiled", 0) && g->max_row - 1 <= kTileExtra && g->ntiles > 0) {
+    k_res_calc_tiled<T><<<g->ntiles, kTile, 0, s>>>(
+        g->d_tile_first, g->d_active, g->d_row, g->d_keys, idx_map(args[0]), idx_map(args[1]),
+        idx_map(args[2]), idx_map(args[3]), idx_map(args[4]), idx_map(args[5]),
+        (const T *)args[0].dat->data_d, (const T *)args[1].dat->data_d,
+        (const T *)args[2].dat->data_d, (const T *)args[3].dat->data_d,
+        (const T *)args[4].dat->data_d, (const T *)args[5].dat->data_d, (T *)args[6].dat->data_d,
+        K.gm1, K.eps);
+    return;
+  }
+  // one thread per cell (default)
+  auto launch = [&](auto kernel) {
+    kernel<<<(g->nactive + 255) / 256, 256, 0, s>>>(
+        g->nactive, g->d_active, g->d_row, g->d_keys, idx_map(args[0]), idx_map(args[1]),
+        idx_map(args[2]), idx_map(args[3]), idx_map(args[4]), idx_map(args[5]),
+        (const T *)args[0].dat->data_d, (const T *)args[1].dat->data_d,
+        (const T *)args[2].dat->data_d, (const T *)args[3].dat->data_d,
+        (const T *)args[4].dat->data_d, (const T *)args[5].dat->data_d,
+        (T *)args[6].dat->data_d, K.gm1, K.eps);
+  };
+  if (tuning("gather_batch", 1) >= 4) launch(k_res_calc_gather<T, 4>);
+  else if (tuning("gather_batch", 1) >= 2) launch(k_res_calc_gather<T, 2>);
+  else launch(k_res_calc_gather<T, 1>);
 }
 void run_res_calc(char const *name, op_set set, const op_arg *args) {
   if (is_double(args[0])) res_calc_t<double>(name, set, args);
@@ -555,13 +730,17 @@ static void update_t(char const *name, op_set set, const op_arg *args) {
   {
     LoopScope ls(name, compulsory_bytes(set, 5, args), 0);
     T *seqbuf = seq ? (T *)red_seq_buffer(sizeof(T) * 4 * (size_t)n) : nullptr;
-    const int threads = 256;
-    const int grid = seq ? grid_for(n, threads) : red_grid(n, threads);
+    const int threads = 256, U = unroll();
+    const int grid = grid_direct(n, U);  // <= kMaxRedBlocks; fixed by n and U
     RedSlot<T> rslot{(T *)red_partials(0), result};
-    k_update<T><<<grid, threads, 0, s>>>(n, (const T *)args[0].dat->data_d,
-                                         (T *)args[1].dat->data_d, (T *)args[2].dat->data_d,
-                                         (const T *)args[3].dat->data_d, seqbuf, rslot,
-                                         red_ticket());
+    const T *qold = (const T *)args[0].dat->data_d, *adt = (const T *)args[3].dat->data_d;
+    T *q = (T *)args[1].dat->data_d, *res = (T *)args[2].dat->data_d;
+    if (U == 1)
+      k_update<T, 1><<<grid, threads, 0, s>>>(n, qold, q, res, adt, seqbuf, rslot, red_ticket());
+    else if (U == 2)
+      k_update<T, 2><<<grid, threads, 0, s>>>(n, qold, q, res, adt, seqbuf, rslot, red_ticket());
+    else
+      k_update<T, 4><<<grid, threads, 0, s>>>(n, qold, q, res, adt, seqbuf, rslot, red_ticket());
     if (seq) {
       T init = *(const T *)args[4].data;
       k_seq_sum<T><<<1, 32, 0, s>>>(seqbuf, 4LL * n, init, result);

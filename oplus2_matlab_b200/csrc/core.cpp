@@ -87,6 +87,13 @@ int op2b_set_reduction(int m) {
   rt().reduction = m;
   return old;
 }
+int op2b_set_tuning(const char *key, int value) {
+  if (!key) return -1;
+  int old = tuning(key, -1);
+  rt().tuning[key] = value;
+  return old;
+}
+
 int op2b_set_timing(int on) {
   int old = rt().timing;
   rt().timing = on != 0;

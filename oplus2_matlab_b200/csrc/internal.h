@@ -73,6 +73,9 @@ struct Runtime {
 
   std::map<std::string, LoopTimer> timers;
 
+  // kernel variant knobs (op2b_set_tuning), read by the loop launchers
+  std::map<std::string, int> tuning;
+
   // stream capture in progress (graph.cu): per-loop event pairs recorded
   // into the graph when profiling
   bool capture_profile = false;
@@ -100,6 +103,12 @@ struct Runtime {
 };
 
 Runtime &rt();
+
+// value of a tuning knob, or `def` when unset
+inline int tuning(const char *key, int def) {
+  auto it = rt().tuning.find(key);
+  return it == rt().tuning.end() ? def : it->second;
+}
 
 // device copy of a map, uploaded on first use
 const int *map_dev(op_map m);

@@ -1029,6 +1029,20 @@ __global__ void k_sort_rows(const int *row, int nrows, int *keys, int *long_rows
   if ((threadIdx.x & 31) == 0 && mx > 0) atomicMax(maxlen, mx);
 }
 
+// tile_first[b] = first row r with row[r] >= kTile * b (lower bound), for
+// b = 0..ntiles; row has nrows + 1 non-decreasing entries
+__global__ void k_tile_first(const int *row, int nrows, int ntiles, int *tile_first) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= ntiles; b += gridDim.x * blockDim.x) {
+    long long want = (long long)kTile * b;
+    int lo = 0, hi = nrows;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (row[mid] < want) lo = mid + 1; else hi = mid;
+    }
+    tile_first[b] = b == ntiles ? nrows : lo;
+  }
+}
+
 __global__ void k_sort_long_rows(const int *row, const int *long_rows, int *keys) {
   extern __shared__ int s[];
   int r = long_rows[blockIdx.x];
@@ -1115,6 +1129,10 @@ GatherPlan *get_gather_plan(op_set set, const op_arg *args, const std::vector<in
   OP2B_CUDA(cudaMemcpyAsync(h, nlong, sizeof h, cudaMemcpyDeviceToHost, s));
   OP2B_CUDA(cudaStreamSynchronize(s));
   g.max_row = h[1];
+  g.nkeys = total;
+  g.ntiles = (int)((total + kTile - 1) / kTile);
+  g.d_tile_first = (int *)dev_alloc(sizeof(int) * ((size_t)g.ntiles + 1));
+  k_tile_first<<<(g.ntiles + 256) / 256, 256, 0, s>>>(g.d_row, g.nactive, g.ntiles, g.d_tile_first);
   if (h[0] > 0) {
     int P = 1;
     while (P < g.max_row) P <<= 1;
@@ -1153,6 +1171,7 @@ void op2b_release_plans() {
   g_plans.clear();
   for (auto &up : g_gather) {
     dev_free(up->d_row); dev_free(up->d_keys); dev_free(up->d_active);
+    dev_free(up->d_tile_first);
   }
   g_gather.clear();
   extern void op2b_release_host_plans();

@@ -55,7 +55,16 @@ struct GatherPlan {
   int *d_keys = nullptr;          // [set->size * nslots] element * nslots + slot
   int *d_active = nullptr;        // [nactive] target ids, nullptr when all active
   int max_row = 0;
+  // CTA tiles for the contribution-parallel kernels: tile b owns the
+  // targets whose first contribution lies in [kTile*b, kTile*(b+1)), i.e.
+  // targets [d_tile_first[b], d_tile_first[b+1]); [ntiles + 1] entries
+  int ntiles = 0;
+  int *d_tile_first = nullptr;
+  long long nkeys = 0;
 };
+
+// contributions per CTA tile of the contribution-parallel gather kernels
+constexpr int kTile = 256;
 
 // Find or build the reference-compatible plan (device resident).
 DevPlan *get_plan(char const *name, op_set set, int part_size, int nargs, const op_arg *args,

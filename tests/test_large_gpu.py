@@ -44,8 +44,9 @@ def test_airfoil_full_size(op2, case, reduction):
     st = A.fetch()
     assert op2.last_error() == ""
     # TREE: fields bit-identical; the printed rms differs from op_seq.h's
-    # one-at-a-time float sum of 2.9M terms by that sum's own rounding
-    tol = 0.0 if reduction == "seq" else (2e-4 if dt == np.float32 else 1e-12)
+    # one-at-a-time float sum of 2.9M squares by that sum's own rounding
+    # (measured 2.0e-4 at iteration 930); SEQ reproduces it exactly
+    tol = 0.0 if reduction == "seq" else (5e-4 if dt == np.float32 else 1e-12)
     for it, val in g["rms"]:
         rel = abs(float(rms[it - 1]) - val) / val
         assert rel <= tol, (it, float(rms[it - 1]), val, rel)
