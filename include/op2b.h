@@ -104,6 +104,23 @@ long op2b_plan_validate(char const *name, op_set set, int part_size, int nargs, 
  * times its size; benchmark drivers call it between timed steps. */
 int op2b_l2_flush(void);
 
+/* The airfoil update loop (q = qold - res/adt, res = 0, *rms += sum of
+ * del^2) for callers that must not allocate device memory: code that cannot
+ * afford cudaMalloc's device synchronisation, hosts that reserve all device
+ * memory for their own pool, or latency-bound threads that cannot take a
+ * first-call allocation.  No counterpart in the reference.
+ * All pointers are the caller's 16-byte-aligned FP32 device arrays (qold, q,
+ * res: 4 per cell; adt: 1 per cell; rms: 1 value, added to).  Nothing is
+ * allocated: the reduction's scratch is a fixed 16 KB array inside the
+ * library, so ncell must be at most 4,194,304 (larger sizes return -1 and run
+ * nothing).  The first call on a device looks up that array's address: make
+ * it before any stream capture.  All calls share the array, so calls that
+ * overlap on the GPU race; calls in one stream are safe.  Returns 0, a
+ * negative code for bad arguments, or a CUDA error code; asynchronous on
+ * `stream` (a cudaStream_t, NULL for the default stream). */
+int op2b_update_noalloc(int ncell, const float *qold, float *q, float *res, const float *adt,
+                        float *rms, void *stream);
+
 /* Library build string (arch, flags). */
 char const *op2b_version(void);
 
