@@ -39,6 +39,9 @@ enum { OP2B_REDUCE_TREE = 0, OP2B_REDUCE_SEQ = 1 };
  *   "gather_tiled"  0: one thread per incremented element, contributions
  *                   loaded in batches (default); 1: one thread per
  *                   contribution in CTA tiles, folded in shared memory
+ *   "gather_flux"   1: res_calc as two passes, each edge's flux computed once
+ *                   into a buffer, then folded per cell in edge order
+ *                   (default); 0: one pass, each cell recomputes its fluxes
  *   "gather_batch"  contributions whose loads are issued together per
  *                   thread in the per-element GATHER kernel (1, 2, 4)
  *   "unroll"        elements per thread in the direct loops (1, 2, 4) */

@@ -19,6 +19,8 @@
 
 #include <string.h>
 
+#include <algorithm>
+
 #include "loops.h"
 #include "reduce.cuh"
 
@@ -178,28 +180,43 @@ __global__ void k_save_soln(int n, const T *__restrict__ q, T *__restrict__ qold
 
 // adt_calc: direct over cells, x gathered through pcell (one 16-byte load
 // of the 4 node indices when the four args share a dim-4 map in order)
-template <class T>
+template <class T, int U>
 __global__ void k_adt_calc(int n, IdxMap m0, IdxMap m1, IdxMap m2, IdxMap m3, IdxMap mq,
                            const T *__restrict__ x0, const T *__restrict__ x1,
                            const T *__restrict__ x2, const T *__restrict__ x3,
                            const T *__restrict__ q, T *__restrict__ adt, AirConsts<T> K) {
   const bool quad = m0.map && m0.map == m1.map && m0.map == m2.map && m0.map == m3.map &&
                     m0.dim == 4 && m0.idx == 0 && m1.idx == 1 && m2.idx == 2 && m3.idx == 3;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-    int n0, n1, n2, n3;
-    if (quad) {
-      int4 v = __ldg(reinterpret_cast<const int4 *>(m0.map) + c);
-      n0 = v.x; n1 = v.y; n2 = v.z; n3 = v.w;
-    } else {
-      n0 = at(m0, c); n1 = at(m1, c); n2 = at(m2, c); n3 = at(m3, c);
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x + threadIdx.x; base < n; base += stride * U) {
+    int nd[U][4];
+#pragma unroll
+    for (int u = 0; u < U; u++) {  // node indices of U cells
+      const int c = base + u * stride;
+      if (c >= n) continue;
+      if (quad) {
+        int4 v = __ldg(reinterpret_cast<const int4 *>(m0.map) + c);
+        nd[u][0] = v.x; nd[u][1] = v.y; nd[u][2] = v.z; nd[u][3] = v.w;
+      } else {
+        nd[u][0] = at(m0, c); nd[u][1] = at(m1, c); nd[u][2] = at(m2, c); nd[u][3] = at(m3, c);
+      }
     }
-    T a[2], b[2], d[2], e[2], qq[4];
-    ld4(q + 4 * (size_t)at(mq, c), qq);
-    ld2(x0 + 2 * (size_t)n0, a);
-    ld2(x1 + 2 * (size_t)n1, b);
-    ld2(x2 + 2 * (size_t)n2, d);
-    ld2(x3 + 2 * (size_t)n3, e);
-    adt[c] = adt_calc(a, b, d, e, qq, K);
+    T xs[U][4][2], qq[U][4];
+#pragma unroll
+    for (int u = 0; u < U; u++) {  // then every gather of the U cells
+      const int c = base + u * stride;
+      if (c >= n) continue;
+      ld4(q + 4 * (size_t)at(mq, c), qq[u]);
+      ld2(x0 + 2 * (size_t)nd[u][0], xs[u][0]);
+      ld2(x1 + 2 * (size_t)nd[u][1], xs[u][1]);
+      ld2(x2 + 2 * (size_t)nd[u][2], xs[u][2]);
+      ld2(x3 + 2 * (size_t)nd[u][3], xs[u][3]);
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int c = base + u * stride;
+      if (c < n) adt[c] = adt_calc(xs[u][0], xs[u][1], xs[u][2], xs[u][3], qq[u], K);
+    }
   }
 }
 
@@ -326,6 +343,73 @@ __global__ void k_res_calc_gather(int nrows, const int *__restrict__ active,
         r[0] += f[0]; r[1] += f[1]; r[2] += f[2]; r[3] += f[3];
       } else {
         r[0] -= f[0]; r[1] -= f[1]; r[2] -= f[2]; r[3] -= f[3];
+      }
+    }
+  }
+  st4(res + 4 * (size_t)c, r);
+}
+
+// res_calc, GATHER in two passes.  Pass 1, one thread per edge in edge
+// order (coalesced map reads): the flux f of airfoil/res_calc.h, computed
+// once, into flux[e].  Pass 2, one thread per cell: fold +f (first cell of
+// the edge) or -f (second cell) in ascending edge order onto res -- the
+// order of op_seq.h, so still bit-identical.  The flux buffer (16 B per
+// edge in FP32) is written and re-read while it sits in L2.
+template <class T>
+__global__ void k_res_flux(int nedge, IdxMap mx1, IdxMap mx2, IdxMap mq1, IdxMap mq2,
+                           IdxMap ma1, IdxMap ma2, const T *__restrict__ xa,
+                           const T *__restrict__ xb, const T *__restrict__ qa,
+                           const T *__restrict__ qb, const T *__restrict__ adta,
+                           const T *__restrict__ adtb, T *__restrict__ flux, T gm1, T eps) {
+  const bool same_cells = mq1.map == ma1.map && mq1.idx == ma1.idx && mq2.map == ma2.map &&
+                          mq2.idx == ma2.idx && mq1.dim == ma1.dim && mq2.dim == ma2.dim;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nedge; e += gridDim.x * blockDim.x) {
+    int n1, n2, c1, c2, a1, a2;
+    at2(mx1, mx2, e, n1, n2);
+    at2(mq1, mq2, e, c1, c2);
+    if (same_cells) {
+      a1 = c1;
+      a2 = c2;
+    } else {
+      at2(ma1, ma2, e, a1, a2);
+    }
+    T p[2], s[2], q1[4], q2[4], f[4];
+    ld4(qa + 4 * (size_t)c1, q1);
+    ld4(qb + 4 * (size_t)c2, q2);
+    ld2(xa + 2 * (size_t)n1, p);
+    ld2(xb + 2 * (size_t)n2, s);
+    const T d1 = __ldg(adta + a1), d2 = __ldg(adtb + a2);
+    res_flux(p, s, q1, q2, d1, d2, gm1, eps, f);
+    st4(flux + 4 * (size_t)e, f);
+  }
+}
+
+template <class T>
+__global__ void k_res_fold(int nrows, const int *__restrict__ active, const int *__restrict__ row,
+                           const int *__restrict__ keys, const T *__restrict__ flux,
+                           T *__restrict__ res) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nrows) return;
+  const int c = active ? active[t] : t;
+  T r[4];
+  ldw4(res + 4 * (size_t)c, r);
+  const int k1 = row[t + 1];
+  constexpr int B = 4;  // keys, then fluxes, of up to B contributions in flight
+  for (int kb = row[t]; kb < k1; kb += B) {
+    int key[B];
+    T f[B][4];
+#pragma unroll
+    for (int b = 0; b < B; b++) key[b] = kb + b < k1 ? __ldg(keys + kb + b) : -1;
+#pragma unroll
+    for (int b = 0; b < B; b++)
+      if (key[b] >= 0) ld4(flux + 4 * (size_t)(key[b] >> 1), f[b]);
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+      if (key[b] < 0) continue;
+      if ((key[b] & 1) == 0) {
+        r[0] += f[b][0]; r[1] += f[b][1]; r[2] += f[b][2]; r[3] += f[b][3];
+      } else {
+        r[0] -= f[b][0]; r[1] -= f[b][1]; r[2] -= f[b][2]; r[3] -= f[b][3];
       }
     }
   }
@@ -574,7 +658,7 @@ static int unroll() {
 }
 static int grid_direct(long long n, int U) {
   long long g = (n + 256LL * U - 1) / (256LL * U);
-  long long cap = (long long)rt().num_sms * 8;
+  long long cap = (long long)rt().num_sms * tuning("direct_ctas_per_sm", 8);
   if (g < 1) g = 1;
   return (int)(g < cap ? g : cap);
 }
@@ -613,11 +697,16 @@ static void adt_calc_t(char const *name, op_set set, const op_arg *args) {
   if (error_pending()) return;
   LoopScope ls(name, compulsory_bytes(set, 6, args), 0);
   int n = set->size;
-  k_adt_calc<T><<<grid_for(n, 256), 256, 0, rt().stream>>>(
-      n, idx_map(args[0]), idx_map(args[1]), idx_map(args[2]), idx_map(args[3]), idx_map(args[4]),
-      (const T *)args[0].dat->data_d, (const T *)args[1].dat->data_d,
-      (const T *)args[2].dat->data_d, (const T *)args[3].dat->data_d,
-      (const T *)args[4].dat->data_d, (T *)args[5].dat->data_d, K);
+  const int U = tuning("adt_unroll", 1) >= 2 ? 2 : 1;
+  auto launch = [&](auto kernel, int u) {
+    kernel<<<grid_direct(n, u), 256, 0, rt().stream>>>(
+        n, idx_map(args[0]), idx_map(args[1]), idx_map(args[2]), idx_map(args[3]),
+        idx_map(args[4]), (const T *)args[0].dat->data_d, (const T *)args[1].dat->data_d,
+        (const T *)args[2].dat->data_d, (const T *)args[3].dat->data_d,
+        (const T *)args[4].dat->data_d, (T *)args[5].dat->data_d, K);
+  };
+  if (U == 2) launch(k_adt_calc<T, 2>, 2);
+  else launch(k_adt_calc<T, 1>, 1);
 }
 void run_adt_calc(char const *name, op_set set, const op_arg *args) {
   if (is_double(args[0])) adt_calc_t<double>(name, set, args);
@@ -653,6 +742,28 @@ static void res_calc_t(char const *name, op_set set, const op_arg *args) {
   if (!g) return;
   LoopScope ls(name, compulsory_bytes(set, 8, args), 0);
   if (g->nactive == 0) return;
+  if (tuning("gather_flux", 1)) {
+    // two passes: each edge's flux once, then the ordered per-cell fold
+    const int ne = set->size;
+    const size_t need = sizeof(T) * 4 * (size_t)ne;
+    if (g->contrib_bytes < need) {
+      dev_free(g->d_contrib);
+      g->d_contrib = dev_alloc(need);
+      g->contrib_bytes = g->d_contrib ? need : 0;
+      if (!g->d_contrib) return;
+    }
+    T *flux = (T *)g->d_contrib;
+    k_res_flux<T><<<grid_for(ne, 256), 256, 0, s>>>(
+        ne, idx_map(args[0]), idx_map(args[1]), idx_map(args[2]), idx_map(args[3]),
+        idx_map(args[4]), idx_map(args[5]), (const T *)args[0].dat->data_d,
+        (const T *)args[1].dat->data_d, (const T *)args[2].dat->data_d,
+        (const T *)args[3].dat->data_d, (const T *)args[4].dat->data_d,
+        (const T *)args[5].dat->data_d, flux, K.gm1, K.eps);
+    k_res_fold<T><<<(g->nactive + 255) / 256, 256, 0, s>>>(g->nactive, g->d_active, g->d_row,
+                                                          g->d_keys, flux,
+                                                          (T *)args[6].dat->data_d);
+    return;
+  }
   if (tuning("gather_tiled", 0) && g->max_row - 1 <= kTileExtra && g->ntiles > 0) {
     k_res_calc_tiled<T><<<g->ntiles, kTile, 0, s>>>(
         g->d_tile_first, g->d_active, g->d_row, g->d_keys, idx_map(args[0]), idx_map(args[1]),
@@ -731,7 +842,12 @@ static void update_t(char const *name, op_set set, const op_arg *args) {
     LoopScope ls(name, compulsory_bytes(set, 5, args), 0);
     T *seqbuf = seq ? (T *)red_seq_buffer(sizeof(T) * 4 * (size_t)n) : nullptr;
     const int threads = 256, U = unroll();
-    const int grid = grid_direct(n, U);  // <= kMaxRedBlocks; fixed by n and U
+    // fewer, fuller CTAs than the other direct loops: fewer partials for the
+    // last block to fold (measured best at 4 per SM); <= kMaxRedBlocks and
+    // fixed by n and U, so the sum is reproducible
+    long long gw = (n + 256LL * U - 1) / (256LL * U);
+    long long gcap = (long long)rt().num_sms * tuning("update_ctas_per_sm", 4);
+    const int grid = (int)std::max(1LL, std::min(gw, std::min(gcap, (long long)kMaxRedBlocks)));
     RedSlot<T> rslot{(T *)red_partials(0), result};
     const T *qold = (const T *)args[0].dat->data_d, *adt = (const T *)args[3].dat->data_d;
     T *q = (T *)args[1].dat->data_d, *res = (T *)args[2].dat->data_d;

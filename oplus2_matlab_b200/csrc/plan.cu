@@ -1172,6 +1172,7 @@ void op2b_release_plans() {
   for (auto &up : g_gather) {
     dev_free(up->d_row); dev_free(up->d_keys); dev_free(up->d_active);
     dev_free(up->d_tile_first);
+    dev_free(up->d_contrib);
   }
   g_gather.clear();
   extern void op2b_release_host_plans();

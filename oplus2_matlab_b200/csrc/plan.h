@@ -61,6 +61,10 @@ struct GatherPlan {
   int ntiles = 0;
   int *d_tile_first = nullptr;
   long long nkeys = 0;
+  // per-element contribution buffer of the two-pass kernels, allocated on
+  // first use (outside any graph capture) and kept with the plan
+  void *d_contrib = nullptr;
+  size_t contrib_bytes = 0;
 };
 
 // contributions per CTA tile of the contribution-parallel gather kernels
