@@ -869,4 +869,259 @@ void run_airfoil_update(char const *name, op_set set, const op_arg *args) {
   else update_t<float>(name, set, args);
 }
 
+// ------------------------------------------------------- fused loop pairs --
+// Two consecutive op_par_loop calls run as one kernel when the second only
+// reads what the first leaves unchanged, or reads it at the same element
+// (loops.cpp decides; these are the kernels).  The arithmetic of each loop
+// and the order of every increment are unchanged, so results are identical
+// to running the two loops one after the other.
+
+// save_soln then adt_calc over the same cells: q is read once
+template <class T>
+__global__ void k_save_adt(int n, const T *__restrict__ q, T *__restrict__ qold, IdxMap m0,
+                           IdxMap m1, IdxMap m2, IdxMap m3, const T *__restrict__ x0,
+                           const T *__restrict__ x1, const T *__restrict__ x2,
+                           const T *__restrict__ x3, const T *__restrict__ q2,
+                           T *__restrict__ adt, AirConsts<T> K) {
+  const bool quad = m0.map && m0.map == m1.map && m0.map == m2.map && m0.map == m3.map &&
+                    m0.dim == 4 && m0.idx == 0 && m1.idx == 1 && m2.idx == 2 && m3.idx == 3;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    int nd[4];
+    if (quad) {
+      int4 v = __ldg(reinterpret_cast<const int4 *>(m0.map) + c);
+      nd[0] = v.x; nd[1] = v.y; nd[2] = v.z; nd[3] = v.w;
+    } else {
+      nd[0] = at(m0, c); nd[1] = at(m1, c); nd[2] = at(m2, c); nd[3] = at(m3, c);
+    }
+    T qq[4], qa[4], a[2], b[2], d[2], e[2];
+    ld4(q + 4 * (size_t)c, qq);
+    if (q2 != q) ld4(q2 + 4 * (size_t)c, qa);
+    ld2(x0 + 2 * (size_t)nd[0], a);
+    ld2(x1 + 2 * (size_t)nd[1], b);
+    ld2(x2 + 2 * (size_t)nd[2], d);
+    ld2(x3 + 2 * (size_t)nd[3], e);
+    st4(qold + 4 * (size_t)c, qq);
+    adt[c] = adt_calc(a, b, d, e, q2 != q ? qa : qq, K);
+  }
+}
+
+// update then adt_calc over the same cells: adt_calc reads the q this
+// thread has just written and overwrites the adt it has just read
+template <class T>
+__global__ void k_update_adt(int n, const T *__restrict__ qold, T *__restrict__ q,
+                             T *__restrict__ res, T *__restrict__ adt, IdxMap m0, IdxMap m1,
+                             IdxMap m2, IdxMap m3, const T *__restrict__ x0,
+                             const T *__restrict__ x1, const T *__restrict__ x2,
+                             const T *__restrict__ x3, AirConsts<T> K, RedSlot<T> slot,
+                             unsigned *ticket) {
+  const bool quad = m0.map && m0.map == m1.map && m0.map == m2.map && m0.map == m3.map &&
+                    m0.dim == 4 && m0.idx == 0 && m1.idx == 1 && m2.idx == 2 && m3.idx == 3;
+  T rms = T(0);
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    int nd[4];
+    if (quad) {
+      int4 v = __ldg(reinterpret_cast<const int4 *>(m0.map) + c);
+      nd[0] = v.x; nd[1] = v.y; nd[2] = v.z; nd[3] = v.w;
+    } else {
+      nd[0] = at(m0, c); nd[1] = at(m1, c); nd[2] = at(m2, c); nd[3] = at(m3, c);
+    }
+    T qo[4], r[4], a[2], b[2], d[2], e[2];
+    ld4(qold + 4 * (size_t)c, qo);
+    ldw4(res + 4 * (size_t)c, r);
+    const T ad = adt[c];
+    ld2(x0 + 2 * (size_t)nd[0], a);
+    ld2(x1 + 2 * (size_t)nd[1], b);
+    ld2(x2 + 2 * (size_t)nd[2], d);
+    ld2(x3 + 2 * (size_t)nd[3], e);
+    // airfoil/update.h:1-12
+    T adti = T(1.0f) / ad;
+    T qn[4];
+    for (int k = 0; k < 4; k++) {
+      T del = adti * r[k];
+      qn[k] = qo[k] - del;
+      rms += del * del;
+    }
+    st4(q + 4 * (size_t)c, qn);
+    const T z[4] = {T(0), T(0), T(0), T(0)};
+    st4(res + 4 * (size_t)c, z);
+    // airfoil/adt_calc.h on the new q
+    adt[c] = adt_calc(a, b, d, e, qn, K);
+  }
+  const T v[1] = {rms}, id[1] = {T(0)};
+  RedSlot<T> sl[1] = {slot};
+  grid_finish<T, OpSum, OpSum, 1>(v, id, OpSum(), OpSum(), sl, ticket);
+}
+
+// res_calc's ordered fold followed by bres_calc's contributions to the same
+// cell, in bedge order: the per-cell order of running the two loops in turn
+template <class T>
+__global__ void k_res_fold_bres(int nrows, const int *__restrict__ row,
+                                const int *__restrict__ keys, const T *__restrict__ flux,
+                                const int *__restrict__ brow, const int *__restrict__ bkeys,
+                                IdxMap bx1, IdxMap bx2, IdxMap bq, IdxMap ba, IdxMap bb,
+                                const T *__restrict__ xa, const T *__restrict__ xb,
+                                const T *__restrict__ q, const T *__restrict__ adt,
+                                const int *__restrict__ bound, T *__restrict__ res,
+                                AirConsts<T> K) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nrows) return;
+  T r[4];
+  ldw4(res + 4 * (size_t)c, r);
+  const int k1 = row[c + 1];
+  constexpr int B = 4;
+  for (int kb = row[c]; kb < k1; kb += B) {
+    int key[B];
+    T f[B][4];
+#pragma unroll
+    for (int b = 0; b < B; b++) key[b] = kb + b < k1 ? __ldg(keys + kb + b) : -1;
+#pragma unroll
+    for (int b = 0; b < B; b++)
+      if (key[b] >= 0) ld4(flux + 4 * (size_t)(key[b] >> 1), f[b]);
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+      if (key[b] < 0) continue;
+      if ((key[b] & 1) == 0) {
+        r[0] += f[b][0]; r[1] += f[b][1]; r[2] += f[b][2]; r[3] += f[b][3];
+      } else {
+        r[0] -= f[b][0]; r[1] -= f[b][1]; r[2] -= f[b][2]; r[3] -= f[b][3];
+      }
+    }
+  }
+  const int j1 = brow[c + 1];
+  for (int j = brow[c]; j < j1; j++) {
+    const int e = __ldg(bkeys + j);
+    T p[2], s[2], q1[4];
+    ld2(xa + 2 * (size_t)at(bx1, e), p);
+    ld2(xb + 2 * (size_t)at(bx2, e), s);
+    ld4(q + 4 * (size_t)at(bq, e), q1);
+    bres_apply(p, s, q1, __ldg(adt + at(ba, e)), __ldg(bound + at(bb, e)), K, r);
+  }
+  st4(res + 4 * (size_t)c, r);
+}
+
+// brow[c] = first bres contribution of cell c = row_b[lower_bound(active_b, c)]
+__global__ void k_bres_rows(int ncell, const int *__restrict__ active_b, int nactive_b,
+                            const int *__restrict__ row_b, int *brow) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= ncell; c += gridDim.x * blockDim.x) {
+    int lo = 0, hi = nactive_b;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (active_b[mid] < c) lo = mid + 1; else hi = mid;
+    }
+    brow[c] = row_b[lo];
+  }
+}
+
+template <class T>
+static bool save_adt_t(op_set set, const op_arg *sa, const op_arg *aa) {
+  AirConsts<T> K = air_consts<T>();
+  if (error_pending()) return true;
+  LoopScope ls("save_soln+adt_calc", compulsory_bytes(set, 2, sa) + compulsory_bytes(set, 6, aa), 0);
+  const int n = set->size;
+  k_save_adt<T><<<grid_for(n, 256), 256, 0, rt().stream>>>(
+      n, (const T *)sa[0].dat->data_d, (T *)sa[1].dat->data_d, idx_map(aa[0]), idx_map(aa[1]),
+      idx_map(aa[2]), idx_map(aa[3]), (const T *)aa[0].dat->data_d,
+      (const T *)aa[1].dat->data_d, (const T *)aa[2].dat->data_d,
+      (const T *)aa[3].dat->data_d, (const T *)aa[4].dat->data_d, (T *)aa[5].dat->data_d, K);
+  return true;
+}
+
+bool run_save_adt(op_set set, const op_arg *sa, const op_arg *aa) {
+  return is_double(sa[0]) ? save_adt_t<double>(set, sa, aa) : save_adt_t<float>(set, sa, aa);
+}
+
+template <class T>
+static bool update_adt_t(op_set set, const op_arg *ua, const op_arg *aa) {
+  AirConsts<T> K = air_consts<T>();
+  if (error_pending()) return true;
+  cudaStream_t s = rt().stream;
+  const int n = set->size;
+  int slot = red_new_slot();
+  T *result = (T *)red_slot_ptr(slot);
+  {
+    LoopScope ls("update+adt_calc", compulsory_bytes(set, 5, ua) + compulsory_bytes(set, 6, aa), 0);
+    long long gw = (n + 255LL) / 256;
+    long long gcap = (long long)rt().num_sms * tuning("update_ctas_per_sm", 4);
+    const int grid = (int)std::max(1LL, std::min(gw, std::min(gcap, (long long)kMaxRedBlocks)));
+    RedSlot<T> rslot{(T *)red_partials(0), result};
+    k_update_adt<T><<<grid, 256, 0, s>>>(
+        n, (const T *)ua[0].dat->data_d, (T *)ua[1].dat->data_d, (T *)ua[2].dat->data_d,
+        (T *)ua[3].dat->data_d, idx_map(aa[0]), idx_map(aa[1]), idx_map(aa[2]), idx_map(aa[3]),
+        (const T *)aa[0].dat->data_d, (const T *)aa[1].dat->data_d,
+        (const T *)aa[2].dat->data_d, (const T *)aa[3].dat->data_d, K, rslot, red_ticket());
+  }
+  red_finish({GblRequest{ua[4].data, slot, OP_INC, sizeof(T) == 8 ? GBL_F64 : GBL_F32, false}});
+  return true;
+}
+
+bool run_update_adt(op_set set, const op_arg *ua, const op_arg *aa) {
+  return is_double(ua[0]) ? update_adt_t<double>(set, ua, aa) : update_adt_t<float>(set, ua, aa);
+}
+
+// fused res_calc + bres_calc needs the bres contributions indexed by cell
+struct BresRows {
+  const GatherPlan *res = nullptr, *bres = nullptr;
+  int *d_brow = nullptr;
+};
+static std::vector<BresRows> g_bres_rows;
+
+void release_fused_plans() {
+  for (auto &b : g_bres_rows) dev_free(b.d_brow);
+  g_bres_rows.clear();
+}
+
+template <class T>
+static bool res_bres_t(op_set rset, const op_arg *ra, op_set bset, const op_arg *ba) {
+  AirConsts<T> K = air_consts<T>();
+  if (error_pending()) return true;
+  cudaStream_t s = rt().stream;
+  GatherPlan *g = get_gather_plan(rset, ra, {6, 7});
+  GatherPlan *gb = get_gather_plan(bset, ba, {4});
+  if (!g || !gb) return true;
+  // only when every cell is a res_calc target, so the fold covers bres's cells
+  if (g->d_active || g->nactive != ra[6].dat->set->size) return false;
+  const BresRows *br = nullptr;
+  for (auto &b : g_bres_rows)
+    if (b.res == g && b.bres == gb) br = &b;
+  if (!br) {
+    BresRows b{g, gb, (int *)dev_alloc(sizeof(int) * ((size_t)g->nactive + 1))};
+    if (!b.d_brow) return true;
+    if (gb->d_active)
+      k_bres_rows<<<grid_for(g->nactive + 1, 256), 256, 0, s>>>(g->nactive, gb->d_active,
+                                                                gb->nactive, gb->d_row, b.d_brow);
+    else
+      OP2B_CUDA(cudaMemcpyAsync(b.d_brow, gb->d_row, sizeof(int) * ((size_t)g->nactive + 1),
+                                cudaMemcpyDeviceToDevice, s));
+    g_bres_rows.push_back(b);
+    br = &g_bres_rows.back();
+  }
+  const int ne = rset->size;
+  const size_t need = sizeof(T) * 4 * (size_t)ne;
+  if (g->contrib_bytes < need) {
+    dev_free(g->d_contrib);
+    g->d_contrib = dev_alloc(need);
+    g->contrib_bytes = g->d_contrib ? need : 0;
+    if (!g->d_contrib) return true;
+  }
+  T *flux = (T *)g->d_contrib;
+  LoopScope ls("res_calc+bres_calc",
+               compulsory_bytes(rset, 8, ra) + compulsory_bytes(bset, 6, ba), 0);
+  k_res_flux<T><<<grid_for(ne, 256), 256, 0, s>>>(
+      ne, idx_map(ra[0]), idx_map(ra[1]), idx_map(ra[2]), idx_map(ra[3]), idx_map(ra[4]),
+      idx_map(ra[5]), (const T *)ra[0].dat->data_d, (const T *)ra[1].dat->data_d,
+      (const T *)ra[2].dat->data_d, (const T *)ra[3].dat->data_d, (const T *)ra[4].dat->data_d,
+      (const T *)ra[5].dat->data_d, flux, K.gm1, K.eps);
+  k_res_fold_bres<T><<<(g->nactive + 255) / 256, 256, 0, s>>>(
+      g->nactive, g->d_row, g->d_keys, flux, br->d_brow, gb->d_keys, idx_map(ba[0]),
+      idx_map(ba[1]), idx_map(ba[2]), idx_map(ba[3]), idx_map(ba[5]),
+      (const T *)ba[0].dat->data_d, (const T *)ba[1].dat->data_d, (const T *)ba[2].dat->data_d,
+      (const T *)ba[3].dat->data_d, (const int *)ba[5].dat->data_d, (T *)ra[6].dat->data_d, K);
+  return true;
+}
+
+bool run_res_bres(op_set rset, const op_arg *ra, op_set bset, const op_arg *ba) {
+  return is_double(ra[0]) ? res_bres_t<double>(rset, ra, bset, ba)
+                          : res_bres_t<float>(rset, ra, bset, ba);
+}
+
 }  // namespace op2b

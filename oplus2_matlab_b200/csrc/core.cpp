@@ -78,16 +78,19 @@ int op2b_set_error_mode(int mode) {
   return old;
 }
 int op2b_set_strategy(int s) {
+  flush_pending();
   int old = rt().strategy;
   rt().strategy = s;
   return old;
 }
 int op2b_set_reduction(int m) {
+  flush_pending();
   int old = rt().reduction;
   rt().reduction = m;
   return old;
 }
 int op2b_set_tuning(const char *key, int value) {
+  flush_pending();
   if (!key) return -1;
   int old = tuning(key, -1);
   rt().tuning[key] = value;
@@ -327,6 +330,7 @@ void op_diagnostic_output(void) {
 // kernels (CUDA events) rather than host wall time around a synchronising
 // stub, because loops here do not synchronise.
 void op_timing_output(void) {
+  flush_pending();
   flush_timers();
   if (OP_kern_max > 0) {
     printf("\n  count     time     GB/s     GB/s   kernel name ");

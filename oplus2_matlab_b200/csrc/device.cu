@@ -14,6 +14,8 @@
 
 namespace op2b {
 
+void release_fused_plans();  // airfoil.cu
+
 void ensure_cuda() {
   Runtime &R = rt();
   if (R.cuda_ready) return;
@@ -212,6 +214,7 @@ op_dat op_decl_dat_char(op_set set, int dim, char const *type, int size, char *d
 // parameters (the parameter bank is constant memory too).  A later
 // declaration of the same name replaces the earlier one (jac2/jac.cpp:137-140).
 void op_decl_const_char(int dim, char const *type, int size, char *dat, char const *name) {
+  flush_pending();
   if (dim <= 0 || size <= 0 || dat == nullptr) {
     fail(-1, "op_decl_const error -- invalid constant %s\n", name ? name : "(null)");
     return;
@@ -227,6 +230,7 @@ void op_decl_const_char(int dim, char const *type, int size, char *dat, char con
 
 // common/op_lib.cu:116-121: device -> the caller's original array
 void op_fetch_data(op_dat dat) {
+  flush_pending();
   if (!dat || !dat->data_d) return;
   Runtime &R = rt();
   deliver_deferred();
@@ -237,6 +241,7 @@ void op_fetch_data(op_dat dat) {
 
 // common/op_lib.cu:186-209
 void op_exit(void) {
+  flush_pending();
   Runtime &R = rt();
   if (R.cuda_ready) {
     deliver_deferred();
@@ -244,6 +249,7 @@ void op_exit(void) {
     flush_timers();
   }
   op2b_release_plans();
+  release_fused_plans();
   for (auto &m : R.maps) dev_free(m.d);
   R.maps.clear();
   for (int i = 0; i < OP_dat_index; i++) dev_free(OP_dat_list[i]->data_d);
@@ -273,12 +279,14 @@ void op2b_set_stream(void *s) {
 }
 
 int op2b_sync(void) {
+  flush_pending();
   ensure_cuda();
   deliver_deferred();
   return (int)cudaStreamSynchronize(rt().stream);
 }
 
 double op2b_loop_time(char const *name, int *count) {
+  flush_pending();
   flush_timers();
   auto it = rt().timers.find(name);
   if (it == rt().timers.end()) return -1.0;

@@ -169,6 +169,7 @@ void red_reserve_for_graph() { rs().graph_slots = std::max(rs().graph_slots, rs(
 }  // namespace op2b
 
 extern "C" int op2b_set_gbl_deferred(int on) {
+  op2b::flush_pending();
   op2b::Runtime &R = op2b::rt();
   int old = R.gbl_deferred;
   if (old && !on) op2b::deliver_deferred();

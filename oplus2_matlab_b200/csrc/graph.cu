@@ -53,6 +53,7 @@ int op2b_capture_begin(int profile) {
 }
 
 void *op2b_capture_end(void) {
+  flush_pending();
   Runtime &R = rt();
   Graph *g = new Graph();
   cudaError_t e = cudaStreamEndCapture(R.stream, &g->graph);

@@ -113,6 +113,10 @@ inline int tuning(const char *key, int def) {
 // device copy of a map, uploaded on first use
 const int *map_dev(op_map m);
 
+// launch the loop held back for fusion, if any (loops.cpp); every call that
+// needs device results to be complete or issued runs it first
+void flush_pending();
+
 // device memory helpers (long-lived allocations)
 void *dev_alloc(size_t bytes);
 void dev_free(void *p);

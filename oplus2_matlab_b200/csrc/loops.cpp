@@ -129,7 +129,101 @@ int jac_update_variant(int n, const op_arg *a) {
   return 0;
 }
 
+enum Kind { K_NONE, K_SAVE, K_ADT, K_RES, K_BRES, K_AUPDATE, K_JRES, K_JUPDATE };
+
+Kind classify(int nargs, const op_arg *args, int *variant) {
+  *variant = 0;
+  if (is_res_calc(nargs, args)) return K_RES;
+  if (is_adt_calc(nargs, args)) return K_ADT;
+  if (is_bres_calc(nargs, args)) return K_BRES;
+  if (is_save_soln(nargs, args)) return K_SAVE;
+  if (is_airfoil_update(nargs, args)) return K_AUPDATE;
+  if ((*variant = jac_res_variant(nargs, args))) return K_JRES;
+  if ((*variant = jac_update_variant(nargs, args))) return K_JUPDATE;
+  return K_NONE;
+}
+
+void run_kind(Kind k, int variant, char const *name, op_set set, const op_arg *args) {
+  switch (k) {
+    case K_RES: return run_res_calc(name, set, args);
+    case K_ADT: return run_adt_calc(name, set, args);
+    case K_BRES: return run_bres_calc(name, set, args);
+    case K_SAVE: return run_save_soln(name, set, args);
+    case K_AUPDATE: return run_airfoil_update(name, set, args);
+    case K_JRES: return run_jac_res(name, set, args, variant);
+    case K_JUPDATE: return run_jac_update(name, set, args, variant);
+    default: return;
+  }
+}
+
+// The loop held back in case the next call can be fused with it.
+struct Pending {
+  Kind kind = K_NONE;
+  std::string name;
+  op_set set = nullptr;
+  std::vector<op_arg> args;
+};
+Pending g_pending;
+
+bool dat_in(op_dat d, std::initializer_list<op_dat> ds) {
+  for (op_dat x : ds)
+    if (x == d) return true;
+  return false;
+}
+
+// Can `next` run fused with the held-back loop?  Each case checks that the
+// second loop reads nothing the first writes, except at the same element,
+// and writes nothing the first reads elsewhere.
+bool try_fuse(const Pending &p, Kind k, op_set set, const op_arg *a) {
+  const op_arg *pa = p.args.data();
+  if (p.kind == K_SAVE && k == K_ADT && set == p.set) {
+    // save_soln(q -> qold), adt_calc(x, q' -> adt)
+    op_dat q = pa[0].dat, qold = pa[1].dat;
+    if (dat_in(a[5].dat, {q, qold}) || a[0].dat == qold || a[1].dat == qold ||
+        a[2].dat == qold || a[3].dat == qold || a[4].dat == qold)
+      return false;
+    return run_save_adt(set, pa, a);
+  }
+  if (p.kind == K_AUPDATE && k == K_ADT && set == p.set) {
+    // update(qold, q W, res RW, adt) then adt_calc(x via map, q' = q, adt' = adt)
+    op_dat q = pa[1].dat, res = pa[2].dat, adt = pa[3].dat;
+    if (a[4].dat != q || a[5].dat != adt) return false;
+    for (int i = 0; i < 4; i++)
+      if (dat_in(a[i].dat, {q, res, adt})) return false;
+    return run_update_adt(set, pa, a);
+  }
+  if (p.kind == K_RES && k == K_BRES) {
+    // res_calc(x, q, adt -> res INC), bres_calc(x, q, adt, bound -> res INC)
+    op_dat res = pa[6].dat;
+    if (a[4].dat != res) return false;
+    for (int i : {0, 1, 2, 3, 5})
+      if (a[i].dat == res) return false;
+    return run_res_bres(p.set, pa, set, a);
+  }
+  return false;
+}
+
+// loops that may start a fused pair; update only when its reduction need
+// not reach the host before the call returns
+bool holdable(Kind k) {
+  if (!tuning("fuse", 1)) return false;
+  if (k == K_SAVE) return true;
+  if (k == K_RES)
+    return effective_strategy("res_calc") == OP2B_STRATEGY_GATHER && tuning("gather_flux", 1);
+  if (k == K_AUPDATE) return rt().gbl_deferred && rt().reduction == OP2B_REDUCE_TREE;
+  return false;
+}
+
 }  // namespace
+
+namespace op2b {
+void flush_pending() {
+  if (g_pending.kind == K_NONE) return;
+  Pending p;
+  std::swap(p, g_pending);
+  run_kind(p.kind, 0, p.name.c_str(), p.set, p.args.data());
+}
+}  // namespace op2b
 
 extern "C" {
 
@@ -158,17 +252,30 @@ void op2b_par_loop(char const *name, op_set set, int nargs, const op_arg *args) 
     else printf(" kernel routine with indirection: %s \n", name);
   }
   int v;
-  if (is_res_calc(nargs, args)) return run_res_calc(name, set, args);
-  if (is_adt_calc(nargs, args)) return run_adt_calc(name, set, args);
-  if (is_bres_calc(nargs, args)) return run_bres_calc(name, set, args);
-  if (is_save_soln(nargs, args)) return run_save_soln(name, set, args);
-  if (is_airfoil_update(nargs, args)) return run_airfoil_update(name, set, args);
-  if ((v = jac_res_variant(nargs, args))) return run_jac_res(name, set, args, v);
-  if ((v = jac_update_variant(nargs, args))) return run_jac_update(name, set, args, v);
-  fail(1,
-       "op2b error: no device implementation of loop \"%s\" with this argument signature "
-       "(%d args)\n",
-       name, nargs);
+  Kind k = classify(nargs, args, &v);
+  if (k == K_NONE) {
+    flush_pending();
+    fail(1,
+         "op2b error: no device implementation of loop \"%s\" with this argument signature "
+         "(%d args)\n",
+         name, nargs);
+    return;
+  }
+  if (g_pending.kind != K_NONE) {
+    if (try_fuse(g_pending, k, set, args)) {
+      g_pending = Pending();
+      return;
+    }
+    flush_pending();
+  }
+  if (holdable(k)) {
+    g_pending.kind = k;
+    g_pending.name = name;
+    g_pending.set = set;
+    g_pending.args.assign(args, args + nargs);
+    return;
+  }
+  run_kind(k, v, name, set, args);
 }
 
 // the per-loop entry points of the generated app mains

@@ -66,4 +66,11 @@ void run_airfoil_update(char const *name, op_set set, const op_arg *args);
 void run_jac_res(char const *name, op_set set, const op_arg *args, int variant);
 void run_jac_update(char const *name, op_set set, const op_arg *args, int variant);
 
+// fused loop pairs (airfoil.cu); false = not applicable, run them separately
+bool run_save_adt(op_set set, const op_arg *save_args, const op_arg *adt_args);
+bool run_update_adt(op_set set, const op_arg *update_args, const op_arg *adt_args);
+bool run_res_bres(op_set res_set, const op_arg *res_args, op_set bres_set,
+                  const op_arg *bres_args);
+void release_fused_plans();
+
 }  // namespace op2b
