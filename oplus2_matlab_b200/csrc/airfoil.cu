@@ -21,6 +21,7 @@
 
 #include <algorithm>
 
+#include "launch.cuh"
 #include "loops.h"
 #include "reduce.cuh"
 
@@ -61,6 +62,11 @@ __device__ __forceinline__ void st4(double *p, const double v[4]) {
   reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
 }
 
+// 1/x rounded to nearest: IEEE division of one by x, i.e. the reference's
+// `1.0f/x` on x86, bit for bit, in fewer instructions than a general divide
+__device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
+
 __device__ __forceinline__ int at(const IdxMap &m, int e) {
   return m.map ? __ldg(m.map + m.idx + (size_t)e * m.dim) : e;
 }
@@ -76,7 +82,7 @@ template <class T>
 __device__ __forceinline__ T adt_calc(const T x1[2], const T x2[2], const T x3[2], const T x4[2],
                                       const T q[4], const AirConsts<T> &K) {
   T dx, dy, ri, u, v, c, adt;
-  ri = T(1.0f) / q[0];
+  ri = rcp(q[0]);
   u = ri * q[1];
   v = ri * q[2];
   c = sqrt(K.gam * K.gm1 * (ri * q[3] - T(0.5f) * (u * u + v * v)));
@@ -101,10 +107,10 @@ __device__ __forceinline__ void res_flux(const T x1[2], const T x2[2], const T q
                                          const T q2[4], T adt1, T adt2, T gm1, T eps, T f[4]) {
   T dx = x1[0] - x2[0];
   T dy = x1[1] - x2[1];
-  T ri = T(1.0f) / q1[0];
+  T ri = rcp(q1[0]);
   T p1 = gm1 * (q1[3] - T(0.5f) * ri * (q1[1] * q1[1] + q1[2] * q1[2]));
   T vol1 = ri * (q1[1] * dy - q1[2] * dx);
-  ri = T(1.0f) / q2[0];
+  ri = rcp(q2[0]);
   T p2 = gm1 * (q2[3] - T(0.5f) * ri * (q2[1] * q2[1] + q2[2] * q2[2]));
   T vol2 = ri * (q2[1] * dy - q2[2] * dx);
   T mu = T(0.5f) * (adt1 + adt2) * eps;
@@ -120,7 +126,7 @@ __device__ __forceinline__ void bres_apply(const T x1[2], const T x2[2], const T
                                            int bound, const AirConsts<T> &K, T r[4]) {
   T dx = x1[0] - x2[0];
   T dy = x1[1] - x2[1];
-  T ri = T(1.0f) / q1[0];
+  T ri = rcp(q1[0]);
   T p1 = K.gm1 * (q1[3] - T(0.5f) * ri * (q1[1] * q1[1] + q1[2] * q1[2]));
   if (bound == 1) {
     r[1] += +p1 * dy;
@@ -128,7 +134,7 @@ __device__ __forceinline__ void bres_apply(const T x1[2], const T x2[2], const T
   } else {
     const T *qinf = K.qinf;
     T vol1 = ri * (q1[1] * dy - q1[2] * dx);
-    ri = T(1.0f) / qinf[0];
+    ri = rcp(qinf[0]);
     T p2 = K.gm1 * (qinf[3] - T(0.5f) * ri * (qinf[1] * qinf[1] + qinf[2] * qinf[2]));
     T vol2 = ri * (qinf[1] * dy - qinf[2] * dx);
     T mu = adt1 * K.eps;
@@ -162,6 +168,8 @@ __device__ __forceinline__ void at2(const IdxMap &a, const IdxMap &b, int e, int
 // save_soln: qold = q, U elements per thread issued before any store
 template <class T, int U>
 __global__ void k_save_soln(int n, const T *__restrict__ q, T *__restrict__ qold) {
+  pdl_wait();
+  pdl_trigger();
   const int stride = gridDim.x * blockDim.x;
   for (int base = blockIdx.x * blockDim.x + threadIdx.x; base < n; base += stride * U) {
     T v[U][4];
@@ -188,8 +196,8 @@ __global__ void k_adt_calc(int n, IdxMap m0, IdxMap m1, IdxMap m2, IdxMap m3, Id
   const bool quad = m0.map && m0.map == m1.map && m0.map == m2.map && m0.map == m3.map &&
                     m0.dim == 4 && m0.idx == 0 && m1.idx == 1 && m2.idx == 2 && m3.idx == 3;
   const int stride = gridDim.x * blockDim.x;
-  for (int base = blockIdx.x * blockDim.x + threadIdx.x; base < n; base += stride * U) {
-    int nd[U][4];
+  int nd[U][4];
+  auto nodes = [&](int base) {
 #pragma unroll
     for (int u = 0; u < U; u++) {  // node indices of U cells
       const int c = base + u * stride;
@@ -201,6 +209,13 @@ __global__ void k_adt_calc(int n, IdxMap m0, IdxMap m1, IdxMap m2, IdxMap m3, Id
         nd[u][0] = at(m0, c); nd[u][1] = at(m1, c); nd[u][2] = at(m2, c); nd[u][3] = at(m3, c);
       }
     }
+  };
+  const int base0 = blockIdx.x * blockDim.x + threadIdx.x;
+  nodes(base0);  // map entries: read-only, fetched before the wait
+  pdl_wait();
+  pdl_trigger();
+  for (int base = base0; base < n; base += stride * U) {
+    if (base != base0) nodes(base);
     T xs[U][4][2], qq[U][4];
 #pragma unroll
     for (int u = 0; u < U; u++) {  // then every gather of the U cells
@@ -416,6 +431,259 @@ __global__ void k_res_fold(int nrows, const int *__restrict__ active, const int 
   st4(res + 4 * (size_t)c, r);
 }
 
+// ------------------------------------------------- list-ordered res_calc --
+// res_calc (and bres_calc after it) in two passes over fixed-width
+// contribution lists (SlotPlan).  Pass 1, one thread per edge in edge order
+// (coalesced map reads and stores): the flux f of airfoil/res_calc.h,
+// computed once, into v[e]; one thread per boundary edge: the increment
+// bres_calc adds to its cell, into v[nedge + b].  Pass 2, a direct loop over
+// cells: one load of the cell's list, then its values added in list order
+// (negated for the second cell of an edge) onto res -- the order of
+// op_seq.h running res_calc then bres_calc, so bit-identical.  v is written
+// and re-read while it sits in L2.
+
+// one boundary edge's increment of its cell: bres_apply onto -0.0 gives the
+// exact values bres_calc adds (-0.0 where it adds nothing)
+template <class T>
+__device__ __forceinline__ void bres_contrib(const T x1[2], const T x2[2], const T q1[4], T adt1,
+                                             int bound, const AirConsts<T> &K, T v[4]) {
+  v[0] = v[1] = v[2] = v[3] = T(-0.0);
+  bres_apply(x1, x2, q1, adt1, bound, K, v);
+}
+
+template <class T>
+struct ResEdges {  // res_calc's arguments (airfoil/airfoil_op.cpp:259-267)
+  int n;
+  IdxMap x1, x2, q1, q2, a1, a2;
+  const T *xa, *xb, *qa, *qb, *adta, *adtb;
+};
+template <class T>
+struct BresEdges {  // bres_calc's arguments (airfoil/airfoil_op.cpp:269-276)
+  int n;  // 0: no bres_calc in this pass
+  IdxMap x1, x2, q, a, bound;
+  const T *xa, *xb, *q_d, *adt;
+  const int *bound_d;
+};
+
+__device__ __forceinline__ bool same_map(const IdxMap &a, const IdxMap &b) {
+  return a.map == b.map && a.idx == b.idx && a.dim == b.dim;
+}
+
+template <class T>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4)
+    k_res_flux_list(ResEdges<T> E, BresEdges<T> B, T *__restrict__ v, AirConsts<T> K) {
+  const bool same_a = same_map(E.q1, E.a1) && same_map(E.q2, E.a2);
+  const int total = E.n + B.n;
+  const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  // map entries of this thread's first edge: read-only, fetched before the
+  // previous kernel has finished
+  int n1 = 0, n2 = 0, c1 = 0, c2 = 0, a1 = 0, a2 = 0;
+  auto edge_maps = [&](int e) {
+    at2(E.x1, E.x2, e, n1, n2);
+    at2(E.q1, E.q2, e, c1, c2);
+    if (same_a) {
+      a1 = c1; a2 = c2;
+    } else {
+      at2(E.a1, E.a2, e, a1, a2);
+    }
+  };
+  if (i0 < E.n) edge_maps(i0);
+  pdl_wait();
+  pdl_trigger();
+  for (int i = i0; i < total; i += gridDim.x * blockDim.x) {
+    T f[4];
+    if (i < E.n) {
+      if (i != i0) edge_maps(i);
+      T p[2], s[2], q1[4], q2[4];
+      ld4(E.qa + 4 * (size_t)c1, q1);
+      ld4(E.qb + 4 * (size_t)c2, q2);
+      ld2(E.xa + 2 * (size_t)n1, p);
+      ld2(E.xb + 2 * (size_t)n2, s);
+      const T d1 = __ldg(E.adta + a1), d2 = __ldg(E.adtb + a2);
+      res_flux(p, s, q1, q2, d1, d2, K.gm1, K.eps, f);
+    } else {
+      const int b = i - E.n;
+      int m1, m2;
+      at2(B.x1, B.x2, b, m1, m2);
+      T p[2], s[2], q1[4];
+      ld2(B.xa + 2 * (size_t)m1, p);
+      ld2(B.xb + 2 * (size_t)m2, s);
+      ld4(B.q_d + 4 * (size_t)at(B.q, b), q1);
+      const T b1 = __ldg(B.adt + at(B.a, b));
+      bres_contrib(p, s, q1, b1, __ldg(B.bound_d + at(B.bound, b)), K, f);
+    }
+    st4(v + 4 * (size_t)i, f);
+  }
+}
+
+// r += the listed values of cell c, in list order
+template <class T>
+__device__ __forceinline__ void fold_list(const int *__restrict__ ell, int W,
+                                          const T *__restrict__ v, int c, T r[4]) {
+  for (int j0 = 0; j0 < W; j0 += 4) {
+    int k[4];
+    if (W - j0 >= 4 && ((W & 3) == 0)) {
+      const int4 kk = __ldg(reinterpret_cast<const int4 *>(ell + (size_t)c * W + j0));
+      k[0] = kk.x; k[1] = kk.y; k[2] = kk.z; k[3] = kk.w;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; j++) k[j] = j0 + j < W ? __ldg(ell + (size_t)c * W + j0 + j) : -1;
+    }
+    T f[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (k[j] >= 0) ld4(v + 4 * (size_t)(k[j] >> 1), f[j]);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      if (k[j] < 0) continue;
+      if (k[j] & 1) {
+        r[0] -= f[j][0]; r[1] -= f[j][1]; r[2] -= f[j][2]; r[3] -= f[j][3];
+      } else {
+        r[0] += f[j][0]; r[1] += f[j][1]; r[2] += f[j][2]; r[3] += f[j][3];
+      }
+    }
+  }
+}
+
+template <class T>
+__global__ void k_res_fold_list(int n, const int *__restrict__ ell, int W,
+                                const T *__restrict__ v, T *__restrict__ res) {
+  pdl_wait();
+  pdl_trigger();
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    T r[4];
+    ldw4(res + 4 * (size_t)c, r);
+    fold_list(ell, W, v, c, r);
+    st4(res + 4 * (size_t)c, r);
+  }
+}
+
+// the fold followed by update (airfoil/update.h:1-12) on the same cell and,
+// with ADT, adt_calc on the new q (airfoil/adt_calc.h); update's del^2 go
+// to the tree reduction, or to seq (element order) for the serial fold
+struct CellNodes {  // adt_calc's four x arguments through pcell
+  IdxMap m0, m1, m2, m3;
+};
+// the first min(W, 4) entries of cell c's list; -1 past the end
+__device__ __forceinline__ void list_head(const int *__restrict__ ell, int W, int c, int k[4]) {
+  if ((W & 3) == 0) {
+    const int4 kk = __ldg(reinterpret_cast<const int4 *>(ell + (size_t)c * W));
+    k[0] = kk.x; k[1] = kk.y; k[2] = kk.z; k[3] = kk.w;
+  } else {
+#pragma unroll
+    for (int j = 0; j < 4; j++) k[j] = j < W ? __ldg(ell + (size_t)c * W + j) : -1;
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void add_listed(T r[4], int k, const T f[4]) {
+  if (k < 0) return;
+  if (k & 1) {
+    r[0] -= f[0]; r[1] -= f[1]; r[2] -= f[2]; r[3] -= f[3];
+  } else {
+    r[0] += f[0]; r[1] += f[1]; r[2] += f[2]; r[3] += f[3];
+  }
+}
+
+// U cells per thread: every index load of the U cells, then every data
+// load, then the arithmetic, so up to U cells' gathers are in flight at
+// once; MINB is the launch-bounds occupancy target (register cap)
+template <class T, bool ADT, int U, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+    k_fold_update(int n, const int *__restrict__ ell, int W, const T *__restrict__ vals,
+                  const T *__restrict__ qold, T *__restrict__ q, T *__restrict__ res,
+                  T *__restrict__ adt, CellNodes N, const T *__restrict__ x0,
+                  const T *__restrict__ x1, const T *__restrict__ x2, const T *__restrict__ x3,
+                  AirConsts<T> K, T *seq, RedSlot<T> slot, unsigned *ticket) {
+  const bool quad = N.m0.map && N.m0.map == N.m1.map && N.m0.map == N.m2.map &&
+                    N.m0.map == N.m3.map && N.m0.dim == 4 && N.m0.idx == 0 && N.m1.idx == 1 &&
+                    N.m2.idx == 2 && N.m3.idx == 3;
+  const int stride = gridDim.x * blockDim.x;
+  T rms = T(0);
+  int nd[U][4], k[U][4];
+  // list heads and node indices of U cells: plan and map data (read-only)
+  auto indices = [&](int base) {
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int c = base + u * stride;
+      if (c >= n) continue;
+      list_head(ell, W, c, k[u]);
+      if (ADT) {
+        if (quad) {
+          int4 v = __ldg(reinterpret_cast<const int4 *>(N.m0.map) + c);
+          nd[u][0] = v.x; nd[u][1] = v.y; nd[u][2] = v.z; nd[u][3] = v.w;
+        } else {
+          nd[u][0] = at(N.m0, c); nd[u][1] = at(N.m1, c);
+          nd[u][2] = at(N.m2, c); nd[u][3] = at(N.m3, c);
+        }
+      }
+    }
+  };
+  const int base0 = blockIdx.x * blockDim.x + threadIdx.x;
+  indices(base0);  // before the previous kernel has finished
+  pdl_wait();
+  pdl_trigger();
+  for (int base = base0; base < n; base += stride * U) {
+    if (base != base0) indices(base);
+    T r[U][4], qo[U][4], ad[U], xs[U][4][2], f[U][4][4];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int c = base + u * stride;
+      if (c >= n) continue;
+      ldw4(res + 4 * (size_t)c, r[u]);
+      ld4(qold + 4 * (size_t)c, qo[u]);
+      ad[u] = adt[c];
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (k[u][j] >= 0) ld4(vals + 4 * (size_t)(k[u][j] >> 1), f[u][j]);
+      if (ADT) {
+        ld2(x0 + 2 * (size_t)nd[u][0], xs[u][0]);
+        ld2(x1 + 2 * (size_t)nd[u][1], xs[u][1]);
+        ld2(x2 + 2 * (size_t)nd[u][2], xs[u][2]);
+        ld2(x3 + 2 * (size_t)nd[u][3], xs[u][3]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int c = base + u * stride;
+      if (c >= n) continue;
+#pragma unroll
+      for (int j = 0; j < 4; j++) add_listed(r[u], k[u][j], f[u][j]);
+      for (int j = 4; j < W; j++) {  // lists longer than 4
+        const int kk = __ldg(ell + (size_t)c * W + j);
+        T g[4];
+        ld4(vals + 4 * (size_t)(kk >> 1), g);
+        add_listed(r[u], kk, g);
+      }
+      // airfoil/update.h:1-12
+      T adti = rcp(ad[u]);
+      T qn[4], sq[4];
+      for (int d = 0; d < 4; d++) {
+        T del = adti * r[u][d];
+        qn[d] = qo[u][d] - del;
+        sq[d] = del * del;
+        rms += sq[d];
+      }
+      st4(q + 4 * (size_t)c, qn);
+      const T z[4] = {T(0), T(0), T(0), T(0)};
+      st4(res + 4 * (size_t)c, z);
+      if (seq) st4(seq + 4 * (size_t)c, sq);
+      if (ADT) adt[c] = adt_calc(xs[u][0], xs[u][1], xs[u][2], xs[u][3], qn, K);
+    }
+  }
+  if (seq) return;
+  const T v[1] = {rms}, id[1] = {T(0)};
+  RedSlot<T> sl[1] = {slot};
+  grid_finish<T, OpSum, OpSum, 1>(v, id, OpSum(), OpSum(), sl, ticket);
+}
+
+template <class T>
+__global__ void k_fill(T *p, size_t n, T v) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
 // bres_calc, GATHER: one thread per cell that has boundary edges
 template <class T>
 __global__ void k_bres_calc_gather(int nrows, const int *__restrict__ active,
@@ -579,6 +847,8 @@ template <class T, int U>
 __global__ void k_update(int n, const T *__restrict__ qold, T *__restrict__ q,
                          T *__restrict__ res, const T *__restrict__ adt, T *seq,
                          RedSlot<T> slot, unsigned *ticket) {
+  pdl_wait();
+  pdl_trigger();
   T rms = T(0);
   const int stride = gridDim.x * blockDim.x;
   for (int base = blockIdx.x * blockDim.x + threadIdx.x; base < n; base += stride * U) {
@@ -596,7 +866,7 @@ __global__ void k_update(int n, const T *__restrict__ qold, T *__restrict__ q,
     for (int u = 0; u < U; u++) {
       int c = base + u * stride;
       if (c >= n) continue;
-      T adti = T(1.0f) / ad[u];
+      T adti = rcp(ad[u]);
       T qn[4], sq[4];
       for (int d = 0; d < 4; d++) {
         T del = adti * r[u][d];
@@ -682,9 +952,9 @@ static void save_soln_t(char const *name, op_set set, const op_arg *args) {
   const T *q = (const T *)args[0].dat->data_d;
   T *qold = (T *)args[1].dat->data_d;
   cudaStream_t s = rt().stream;
-  if (U == 1) k_save_soln<T, 1><<<grid_direct(n, 1), 256, 0, s>>>(n, q, qold);
-  else if (U == 2) k_save_soln<T, 2><<<grid_direct(n, 2), 256, 0, s>>>(n, q, qold);
-  else k_save_soln<T, 4><<<grid_direct(n, 4), 256, 0, s>>>(n, q, qold);
+  if (U == 1) launch_pdl(k_save_soln<T, 1>, grid_direct(n, 1), 256, 0, s, n, q, qold);
+  else if (U == 2) launch_pdl(k_save_soln<T, 2>, grid_direct(n, 2), 256, 0, s, n, q, qold);
+  else launch_pdl(k_save_soln<T, 4>, grid_direct(n, 4), 256, 0, s, n, q, qold);
 }
 void run_save_soln(char const *name, op_set set, const op_arg *args) {
   if (is_double(args[0])) save_soln_t<double>(name, set, args);
@@ -699,11 +969,11 @@ static void adt_calc_t(char const *name, op_set set, const op_arg *args) {
   int n = set->size;
   const int U = tuning("adt_unroll", 1) >= 2 ? 2 : 1;
   auto launch = [&](auto kernel, int u) {
-    kernel<<<grid_direct(n, u), 256, 0, rt().stream>>>(
-        n, idx_map(args[0]), idx_map(args[1]), idx_map(args[2]), idx_map(args[3]),
-        idx_map(args[4]), (const T *)args[0].dat->data_d, (const T *)args[1].dat->data_d,
-        (const T *)args[2].dat->data_d, (const T *)args[3].dat->data_d,
-        (const T *)args[4].dat->data_d, (T *)args[5].dat->data_d, K);
+    launch_pdl(kernel, grid_direct(n, u), 256, 0, rt().stream, n, idx_map(args[0]),
+               idx_map(args[1]), idx_map(args[2]), idx_map(args[3]), idx_map(args[4]),
+               (const T *)args[0].dat->data_d, (const T *)args[1].dat->data_d,
+               (const T *)args[2].dat->data_d, (const T *)args[3].dat->data_d,
+               (const T *)args[4].dat->data_d, (T *)args[5].dat->data_d, K);
   };
   if (U == 2) launch(k_adt_calc<T, 2>, 2);
   else launch(k_adt_calc<T, 1>, 1);
@@ -740,6 +1010,9 @@ static void res_calc_t(char const *name, op_set set, const op_arg *args) {
   }
   GatherPlan *g = get_gather_plan(set, args, {6, 7});
   if (!g) return;
+  if (tuning("gather_flux", 1) && tuning("gather_slots", 1) &&
+      run_res_chain(name, set, args, nullptr, nullptr, nullptr, nullptr))
+    return;
   LoopScope ls(name, compulsory_bytes(set, 8, args), 0);
   if (g->nactive == 0) return;
   if (tuning("gather_flux", 1)) {
@@ -851,12 +1124,12 @@ static void update_t(char const *name, op_set set, const op_arg *args) {
     RedSlot<T> rslot{(T *)red_partials(0), result};
     const T *qold = (const T *)args[0].dat->data_d, *adt = (const T *)args[3].dat->data_d;
     T *q = (T *)args[1].dat->data_d, *res = (T *)args[2].dat->data_d;
-    if (U == 1)
-      k_update<T, 1><<<grid, threads, 0, s>>>(n, qold, q, res, adt, seqbuf, rslot, red_ticket());
-    else if (U == 2)
-      k_update<T, 2><<<grid, threads, 0, s>>>(n, qold, q, res, adt, seqbuf, rslot, red_ticket());
-    else
-      k_update<T, 4><<<grid, threads, 0, s>>>(n, qold, q, res, adt, seqbuf, rslot, red_ticket());
+    auto launch = [&](auto kernel) {
+      launch_pdl(kernel, grid, threads, 0, s, n, qold, q, res, adt, seqbuf, rslot, red_ticket());
+    };
+    if (U == 1) launch(k_update<T, 1>);
+    else if (U == 2) launch(k_update<T, 2>);
+    else launch(k_update<T, 4>);
     if (seq) {
       T init = *(const T *)args[4].data;
       k_seq_sum<T><<<1, 32, 0, s>>>(seqbuf, 4LL * n, init, result);
@@ -885,14 +1158,21 @@ __global__ void k_save_adt(int n, const T *__restrict__ q, T *__restrict__ qold,
                            T *__restrict__ adt, AirConsts<T> K) {
   const bool quad = m0.map && m0.map == m1.map && m0.map == m2.map && m0.map == m3.map &&
                     m0.dim == 4 && m0.idx == 0 && m1.idx == 1 && m2.idx == 2 && m3.idx == 3;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-    int nd[4];
+  int nd[4];
+  auto nodes = [&](int c) {
     if (quad) {
       int4 v = __ldg(reinterpret_cast<const int4 *>(m0.map) + c);
       nd[0] = v.x; nd[1] = v.y; nd[2] = v.z; nd[3] = v.w;
     } else {
       nd[0] = at(m0, c); nd[1] = at(m1, c); nd[2] = at(m2, c); nd[3] = at(m3, c);
     }
+  };
+  const int c0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c0 < n) nodes(c0);  // map entries: read-only, fetched early
+  pdl_wait();
+  pdl_trigger();
+  for (int c = c0; c < n; c += gridDim.x * blockDim.x) {
+    if (c != c0) nodes(c);
     T qq[4], qa[4], a[2], b[2], d[2], e[2];
     ld4(q + 4 * (size_t)c, qq);
     if (q2 != q) ld4(q2 + 4 * (size_t)c, qa);
@@ -916,6 +1196,8 @@ __global__ void k_update_adt(int n, const T *__restrict__ qold, T *__restrict__ 
                              unsigned *ticket) {
   const bool quad = m0.map && m0.map == m1.map && m0.map == m2.map && m0.map == m3.map &&
                     m0.dim == 4 && m0.idx == 0 && m1.idx == 1 && m2.idx == 2 && m3.idx == 3;
+  pdl_wait();
+  pdl_trigger();
   T rms = T(0);
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
     int nd[4];
@@ -934,7 +1216,7 @@ __global__ void k_update_adt(int n, const T *__restrict__ qold, T *__restrict__ 
     ld2(x2 + 2 * (size_t)nd[2], d);
     ld2(x3 + 2 * (size_t)nd[3], e);
     // airfoil/update.h:1-12
-    T adti = T(1.0f) / ad;
+    T adti = rcp(ad);
     T qn[4];
     for (int k = 0; k < 4; k++) {
       T del = adti * r[k];
@@ -1018,11 +1300,12 @@ static bool save_adt_t(op_set set, const op_arg *sa, const op_arg *aa) {
   if (error_pending()) return true;
   LoopScope ls("save_soln+adt_calc", compulsory_bytes(set, 2, sa) + compulsory_bytes(set, 6, aa), 0);
   const int n = set->size;
-  k_save_adt<T><<<grid_for(n, 256), 256, 0, rt().stream>>>(
-      n, (const T *)sa[0].dat->data_d, (T *)sa[1].dat->data_d, idx_map(aa[0]), idx_map(aa[1]),
-      idx_map(aa[2]), idx_map(aa[3]), (const T *)aa[0].dat->data_d,
-      (const T *)aa[1].dat->data_d, (const T *)aa[2].dat->data_d,
-      (const T *)aa[3].dat->data_d, (const T *)aa[4].dat->data_d, (T *)aa[5].dat->data_d, K);
+  launch_pdl(k_save_adt<T>, grid_for(n, 256), 256, 0, rt().stream, n,
+             (const T *)sa[0].dat->data_d, (T *)sa[1].dat->data_d, idx_map(aa[0]), idx_map(aa[1]),
+             idx_map(aa[2]), idx_map(aa[3]), (const T *)aa[0].dat->data_d,
+             (const T *)aa[1].dat->data_d, (const T *)aa[2].dat->data_d,
+             (const T *)aa[3].dat->data_d, (const T *)aa[4].dat->data_d, (T *)aa[5].dat->data_d,
+             K);
   return true;
 }
 
@@ -1044,11 +1327,12 @@ static bool update_adt_t(op_set set, const op_arg *ua, const op_arg *aa) {
     long long gcap = (long long)rt().num_sms * tuning("update_ctas_per_sm", 4);
     const int grid = (int)std::max(1LL, std::min(gw, std::min(gcap, (long long)kMaxRedBlocks)));
     RedSlot<T> rslot{(T *)red_partials(0), result};
-    k_update_adt<T><<<grid, 256, 0, s>>>(
-        n, (const T *)ua[0].dat->data_d, (T *)ua[1].dat->data_d, (T *)ua[2].dat->data_d,
-        (T *)ua[3].dat->data_d, idx_map(aa[0]), idx_map(aa[1]), idx_map(aa[2]), idx_map(aa[3]),
-        (const T *)aa[0].dat->data_d, (const T *)aa[1].dat->data_d,
-        (const T *)aa[2].dat->data_d, (const T *)aa[3].dat->data_d, K, rslot, red_ticket());
+    launch_pdl(k_update_adt<T>, grid, 256, 0, s, n, (const T *)ua[0].dat->data_d,
+               (T *)ua[1].dat->data_d, (T *)ua[2].dat->data_d, (T *)ua[3].dat->data_d,
+               idx_map(aa[0]), idx_map(aa[1]), idx_map(aa[2]), idx_map(aa[3]),
+               (const T *)aa[0].dat->data_d, (const T *)aa[1].dat->data_d,
+               (const T *)aa[2].dat->data_d, (const T *)aa[3].dat->data_d, K, rslot,
+               red_ticket());
   }
   red_finish({GblRequest{ua[4].data, slot, OP_INC, sizeof(T) == 8 ? GBL_F64 : GBL_F32, false}});
   return true;
@@ -1120,8 +1404,133 @@ static bool res_bres_t(op_set rset, const op_arg *ra, op_set bset, const op_arg 
 }
 
 bool run_res_bres(op_set rset, const op_arg *ra, op_set bset, const op_arg *ba) {
+  if (tuning("gather_slots", 1) &&
+      run_res_chain(nullptr, rset, ra, bset, ba, nullptr, nullptr))
+    return true;
   return is_double(ra[0]) ? res_bres_t<double>(rset, ra, bset, ba)
                           : res_bres_t<float>(rset, ra, bset, ba);
+}
+
+// res_calc [+ bres_calc [+ update [+ adt_calc]]] over contribution lists:
+// the flux pass, then one per-cell pass that folds the cell's list and, when
+// update follows, applies it (and adt_calc) to the cell before storing
+template <class T>
+static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op_set bset,
+                        const op_arg *ba, const op_arg *ua, const op_arg *aa) {
+  AirConsts<T> K = air_consts<T>();
+  if (error_pending()) return true;
+  cudaStream_t s = rt().stream;
+  GatherPlan *g = get_gather_plan(rset, ra, {6, 7});
+  GatherPlan *gb = ba ? get_gather_plan(bset, ba, {4}) : nullptr;
+  if (!g || (ba && !gb)) return true;
+  SlotPlan *sp = get_slot_plan(g, gb);
+  if (!sp) return false;
+  const int W = sp->width, ncell = sp->ntarget;
+  const size_t nval = (size_t)sp->na + sp->nb + 1;
+  const size_t need = sizeof(T) * 4 * nval;
+  if (sp->buf_bytes < need) {
+    dev_free(sp->d_buf);
+    sp->d_buf = dev_alloc(need);
+    sp->buf_bytes = sp->d_buf ? need : 0;
+    if (!sp->d_buf) return true;
+    // the padding entry, never written by the flux pass: -0.0
+    k_fill<T><<<1, 32, 0, s>>>((T *)sp->d_buf + 4 * (nval - 1), 4, T(-0.0));
+  }
+  T *vals = (T *)sp->d_buf;
+
+  std::string name = loop_name ? loop_name : "res_calc";
+  double bytes = compulsory_bytes(rset, 8, ra);
+  if (ba) name += "+bres_calc", bytes += compulsory_bytes(bset, 6, ba);
+  if (ua) name += "+update", bytes += compulsory_bytes(ra[6].dat->set, 5, ua);
+  if (aa) name += "+adt_calc", bytes += compulsory_bytes(ra[6].dat->set, 6, aa);
+  const bool seq = ua && rt().reduction == OP2B_REDUCE_SEQ;
+  int rslot_id = ua ? red_new_slot() : -1;
+  {
+    LoopScope ls(name.c_str(), bytes, 0);
+    ResEdges<T> E{rset->size, idx_map(ra[0]), idx_map(ra[1]), idx_map(ra[2]), idx_map(ra[3]),
+                  idx_map(ra[4]), idx_map(ra[5]), (const T *)ra[0].dat->data_d,
+                  (const T *)ra[1].dat->data_d, (const T *)ra[2].dat->data_d,
+                  (const T *)ra[3].dat->data_d, (const T *)ra[4].dat->data_d,
+                  (const T *)ra[5].dat->data_d};
+    BresEdges<T> B;
+    memset(&B, 0, sizeof B);
+    if (ba)
+      B = BresEdges<T>{bset->size, idx_map(ba[0]), idx_map(ba[1]), idx_map(ba[2]),
+                       idx_map(ba[3]), idx_map(ba[5]), (const T *)ba[0].dat->data_d,
+                       (const T *)ba[1].dat->data_d, (const T *)ba[2].dat->data_d,
+                       (const T *)ba[3].dat->data_d, (const int *)ba[5].dat->data_d};
+    const long long nflux = (long long)E.n + B.n;
+    {
+      PhaseScope ph(name + ":flux");
+      // flux_ctas_per_sm = 0: one edge per thread (many short CTAs balance
+      // the SMs); n > 0: at most n CTAs per SM, grid-stride
+      const int per_sm = tuning("flux_ctas_per_sm", 16);
+      long long fg = (nflux + 255) / 256;
+      if (per_sm > 0) fg = std::min(fg, (long long)rt().num_sms * per_sm);
+      launch_pdl(k_res_flux_list<T>, (unsigned)std::max(1LL, fg), 256, 0, s, E, B, vals, K);
+    }
+    PhaseScope ph(name + ":fold");
+    T *res = (T *)ra[6].dat->data_d;
+    if (!ua) {
+      launch_pdl(k_res_fold_list<T>, grid_for(ncell, 256), 256, 0, s, ncell,
+                 (const int *)sp->d_ell, W, (const T *)vals, res);
+    } else {
+      T *seqbuf = seq ? (T *)red_seq_buffer(sizeof(T) * 4 * (size_t)ncell) : nullptr;
+      // a few waves of grid-stride CTAs (fewer, longer CTAs beat one cell
+      // per thread: each CTA ends with a block reduction and a ticket):
+      // measured best at 4 CTAs per SM for the fold + update (one wave at
+      // its occupancy) and 6 with adt_calc; fixed by ncell, so sums
+      // reproduce.  0: one cell per thread
+      long long gw = (ncell + 255LL) / 256;
+      const int per_sm = aa ? tuning("fold_adt_ctas_per_sm", 6) : tuning("fold_ctas_per_sm", 4);
+      long long gcap = per_sm > 0 ? (long long)rt().num_sms * per_sm : (long long)kMaxRedBlocks;
+      const int grid = (int)std::max(1LL, std::min(gw, std::min(gcap, (long long)kMaxRedBlocks)));
+      T *result = (T *)red_slot_ptr(rslot_id);
+      RedSlot<T> rslot{(T *)red_partials(0), result};
+      const T *qold = (const T *)ua[0].dat->data_d;
+      T *q = (T *)ua[1].dat->data_d, *adt = (T *)ua[3].dat->data_d;
+      CellNodes N;
+      memset(&N, 0, sizeof N);
+      const T *xs[4] = {nullptr, nullptr, nullptr, nullptr};
+      if (aa) {
+        N = CellNodes{idx_map(aa[0]), idx_map(aa[1]), idx_map(aa[2]), idx_map(aa[3])};
+        for (int i = 0; i < 4; i++) xs[i] = (const T *)aa[i].dat->data_d;
+      }
+      // fold_variant: 0 one cell per thread at >= 4 CTAs per SM (3 with
+      // adt_calc); 1 the same at >= 6; 2 two cells per thread; 3 two cells
+      // at >= 3 CTAs per SM
+      auto launch = [&](auto kernel) {
+        launch_pdl(kernel, grid, 256, 0, s, ncell, (const int *)sp->d_ell, W, (const T *)vals,
+                   qold, q, res, adt, N, xs[0], xs[1], xs[2], xs[3], K, seqbuf, rslot,
+                   red_ticket());
+      };
+      const int fv = tuning("fold_variant", 0);
+      if (aa) {
+        if (fv == 1) launch(k_fold_update<T, true, 1, 6>);
+        else if (fv == 2) launch(k_fold_update<T, true, 2, 1>);
+        else if (fv == 3) launch(k_fold_update<T, true, 2, 3>);
+        else launch(k_fold_update<T, true, 1, sizeof(T) == 4 ? 3 : 2>);
+      } else {
+        if (fv == 1) launch(k_fold_update<T, false, 1, 6>);
+        else if (fv == 2) launch(k_fold_update<T, false, 2, 1>);
+        else if (fv == 3) launch(k_fold_update<T, false, 2, 3>);
+        else launch(k_fold_update<T, false, 1, sizeof(T) == 4 ? 4 : 2>);
+      }
+      if (seq) {
+        T init = *(const T *)ua[4].data;
+        k_seq_sum<T><<<1, 32, 0, s>>>(seqbuf, 4LL * ncell, init, result);
+      }
+    }
+  }
+  if (ua)
+    red_finish({GblRequest{ua[4].data, rslot_id, OP_INC, sizeof(T) == 8 ? GBL_F64 : GBL_F32, seq}});
+  return true;
+}
+
+bool run_res_chain(char const *name, op_set rset, const op_arg *ra, op_set bset,
+                   const op_arg *ba, const op_arg *ua, const op_arg *aa) {
+  return is_double(ra[0]) ? res_chain_t<double>(name, rset, ra, bset, ba, ua, aa)
+                          : res_chain_t<float>(name, rset, ra, bset, ba, ua, aa);
 }
 
 }  // namespace op2b

@@ -126,6 +126,20 @@ LoopScope::~LoopScope() {
   else t->pending.push_back(ev);
 }
 
+PhaseScope::PhaseScope(const std::string &name) : name_(name) {
+  Runtime &R = rt();
+  if (!R.capture_profile || !capturing()) return;
+  OP2B_CUDA(cudaEventCreate(&a_));
+  OP2B_CUDA(cudaEventCreate(&b_));
+  OP2B_CUDA(cudaEventRecordWithFlags(a_, R.stream, cudaEventRecordExternal));
+}
+
+PhaseScope::~PhaseScope() {
+  if (!a_) return;
+  cudaEventRecordWithFlags(b_, rt().stream, cudaEventRecordExternal);
+  rt().capture_events.push_back({name_, a_, b_});
+}
+
 void flush_timers() {
   Runtime &R = rt();
   for (auto &kv : R.timers) {

@@ -132,6 +132,17 @@ struct LoopScope {
 };
 void flush_timers();  // harvest finished event pairs into OP_kernels
 
+// event pair around one kernel of a fused loop chain, recorded only inside a
+// profiled graph capture (it adds no entry to the op_timing_output table)
+struct PhaseScope {
+  explicit PhaseScope(const std::string &name);
+  ~PhaseScope();
+
+ private:
+  std::string name_;
+  cudaEvent_t a_ = nullptr, b_ = nullptr;
+};
+
 // constants lookup: copies up to n values of the named constant into out,
 // converted to T; returns the number found (0 if never declared)
 int const_get_f32(char const *name, float *out, int n);

@@ -156,14 +156,15 @@ void run_kind(Kind k, int variant, char const *name, op_set set, const op_arg *a
   }
 }
 
-// The loop held back in case the next call can be fused with it.
-struct Pending {
+// The loops held back in case the next call can be fused with them: one of
+// save_soln, update, res_calc; res_calc+bres_calc; res_calc+bres_calc+update.
+struct Held {
   Kind kind = K_NONE;
   std::string name;
   op_set set = nullptr;
   std::vector<op_arg> args;
 };
-Pending g_pending;
+std::vector<Held> g_chain;
 
 bool dat_in(op_dat d, std::initializer_list<op_dat> ds) {
   for (op_dat x : ds)
@@ -171,46 +172,129 @@ bool dat_in(op_dat d, std::initializer_list<op_dat> ds) {
   return false;
 }
 
-// Can `next` run fused with the held-back loop?  Each case checks that the
-// second loop reads nothing the first writes, except at the same element,
-// and writes nothing the first reads elsewhere.
-bool try_fuse(const Pending &p, Kind k, op_set set, const op_arg *a) {
-  const op_arg *pa = p.args.data();
-  if (p.kind == K_SAVE && k == K_ADT && set == p.set) {
+// update(qold, q W, res RW, adt) then adt_calc(x via map, q' = q, adt' = adt)
+bool adt_follows_update(const op_arg *u, op_set uset, op_set set, const op_arg *a) {
+  op_dat q = u[1].dat, res = u[2].dat, adt = u[3].dat;
+  if (set != uset || a[4].dat != q || a[5].dat != adt) return false;
+  for (int i = 0; i < 4; i++)
+    if (dat_in(a[i].dat, {q, res, adt})) return false;
+  return true;
+}
+
+// res_calc(x, q, adt -> res INC), bres_calc(x, q, adt, bound -> res INC)
+bool bres_follows_res(const op_arg *r, const op_arg *b) {
+  op_dat res = r[6].dat;
+  if (b[4].dat != res) return false;
+  for (int i : {0, 1, 2, 3, 5})
+    if (b[i].dat == res) return false;
+  return true;
+}
+
+// update(qold, q, res, adt) on the cells res_calc/bres_calc increment: it
+// reads their result only at its own cell and writes nothing they read
+// (their reads all finish in the flux pass, before update's pass starts)
+bool update_follows_res(const op_arg *r, op_set set, const op_arg *u) {
+  op_dat res = r[6].dat;
+  return set == res->set && u[2].dat == res && u[0].dat != res && u[1].dat != res &&
+         u[3].dat != res;
+}
+
+// the update may wait for the next call only when its reduction need not
+// reach the host before its own call returns
+bool update_holdable() { return rt().gbl_deferred && rt().reduction == OP2B_REDUCE_TREE; }
+
+bool res_holdable() {
+  return effective_strategy("res_calc") == OP2B_STRATEGY_GATHER && tuning("gather_flux", 1);
+}
+
+// run a chain, fused as far as the kernels allow
+void run_chain(const std::vector<Held> &ch, const Held *adt) {
+  const Held &h0 = ch[0];
+  const op_arg *a0 = h0.args.data();
+  if (ch.size() == 1) {
+    if (adt && h0.kind == K_SAVE && run_save_adt(h0.set, a0, adt->args.data())) return;
+    if (adt && h0.kind == K_AUPDATE && run_update_adt(h0.set, a0, adt->args.data())) return;
+    run_kind(h0.kind, 0, h0.name.c_str(), h0.set, a0);
+  } else {
+    const Held &h1 = ch[1];
+    const Held *u = ch.size() > 2 ? &ch[2] : nullptr;
+    if (u && tuning("gather_slots", 1) &&
+        run_res_chain(nullptr, h0.set, a0, h1.set, h1.args.data(), u->args.data(),
+                      adt ? adt->args.data() : nullptr))
+      return;
+    if (!run_res_bres(h0.set, a0, h1.set, h1.args.data())) {
+      run_kind(h0.kind, 0, h0.name.c_str(), h0.set, a0);
+      run_kind(h1.kind, 0, h1.name.c_str(), h1.set, h1.args.data());
+    }
+    if (u) {
+      if (adt && run_update_adt(u->set, u->args.data(), adt->args.data())) return;
+      run_kind(u->kind, 0, u->name.c_str(), u->set, u->args.data());
+    }
+  }
+  if (adt) run_kind(adt->kind, 0, adt->name.c_str(), adt->set, adt->args.data());
+}
+
+Held make_held(Kind k, char const *name, op_set set, int nargs, const op_arg *args) {
+  Held h;
+  h.kind = k;
+  h.name = name;
+  h.set = set;
+  h.args.assign(args, args + nargs);
+  return h;
+}
+
+// Offer the next loop to the held chain.  Returns true when it was taken
+// (held or run fused); false when the caller must flush and run it.
+bool extend_chain(Kind k, char const *name, op_set set, int nargs, const op_arg *a) {
+  if (g_chain.empty()) return false;
+  const Held &h0 = g_chain[0];
+  const op_arg *pa = h0.args.data();
+  const size_t n = g_chain.size();
+  if (n == 1 && h0.kind == K_SAVE && k == K_ADT && set == h0.set) {
     // save_soln(q -> qold), adt_calc(x, q' -> adt)
     op_dat q = pa[0].dat, qold = pa[1].dat;
     if (dat_in(a[5].dat, {q, qold}) || a[0].dat == qold || a[1].dat == qold ||
         a[2].dat == qold || a[3].dat == qold || a[4].dat == qold)
       return false;
-    return run_save_adt(set, pa, a);
+    Held adt = make_held(k, name, set, nargs, a);
+    std::vector<Held> ch;
+    std::swap(ch, g_chain);
+    run_chain(ch, &adt);
+    return true;
   }
-  if (p.kind == K_AUPDATE && k == K_ADT && set == p.set) {
-    // update(qold, q W, res RW, adt) then adt_calc(x via map, q' = q, adt' = adt)
-    op_dat q = pa[1].dat, res = pa[2].dat, adt = pa[3].dat;
-    if (a[4].dat != q || a[5].dat != adt) return false;
-    for (int i = 0; i < 4; i++)
-      if (dat_in(a[i].dat, {q, res, adt})) return false;
-    return run_update_adt(set, pa, a);
+  if (n == 1 && h0.kind == K_AUPDATE && k == K_ADT && adt_follows_update(pa, h0.set, set, a)) {
+    Held adt = make_held(k, name, set, nargs, a);
+    std::vector<Held> ch;
+    std::swap(ch, g_chain);
+    run_chain(ch, &adt);
+    return true;
   }
-  if (p.kind == K_RES && k == K_BRES) {
-    // res_calc(x, q, adt -> res INC), bres_calc(x, q, adt, bound -> res INC)
-    op_dat res = pa[6].dat;
-    if (a[4].dat != res) return false;
-    for (int i : {0, 1, 2, 3, 5})
-      if (a[i].dat == res) return false;
-    return run_res_bres(p.set, pa, set, a);
+  if (n == 1 && h0.kind == K_RES && k == K_BRES && bres_follows_res(pa, a)) {
+    g_chain.push_back(make_held(k, name, set, nargs, a));
+    if (!tuning("fuse_update", 1) || !tuning("gather_slots", 1)) flush_pending();
+    return true;
+  }
+  if (n == 2 && k == K_AUPDATE && update_follows_res(pa, set, a)) {
+    g_chain.push_back(make_held(k, name, set, nargs, a));
+    if (!update_holdable()) flush_pending();
+    return true;
+  }
+  if (n == 3 && k == K_ADT && adt_follows_update(g_chain[2].args.data(), g_chain[2].set, set, a)) {
+    Held adt = make_held(k, name, set, nargs, a);
+    std::vector<Held> ch;
+    std::swap(ch, g_chain);
+    run_chain(ch, &adt);
+    return true;
   }
   return false;
 }
 
-// loops that may start a fused pair; update only when its reduction need
-// not reach the host before the call returns
+// loops that may start a chain
 bool holdable(Kind k) {
   if (!tuning("fuse", 1)) return false;
   if (k == K_SAVE) return true;
-  if (k == K_RES)
-    return effective_strategy("res_calc") == OP2B_STRATEGY_GATHER && tuning("gather_flux", 1);
-  if (k == K_AUPDATE) return rt().gbl_deferred && rt().reduction == OP2B_REDUCE_TREE;
+  if (k == K_RES) return res_holdable();
+  if (k == K_AUPDATE) return update_holdable();
   return false;
 }
 
@@ -218,10 +302,10 @@ bool holdable(Kind k) {
 
 namespace op2b {
 void flush_pending() {
-  if (g_pending.kind == K_NONE) return;
-  Pending p;
-  std::swap(p, g_pending);
-  run_kind(p.kind, 0, p.name.c_str(), p.set, p.args.data());
+  if (g_chain.empty()) return;
+  std::vector<Held> ch;
+  std::swap(ch, g_chain);
+  run_chain(ch, nullptr);
 }
 }  // namespace op2b
 
@@ -261,18 +345,12 @@ void op2b_par_loop(char const *name, op_set set, int nargs, const op_arg *args) 
          name, nargs);
     return;
   }
-  if (g_pending.kind != K_NONE) {
-    if (try_fuse(g_pending, k, set, args)) {
-      g_pending = Pending();
-      return;
-    }
+  if (!g_chain.empty()) {
+    if (extend_chain(k, name, set, nargs, args)) return;
     flush_pending();
   }
   if (holdable(k)) {
-    g_pending.kind = k;
-    g_pending.name = name;
-    g_pending.set = set;
-    g_pending.args.assign(args, args + nargs);
+    g_chain.push_back(make_held(k, name, set, nargs, args));
     return;
   }
   run_kind(k, v, name, set, args);

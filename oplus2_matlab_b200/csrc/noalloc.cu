@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(256) k_update_noalloc(int n, const float *__re
   for (int u = 0; u < 4; u++) {
     int c = base + u * stride;
     if (c >= n) continue;
-    float adti = 1.0f / ad[u];
+    float adti = __frcp_rn(ad[u]);  // IEEE 1/x, as 1.0f/x on x86
     float qn[4];
     for (int d = 0; d < 4; d++) {
       float del = adti * r[u][d];
@@ -80,10 +80,11 @@ __global__ void __launch_bounds__(256) k_update_noalloc(int n, const float *__re
   __shared__ float ws[32];
   __shared__ bool last;
   float b = op2b::block_fold(sum, 0.0f, op2b::OpSum(), ws);
-  if (threadIdx.x == 0) partials[blockIdx.x] = b;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  if (threadIdx.x == 0) {  // the writer fences its partial, then takes a ticket
+    partials[blockIdx.x] = b;
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
   __syncthreads();
   if (!last) return;
   __threadfence();

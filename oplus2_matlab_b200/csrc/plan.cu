@@ -1156,11 +1156,103 @@ GatherPlan *get_gather_plan(op_set set, const op_arg *args, const std::vector<in
   return g_gather.back().get();
 }
 
+// ------------------------------------------------------------- slot plan --
+
+// contributions per target of plan a (cnt = row length) and then of b
+__global__ void k_ell_count(int nrows, const int *active, const int *row, int *cnt) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nrows; t += gridDim.x * blockDim.x)
+    cnt[active ? active[t] : t] += row[t + 1] - row[t];
+}
+
+// write plan a's entries (its CSR keys are already edge << 1 | slot), or
+// plan b's ((na + key) << 1) after a's; cnt is the fill level per target
+__global__ void k_ell_fill(int nrows, const int *active, const int *row, const int *keys,
+                           int width, int offset, int shift, int *cnt, int *ell) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nrows; t += gridDim.x * blockDim.x) {
+    const int c = active ? active[t] : t;
+    const int k0 = row[t], k1 = row[t + 1], base = cnt[c];
+    for (int k = k0; k < k1; k++)
+      ell[(size_t)c * width + base + (k - k0)] = (offset + keys[k]) << shift;
+    cnt[c] = base + k1 - k0;
+  }
+}
+
+__global__ void k_max_int(const int *v, int n, int *out) {
+  int m = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    m = max(m, v[i]);
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+__global__ void k_fill_int(int *p, size_t n, int v) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+static std::vector<std::unique_ptr<SlotPlan>> g_slot_plans;
+
+SlotPlan *get_slot_plan(const GatherPlan *a, const GatherPlan *b) {
+  for (auto &up : g_slot_plans)
+    if (up->a == a && up->b == b) return up->width > 0 ? up.get() : nullptr;
+  std::unique_ptr<SlotPlan> up(new SlotPlan());
+  SlotPlan &p = *up;
+  p.a = a;
+  p.b = b;
+  p.ntarget = a->ntarget;
+  p.na = a->set->size;
+  p.nb = b ? b->set->size : 0;
+  const bool shape = a->nslots == 2 && (!b || (b->nslots == 1 && b->ntarget == a->ntarget)) &&
+                     (long long)p.na + p.nb + 1 < (1LL << 30);
+  if (shape && a->nactive > 0) {
+    cudaStream_t s = rt().stream;
+    const int grid = rt().num_sms * 8;
+    int *cnt = nullptr;
+    OP2B_CUDA(cudaMallocAsync((void **)&cnt, sizeof(int) * ((size_t)p.ntarget + 1), s));
+    int *mx = cnt + p.ntarget;
+    OP2B_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)p.ntarget + 1), s));
+    k_ell_count<<<grid, 256, 0, s>>>(a->nactive, a->d_active, a->d_row, cnt);
+    if (b && b->nactive) k_ell_count<<<grid, 256, 0, s>>>(b->nactive, b->d_active, b->d_row, cnt);
+    k_max_int<<<grid, 256, 0, s>>>(cnt, p.ntarget, mx);
+    int w = 0;
+    OP2B_CUDA(cudaMemcpyAsync(&w, mx, sizeof(int), cudaMemcpyDeviceToHost, s));
+    OP2B_CUDA(cudaStreamSynchronize(s));
+    const long long nkeys = a->nkeys + (b ? b->nkeys : 0);
+    if (w >= 1 && w <= kMaxSlotWidth && (long long)w * p.ntarget <= 2 * nkeys + p.ntarget) {
+      p.width = w;
+      const size_t n = (size_t)w * p.ntarget;
+      p.d_ell = (int *)dev_alloc(sizeof(int) * n);
+      if (!p.d_ell) {
+        p.width = 0;
+      } else {
+        k_fill_int<<<grid, 256, 0, s>>>(p.d_ell, n, (p.na + p.nb) << 1);
+        OP2B_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)p.ntarget, s));
+        k_ell_fill<<<grid, 256, 0, s>>>(a->nactive, a->d_active, a->d_row, a->d_keys, w, 0, 0,
+                                        cnt, p.d_ell);
+        if (b && b->nactive)
+          k_ell_fill<<<grid, 256, 0, s>>>(b->nactive, b->d_active, b->d_row, b->d_keys, w, p.na,
+                                          1, cnt, p.d_ell);
+      }
+    }
+    OP2B_CUDA(cudaFreeAsync(cnt, s));
+    OP2B_CUDA(cudaStreamSynchronize(s));
+  }
+  g_slot_plans.push_back(std::move(up));
+  SlotPlan *r = g_slot_plans.back().get();
+  return r->width > 0 ? r : nullptr;
+}
+
 }  // namespace op2b
 
 using namespace op2b;
 
 void op2b_release_plans() {
+  for (auto &up : g_slot_plans) {
+    dev_free(up->d_ell);
+    dev_free(up->d_buf);
+  }
+  g_slot_plans.clear();
   for (auto &up : g_plans) {
     DevPlan &p = *up;
     dev_free(p.d_nthrcol); dev_free(p.d_thrcol); dev_free(p.d_offset); dev_free(p.d_nelems);

@@ -70,6 +70,34 @@ struct GatherPlan {
 // contributions per CTA tile of the contribution-parallel gather kernels
 constexpr int kTile = 256;
 
+// Fixed-width (ELL) contribution lists for an edge loop `a` with two
+// increment arguments (slot 0 adds the edge's value, slot 1 subtracts it),
+// optionally followed by a loop `b` with one (adds): the kernels store one
+// value per edge of a in v[0, na), one per element of b in v[na, na+nb),
+// and -0.0 in v[na+nb].  Target t owns entries ell[t*width, (t+1)*width):
+// (index << 1 | negate) of its contributions, a's in a's ascending order
+// then b's in b's order, padded with (na+nb) << 1.  Adding the entries in
+// list order is the order of the sequential back-end running a then b;
+// -0.0 is the exact identity of IEEE addition and r + (-v) equals r - v.
+struct SlotPlan {
+  const GatherPlan *a = nullptr, *b = nullptr;
+  int ntarget = 0;
+  int width = 0;            // max contributions of one target
+  int na = 0, nb = 0;       // elements of a and b
+  int *d_ell = nullptr;     // [ntarget * width]
+  void *d_buf = nullptr;    // the (na + nb + 1) values, allocated by the loop
+  size_t buf_bytes = 0;
+};
+
+// widest list the fold kernels accept
+constexpr int kMaxSlotWidth = 8;
+
+// Find or build the lists of a (two slots) and b (nullable, one slot);
+// nullptr when some target has more than kMaxSlotWidth contributions or the
+// padding would more than double the lists (the caller then uses the CSR
+// fold).
+SlotPlan *get_slot_plan(const GatherPlan *a, const GatherPlan *b);
+
 // Find or build the reference-compatible plan (device resident).
 DevPlan *get_plan(char const *name, op_set set, int part_size, int nargs, const op_arg *args,
                   int ninds, const int *inds);

@@ -74,9 +74,11 @@ __device__ __forceinline__ void grid_finish(const T (&v)[N], const T (&identity)
     T b = i == 0 ? block_fold(v[i], identity[i], op0, ws) : block_fold(v[i], identity[i], op1, ws);
     if (threadIdx.x == 0) slot[i].partials[blockIdx.x] = b;
   }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  // thread 0 wrote the partials: it alone fences them before taking a ticket
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
   __syncthreads();
   if (!last) return;
   __threadfence();
