@@ -469,38 +469,49 @@ __device__ __forceinline__ bool same_map(const IdxMap &a, const IdxMap &b) {
   return a.map == b.map && a.idx == b.idx && a.dim == b.dim;
 }
 
-template <class T>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4)
+// PIPE: fetch the next edge's map entries while this edge gathers (more
+// registers: MINB 6 CTAs per SM instead of 8)
+template <class T, bool PIPE, int MINB>
+__global__ void __launch_bounds__(256, MINB)
     k_res_flux_list(ResEdges<T> E, BresEdges<T> B, T *__restrict__ v, AirConsts<T> K) {
   const bool same_a = same_map(E.q1, E.a1) && same_map(E.q2, E.a2);
   const int total = E.n + B.n;
   const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
   // map entries of this thread's first edge: read-only, fetched before the
   // previous kernel has finished
-  int n1 = 0, n2 = 0, c1 = 0, c2 = 0, a1 = 0, a2 = 0;
-  auto edge_maps = [&](int e) {
-    at2(E.x1, E.x2, e, n1, n2);
-    at2(E.q1, E.q2, e, c1, c2);
+  // map entries of an edge (read-only): the first edge's are fetched before
+  // the previous kernel has finished, the next edge's while this one gathers
+  int m[6] = {0, 0, 0, 0, 0, 0}, mn[6] = {0, 0, 0, 0, 0, 0};
+  auto edge_maps = [&](int e, int (&o)[6]) {
+    if (e >= E.n) return;
+    at2(E.x1, E.x2, e, o[0], o[1]);
+    at2(E.q1, E.q2, e, o[2], o[3]);
     if (same_a) {
-      a1 = c1; a2 = c2;
+      o[4] = o[2]; o[5] = o[3];
     } else {
-      at2(E.a1, E.a2, e, a1, a2);
+      at2(E.a1, E.a2, e, o[4], o[5]);
     }
   };
-  if (i0 < E.n) edge_maps(i0);
+  edge_maps(i0, m);
   pdl_wait();
   pdl_trigger();
-  for (int i = i0; i < total; i += gridDim.x * blockDim.x) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = i0; i < total; i += stride) {
     T f[4];
     if (i < E.n) {
-      if (i != i0) edge_maps(i);
       T p[2], s[2], q1[4], q2[4];
-      ld4(E.qa + 4 * (size_t)c1, q1);
-      ld4(E.qb + 4 * (size_t)c2, q2);
-      ld2(E.xa + 2 * (size_t)n1, p);
-      ld2(E.xb + 2 * (size_t)n2, s);
-      const T d1 = __ldg(E.adta + a1), d2 = __ldg(E.adtb + a2);
+      ld4(E.qa + 4 * (size_t)m[2], q1);
+      ld4(E.qb + 4 * (size_t)m[3], q2);
+      ld2(E.xa + 2 * (size_t)m[0], p);
+      ld2(E.xb + 2 * (size_t)m[1], s);
+      const T d1 = __ldg(E.adta + m[4]), d2 = __ldg(E.adtb + m[5]);
+      if (PIPE) {
+        edge_maps(i + stride, mn);
+#pragma unroll
+        for (int j = 0; j < 6; j++) m[j] = mn[j];
+      }
       res_flux(p, s, q1, q2, d1, d2, K.gm1, K.eps, f);
+      if (!PIPE) edge_maps(i + stride, m);
     } else {
       const int b = i - E.n;
       int m1, m2;
@@ -600,31 +611,31 @@ __global__ void __launch_bounds__(256, MINB)
                     N.m2.idx == 2 && N.m3.idx == 3;
   const int stride = gridDim.x * blockDim.x;
   T rms = T(0);
-  int nd[U][4], k[U][4];
-  // list heads and node indices of U cells: plan and map data (read-only)
-  auto indices = [&](int base) {
+  // list heads and node indices of U cells: plan and map data (read-only),
+  // fetched one pass ahead so they arrive while the current pass gathers
+  int nd[U][4], k[U][4], ndn[U][4], kn[U][4];
+  auto indices = [&](int base, int (&kk)[U][4], int (&nn)[U][4]) {
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const int c = base + u * stride;
       if (c >= n) continue;
-      list_head(ell, W, c, k[u]);
+      list_head(ell, W, c, kk[u]);
       if (ADT) {
         if (quad) {
           int4 v = __ldg(reinterpret_cast<const int4 *>(N.m0.map) + c);
-          nd[u][0] = v.x; nd[u][1] = v.y; nd[u][2] = v.z; nd[u][3] = v.w;
+          nn[u][0] = v.x; nn[u][1] = v.y; nn[u][2] = v.z; nn[u][3] = v.w;
         } else {
-          nd[u][0] = at(N.m0, c); nd[u][1] = at(N.m1, c);
-          nd[u][2] = at(N.m2, c); nd[u][3] = at(N.m3, c);
+          nn[u][0] = at(N.m0, c); nn[u][1] = at(N.m1, c);
+          nn[u][2] = at(N.m2, c); nn[u][3] = at(N.m3, c);
         }
       }
     }
   };
   const int base0 = blockIdx.x * blockDim.x + threadIdx.x;
-  indices(base0);  // before the previous kernel has finished
+  indices(base0, k, nd);  // before the previous kernel has finished
   pdl_wait();
   pdl_trigger();
   for (int base = base0; base < n; base += stride * U) {
-    if (base != base0) indices(base);
     T r[U][4], qo[U][4], ad[U], xs[U][4][2], f[U][4][4];
 #pragma unroll
     for (int u = 0; u < U; u++) {
@@ -643,6 +654,7 @@ __global__ void __launch_bounds__(256, MINB)
         ld2(x3 + 2 * (size_t)nd[u][3], xs[u][3]);
       }
     }
+    indices(base + stride * U, kn, ndn);
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const int c = base + u * stride;
@@ -670,6 +682,13 @@ __global__ void __launch_bounds__(256, MINB)
       if (seq) st4(seq + 4 * (size_t)c, sq);
       if (ADT) adt[c] = adt_calc(xs[u][0], xs[u][1], xs[u][2], xs[u][3], qn, K);
     }
+#pragma unroll
+    for (int u = 0; u < U; u++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        k[u][j] = kn[u][j];
+        nd[u][j] = ndn[u][j];
+      }
   }
   if (seq) return;
   const T v[1] = {rms}, id[1] = {T(0)};
@@ -1467,7 +1486,13 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
       const int per_sm = tuning("flux_ctas_per_sm", 16);
       long long fg = (nflux + 255) / 256;
       if (per_sm > 0) fg = std::min(fg, (long long)rt().num_sms * per_sm);
-      launch_pdl(k_res_flux_list<T>, (unsigned)std::max(1LL, fg), 256, 0, s, E, B, vals, K);
+      const unsigned fgrid = (unsigned)std::max(1LL, fg);
+      if (tuning("flux_pipe", 0))
+        launch_pdl(k_res_flux_list<T, true, sizeof(T) == 4 ? 6 : 3>, fgrid, 256, 0, s, E, B, vals,
+                   K);
+      else
+        launch_pdl(k_res_flux_list<T, false, sizeof(T) == 4 ? 8 : 4>, fgrid, 256, 0, s, E, B,
+                   vals, K);
     }
     PhaseScope ph(name + ":fold");
     T *res = (T *)ra[6].dat->data_d;
