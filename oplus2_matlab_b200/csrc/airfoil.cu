@@ -527,6 +527,56 @@ __global__ void __launch_bounds__(256, MINB)
   }
 }
 
+// The same pass for the shape res_calc always has in the airfoil app: both
+// x arguments through one dim-2 map (pedge, idx 0 and 1), q and adt through
+// another (pecell), one dataset each -- one 8-byte load per map, 32-bit
+// index arithmetic (map values are checked against the target set's size
+// at op_decl_map; the host takes this path only for sets below 2^30).
+template <class T>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4)
+    k_res_flux_pair(int ne, const int2 *__restrict__ pedge, const int2 *__restrict__ pecell,
+                    const T *__restrict__ x, const T *__restrict__ q,
+                    const T *__restrict__ adt, BresEdges<T> B, T *__restrict__ v,
+                    AirConsts<T> K) {
+  const unsigned total = (unsigned)ne + (unsigned)B.n, n_e = (unsigned)ne;
+  const unsigned i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned stride = gridDim.x * blockDim.x;
+  int2 nn = make_int2(0, 0), cc = make_int2(0, 0);
+  if (i0 < n_e) {  // map entries: read-only, fetched before the wait
+    nn = __ldg(pedge + i0);
+    cc = __ldg(pecell + i0);
+  }
+  pdl_wait();
+  pdl_trigger();
+  for (unsigned i = i0; i < total; i += stride) {
+    T f[4];
+    if (i < n_e) {
+      T p[2], s[2], q1[4], q2[4];
+      ld4(q + 4u * (unsigned)cc.x, q1);
+      ld4(q + 4u * (unsigned)cc.y, q2);
+      ld2(x + 2u * (unsigned)nn.x, p);
+      ld2(x + 2u * (unsigned)nn.y, s);
+      const T d1 = __ldg(adt + (unsigned)cc.x), d2 = __ldg(adt + (unsigned)cc.y);
+      if (i + stride < n_e) {
+        nn = __ldg(pedge + i + stride);
+        cc = __ldg(pecell + i + stride);
+      }
+      res_flux(p, s, q1, q2, d1, d2, K.gm1, K.eps, f);
+    } else {
+      const int b = (int)(i - n_e);
+      int m1, m2;
+      at2(B.x1, B.x2, b, m1, m2);
+      T p[2], s[2], q1[4];
+      ld2(B.xa + 2 * (size_t)m1, p);
+      ld2(B.xb + 2 * (size_t)m2, s);
+      ld4(B.q_d + 4 * (size_t)at(B.q, b), q1);
+      const T b1 = __ldg(B.adt + at(B.a, b));
+      bres_contrib(p, s, q1, b1, __ldg(B.bound_d + at(B.bound, b)), K, f);
+    }
+    st4(v + 4u * i, f);
+  }
+}
+
 // r += the listed values of cell c, in list order
 template <class T>
 __device__ __forceinline__ void fold_list(const int *__restrict__ ell, int W,
@@ -1487,7 +1537,21 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
       long long fg = (nflux + 255) / 256;
       if (per_sm > 0) fg = std::min(fg, (long long)rt().num_sms * per_sm);
       const unsigned fgrid = (unsigned)std::max(1LL, fg);
-      if (tuning("flux_pipe", 0))
+      auto pair = [](const op_arg &a, const op_arg &b) {
+        return a.map && a.map == b.map && a.map->dim == 2 && a.idx == 0 && b.idx == 1;
+      };
+      const bool shape = pair(ra[0], ra[1]) && pair(ra[2], ra[3]) && pair(ra[4], ra[5]) &&
+                         ra[2].map == ra[4].map && ra[0].dat == ra[1].dat &&
+                         ra[2].dat == ra[3].dat && ra[4].dat == ra[5].dat &&
+                         (long long)nval < (1LL << 30) &&
+                         (long long)ra[2].dat->set->size < (1LL << 30) &&
+                         (long long)ra[0].dat->set->size < (1LL << 30);
+      if (shape && tuning("flux_pair", 1))
+        launch_pdl(k_res_flux_pair<T>, fgrid, 256, 0, s, E.n,
+                   reinterpret_cast<const int2 *>(map_dev(ra[0].map)),
+                   reinterpret_cast<const int2 *>(map_dev(ra[2].map)), E.xa, E.qa, E.adta, B,
+                   vals, K);
+      else if (tuning("flux_pipe", 0))
         launch_pdl(k_res_flux_list<T, true, sizeof(T) == 4 ? 6 : 3>, fgrid, 256, 0, s, E, B, vals,
                    K);
       else
