@@ -145,6 +145,25 @@ PROTOTYPES = [
     ("op2b_mesh_jac1", C.c_int, [C.c_int, _P, _P, _P]),
     ("op2b_mesh_jac2", C.c_int, [C.c_int, _P, _P, _P]),
     ("op2b_splitmix64", C.c_uint64, [C.POINTER(C.c_uint64)]),
+    # op2b_group.h
+    ("op2b_flow_qinf", C.c_int, [C.c_double, C.c_double, C.c_int, _P, _P]),
+    ("op2b_group_create", _P, [C.c_int]),
+    ("op2b_group_destroy", None, [_P]),
+    ("op2b_group_add", C.c_int, [_P, C.POINTER(op2b_mesh), C.c_double, C.c_double, C.c_int,
+                                 C.c_double]),
+    ("op2b_group_run", C.c_int, [_P, C.c_int]),
+    ("op2b_group_poll", C.c_int, [_P, C.POINTER(C.c_int), C.c_int]),
+    ("op2b_group_sync", C.c_int, [_P]),
+    ("op2b_group_iterations", C.c_int, [_P, C.c_int]),
+    ("op2b_group_history", C.c_int, [_P, C.c_int, C.POINTER(C.c_double), C.c_int]),
+    ("op2b_group_fetch_q", C.c_int, [_P, C.c_int, _P]),
+    ("op2b_group_remove", C.c_int, [_P, C.c_int]),
+    ("op2b_group_solve_bytes", C.c_longlong, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
+    ("op2b_group_device_bytes", C.c_longlong, [_P]),
+    ("op2b_group_active", C.c_int, [_P]),
+    ("op2b_group_set_edge_tile", C.c_int, [_P, C.c_int]),
+    ("op2b_group_edge_tile", C.c_int, [_P]),
+    ("op2b_group_autotune", C.c_int, [_P, C.c_int]),
 ]
 
 # data symbols of op_lib.h

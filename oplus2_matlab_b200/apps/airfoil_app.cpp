@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include "op2b.h"
+#include "op2b_group.h"
 #include "op2b_mesh.h"
 #include "op_lib.h"
 
@@ -30,6 +31,9 @@ typedef struct {
 
 int op2b_airfoil_app(const op2b_mesh *m, int fp64, int niter, void *q, double *rms_hist,
                      int strategy, op2b_app_timing *t);
+// the same solve at another flow condition (Mach number, alpha in degrees)
+int op2b_airfoil_app_flow(const op2b_mesh *m, int fp64, int niter, double mach, double alpha_deg,
+                          void *q, double *rms_hist, int strategy, op2b_app_timing *t);
 }
 
 static double now() {
@@ -39,46 +43,17 @@ static double now() {
 }
 
 template <class T>
-static void consts(T &gam, T &gm1, T &cfl, T &eps, T &mach, T &alpha, T qinf[4]);
-
-// airfoil/airfoil.cpp:175-191 in float
-template <>
-void consts<float>(float &gam, float &gm1, float &cfl, float &eps, float &mach, float &alpha,
-                   float qinf[4]) {
-  gam = 1.4f;
-  gm1 = gam - 1.0f;
-  cfl = 0.9f;
-  eps = 0.05f;
-  mach = 0.4f;
-  alpha = 3.0f * atanf(1.0f) / 45.0f;
-  float p = 1.0f, r = 1.0f;
-  float u = sqrtf(gam * p / r) * mach;
-  float e = p / (r * gm1) + 0.5f * u * u;
-  qinf[0] = r; qinf[1] = r * u; qinf[2] = 0.0f; qinf[3] = r * e;
-}
-
-// the float->double variant of the same lines (float literals kept)
-template <>
-void consts<double>(double &gam, double &gm1, double &cfl, double &eps, double &mach,
-                    double &alpha, double qinf[4]) {
-  gam = 1.4f;
-  gm1 = gam - 1.0f;
-  cfl = 0.9f;
-  eps = 0.05f;
-  mach = 0.4f;
-  alpha = 3.0f * atanf(1.0f) / 45.0f;
-  double p = 1.0f, r = 1.0f;
-  double u = sqrt(gam * p / r) * mach;
-  double e = p / (r * gm1) + 0.5f * u * u;
-  qinf[0] = r; qinf[1] = r * u; qinf[2] = 0.0f; qinf[3] = r * e;
-}
-
-template <class T>
-static int run(const op2b_mesh *m, int niter, T *q, double *rms_hist, op2b_app_timing *tm) {
+static int run(const op2b_mesh *m, int niter, double mach_d, double alpha_deg, T *q,
+               double *rms_hist, op2b_app_timing *tm) {
   const char *tn = sizeof(T) == 8 ? "double" : "float";
   double t0 = now();
-  T gam, gm1, cfl, eps, mach, alpha, qinf[4];
-  consts<T>(gam, gm1, cfl, eps, mach, alpha, qinf);
+  // airfoil/airfoil.cpp:134-149: the constants and the free stream, with the
+  // flow condition as parameters (op2b_flow_qinf; Mach 0.4, alpha 0 is the
+  // reference's own)
+  T qinf[4], c4[4];
+  op2b_flow_qinf(mach_d, alpha_deg, sizeof(T) == 8, qinf, c4);
+  T gam = c4[0], gm1 = c4[1], cfl = c4[2], eps = c4[3];
+  T mach = (T)(float)mach_d, alpha = (T)((float)alpha_deg * (atanf(1.0f) / 45.0f));
   const int nc = m->ncell;
   // qold, adt, res start as the app starts them: zero
   T *qold = (T *)calloc((size_t)nc * 4, sizeof(T));
@@ -173,6 +148,14 @@ static int run(const op2b_mesh *m, int niter, T *q, double *rms_hist, op2b_app_t
 extern "C" int op2b_airfoil_app(const op2b_mesh *m, int fp64, int niter, void *q, double *rms_hist,
                                 int strategy, op2b_app_timing *t) {
   op2b_set_strategy(strategy);
-  return fp64 ? run<double>(m, niter, (double *)q, rms_hist, t)
-              : run<float>(m, niter, (float *)q, rms_hist, t);
+  return fp64 ? run<double>(m, niter, 0.4, 0.0, (double *)q, rms_hist, t)
+              : run<float>(m, niter, 0.4, 0.0, (float *)q, rms_hist, t);
+}
+
+extern "C" int op2b_airfoil_app_flow(const op2b_mesh *m, int fp64, int niter, double mach,
+                                     double alpha_deg, void *q, double *rms_hist, int strategy,
+                                     op2b_app_timing *t) {
+  op2b_set_strategy(strategy);
+  return fp64 ? run<double>(m, niter, mach, alpha_deg, (double *)q, rms_hist, t)
+              : run<float>(m, niter, mach, alpha_deg, (float *)q, rms_hist, t);
 }

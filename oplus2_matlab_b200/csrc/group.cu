@@ -1,0 +1,943 @@
+// group.cu -- many airfoil solves on one GPU (op2b_group.h): the batched and
+// served forms of the airfoil iteration.
+//
+// Each solve keeps its own datasets, maps and contribution lists in HBM (one
+// stream-ordered allocation per solve).  One outer iteration of every active
+// solve is five launches, the same five as the plain path's fused chains:
+//   k_grp_save_adt      save_soln + adt_calc              (cell tiles)
+//   k_grp_flux          res_calc flux + bres_calc values  (edge tiles)
+//   k_grp_fold<true>    fold + update + adt_calc          (cell tiles)
+//   k_grp_flux
+//   k_grp_fold<false>   fold + update + rms               (cell tiles)
+// A tile is a run of one solve's elements; a launch's grid is its tile table,
+// so one launch covers every solve, whatever their sizes.  The device
+// functions are the plain path's (airfoil_math.cuh) and the contribution
+// lists have the plain path's order, so q is bit-identical to the plain
+// solve.  The first update's rms is not computed: the reference app zeroes it
+// before the second update (airfoil/airfoil_op.cpp:283-290).
+//
+// The second update's rms: every cell tile of a solve writes one partial
+// (its threads' sums, folded in a fixed tree); the last CTA of the solve to
+// finish (a per-solve ticket) folds the solve's partials in tile order,
+// stores sqrt(sum / ncell) in the solve's history, advances its iteration
+// count and applies the stopping test.  Tiles are fixed by the solve's own
+// cell count (kCellTile), so the rms does not depend on the other solves.
+// A stopped solve's CTAs return at once; the host drops it from the tile
+// tables at the next op2b_group_run after a poll.
+
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <memory>
+#include <vector>
+
+#include "airfoil_math.cuh"
+#include "internal.h"
+#include "launch.cuh"
+#include "op2b_group.h"
+#include "reduce.cuh"
+
+namespace op2b {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kCellsPerThread = 4;
+constexpr int kCellTile = kThreads * kCellsPerThread;  // fixes the rms fold order
+constexpr int kMaxWidth = 8;                           // longest contribution list
+
+template <class T>
+struct SolveDev {  // device view of one solve; written by the host only
+  const T *x;
+  T *q, *qold, *adt, *res, *vals, *partials, *hist;
+  const int *pedge, *pecell, *pbedge, *pbecell, *bound, *pcell, *ell;
+  int ncell, nedge, nbedge, W, ntiles, pad;
+  T qinf[4];
+};
+
+struct SolveState {  // written by the kernels
+  int active, iter, max_iter;
+  unsigned ticket;
+  double rms1, tol;
+};
+
+struct Tile {
+  int solve, start, count, local;
+};
+
+__device__ __forceinline__ bool solve_active(const SolveState *st, int s) {
+  return *reinterpret_cast<const volatile int *>(&st[s].active) != 0;
+}
+
+template <class T>
+__device__ __forceinline__ AirConsts<T> with_qinf(AirConsts<T> K, const SolveDev<T> *d) {
+#pragma unroll
+  for (int i = 0; i < 4; i++) K.qinf[i] = d->qinf[i];
+  return K;
+}
+
+// save_soln + adt_calc over one tile of one solve's cells
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+    k_grp_save_adt(const Tile *__restrict__ tiles, const SolveDev<T> *__restrict__ sd,
+                   const SolveState *st, AirConsts<T> K) {
+  const Tile t = tiles[blockIdx.x];
+  const SolveDev<T> *d = sd + t.solve;
+  const int4 *pcell = reinterpret_cast<const int4 *>(d->pcell);
+  int4 nd[kCellsPerThread];
+#pragma unroll
+  for (int j = 0; j < kCellsPerThread; j++) {  // map entries: read-only
+    const int i = threadIdx.x + j * kThreads;
+    if (i < t.count) nd[j] = __ldg(pcell + t.start + i);
+  }
+  pdl_wait();
+  pdl_trigger();
+  if (!solve_active(st, t.solve)) return;
+  const T *x = d->x, *q = d->q;
+  T *qold = d->qold, *adt = d->adt;
+#pragma unroll
+  for (int j = 0; j < kCellsPerThread; j++) {
+    const int i = threadIdx.x + j * kThreads;
+    if (i >= t.count) continue;
+    const int c = t.start + i;
+    T qq[4], a[2], b[2], e[2], f[2];
+    ld4(q + 4 * (size_t)c, qq);
+    ld2(x + 2 * (size_t)nd[j].x, a);
+    ld2(x + 2 * (size_t)nd[j].y, b);
+    ld2(x + 2 * (size_t)nd[j].z, e);
+    ld2(x + 2 * (size_t)nd[j].w, f);
+    st4(qold + 4 * (size_t)c, qq);
+    adt[c] = adt_calc(a, b, e, f, qq, K);
+  }
+}
+
+// res_calc's flux per edge and bres_calc's increment per boundary edge, over
+// one tile of one solve's values (edges first, then boundary edges)
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+    k_grp_flux(const Tile *__restrict__ tiles, const SolveDev<T> *__restrict__ sd,
+               const SolveState *st, AirConsts<T> K0) {
+  const Tile t = tiles[blockIdx.x];
+  const SolveDev<T> *d = sd + t.solve;
+  const int ne = d->nedge;
+  const int2 *pedge = reinterpret_cast<const int2 *>(d->pedge);
+  const int2 *pecell = reinterpret_cast<const int2 *>(d->pecell);
+  const int i0 = t.start + threadIdx.x, end = t.start + t.count;
+  int2 nn = make_int2(0, 0), cc = make_int2(0, 0);
+  if (i0 < end && i0 < ne) {  // map entries: read-only
+    nn = __ldg(pedge + i0);
+    cc = __ldg(pecell + i0);
+  }
+  pdl_wait();
+  pdl_trigger();
+  if (!solve_active(st, t.solve)) return;
+  const AirConsts<T> K = with_qinf(K0, d);
+  const T *x = d->x, *q = d->q, *adt = d->adt;
+  T *v = d->vals;
+  for (int i = i0; i < end; i += kThreads) {
+    T f[4];
+    if (i < ne) {
+      if (i != i0) {
+        nn = __ldg(pedge + i);
+        cc = __ldg(pecell + i);
+      }
+      T p[2], s[2], q1[4], q2[4];
+      ld4(q + 4 * (size_t)cc.x, q1);
+      ld4(q + 4 * (size_t)cc.y, q2);
+      ld2(x + 2 * (size_t)nn.x, p);
+      ld2(x + 2 * (size_t)nn.y, s);
+      const T d1 = __ldg(adt + cc.x), d2 = __ldg(adt + cc.y);
+      res_flux(p, s, q1, q2, d1, d2, K.gm1, K.eps, f);
+    } else {
+      const int b = i - ne;
+      const int2 bn = __ldg(reinterpret_cast<const int2 *>(d->pbedge) + b);
+      const int c = __ldg(d->pbecell + b);
+      T p[2], s[2], q1[4];
+      ld2(x + 2 * (size_t)bn.x, p);
+      ld2(x + 2 * (size_t)bn.y, s);
+      ld4(q + 4 * (size_t)c, q1);
+      bres_contrib(p, s, q1, __ldg(adt + c), __ldg(d->bound + b), K, f);
+    }
+    st4(v + 4 * (size_t)i, f);
+  }
+}
+
+// the cell pass: fold each cell's listed values onto res in list order, then
+// update (airfoil/update.h:1-12); FIRST: then adt_calc on the new q, no rms;
+// otherwise: the rms partial, and the solve's last CTA ends the iteration
+template <class T, bool FIRST>
+__global__ void __launch_bounds__(kThreads)
+    k_grp_fold(const Tile *__restrict__ tiles, const SolveDev<T> *__restrict__ sd,
+               SolveState *st, AirConsts<T> K) {
+  const Tile t = tiles[blockIdx.x];
+  const SolveDev<T> *d = sd + t.solve;
+  const int W = d->W;
+  const int *ell = d->ell;
+  const int4 *pcell = reinterpret_cast<const int4 *>(d->pcell);
+  int k[kCellsPerThread][4];
+  int4 nd[kCellsPerThread];
+#pragma unroll
+  for (int j = 0; j < kCellsPerThread; j++) {  // list heads and nodes: read-only
+    const int i = threadIdx.x + j * kThreads;
+    if (i >= t.count) continue;
+    list_head(ell, W, t.start + i, k[j]);
+    if (FIRST) nd[j] = __ldg(pcell + t.start + i);
+  }
+  pdl_wait();
+  pdl_trigger();
+  const bool live = solve_active(st, t.solve);  // the same for the whole CTA
+  if (!live) return;
+  const T *x = d->x, *qold = d->qold, *vals = d->vals;
+  T *q = d->q, *res = d->res, *adt = d->adt;
+  T rms = T(0);
+#pragma unroll
+  for (int j = 0; j < kCellsPerThread; j++) {
+    const int i = threadIdx.x + j * kThreads;
+    if (i >= t.count) continue;
+    const int c = t.start + i;
+    T r[4], qo[4], f[4][4], xs[4][2];
+    ldw4(res + 4 * (size_t)c, r);
+    ld4(qold + 4 * (size_t)c, qo);
+    const T ad = adt[c];
+#pragma unroll
+    for (int m = 0; m < 4; m++)
+      if (k[j][m] >= 0) ld4(vals + 4 * (size_t)(k[j][m] >> 1), f[m]);
+    if (FIRST) {
+      ld2(x + 2 * (size_t)nd[j].x, xs[0]);
+      ld2(x + 2 * (size_t)nd[j].y, xs[1]);
+      ld2(x + 2 * (size_t)nd[j].z, xs[2]);
+      ld2(x + 2 * (size_t)nd[j].w, xs[3]);
+    }
+#pragma unroll
+    for (int m = 0; m < 4; m++) add_listed(r, k[j][m], f[m]);
+    for (int m = 4; m < W; m++) {  // lists longer than 4
+      const int kk = __ldg(ell + (size_t)c * W + m);
+      T g[4];
+      ld4(vals + 4 * (size_t)(kk >> 1), g);
+      add_listed(r, kk, g);
+    }
+    const T adti = rcp(ad);
+    T qn[4];
+    for (int m = 0; m < 4; m++) {
+      const T del = adti * r[m];
+      qn[m] = qo[m] - del;
+      rms += del * del;
+    }
+    st4(q + 4 * (size_t)c, qn);
+    const T z[4] = {T(0), T(0), T(0), T(0)};
+    st4(res + 4 * (size_t)c, z);
+    if (FIRST) adt[c] = adt_calc(xs[0], xs[1], xs[2], xs[3], qn, K);
+  }
+  if (FIRST) return;
+  __shared__ T ws[32];
+  __shared__ bool last;
+  const T b = block_fold(rms, T(0), OpSum(), ws);
+  if (threadIdx.x == 0) {  // the writer fences its partial, then takes a ticket
+    d->partials[t.local] = b;
+    __threadfence();
+    last = atomicAdd(&st[t.solve].ticket, 1u) == (unsigned)(d->ntiles - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  T sum = T(0);
+  for (int p = threadIdx.x; p < d->ntiles; p += kThreads) sum += __ldcg(d->partials + p);
+  sum = block_fold(sum, T(0), OpSum(), ws);
+  if (threadIdx.x == 0) {
+    SolveState &s = st[t.solve];
+    const T r = sqrt(sum / (T)d->ncell);  // airfoil/airfoil_op.cpp:291
+    const int it = s.iter;
+    d->hist[it] = r;
+    const int done = it + 1;
+    if (done == 1) s.rms1 = (double)r;
+    const bool stop =
+        done >= s.max_iter || (done >= 2 && s.tol > 0.0 && (double)r < s.tol * s.rms1);
+    s.iter = done;
+    if (stop) s.active = 0;
+    s.ticket = 0u;
+  }
+}
+
+// ------------------------------------------------ contribution lists ------
+// The plain path's list order, built per solve: res_calc's (edge << 1 |
+// side) ascending, then bres_calc's ((nedge + b) << 1) ascending, padded with
+// (nedge + nbedge) << 1 -- one sort of the cell's entries gives exactly this.
+
+__global__ void k_gl_count(int ne, int nb, const int *pecell, const int *pbecell, int *cnt) {
+  const int n = 2 * ne + nb;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    atomicAdd(cnt + (i < 2 * ne ? pecell[i] : pbecell[i - 2 * ne]), 1);
+}
+
+__global__ void k_gl_max(const int *v, int n, int *out) {
+  int m = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    m = max(m, v[i]);
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+__global__ void k_gl_pad(int ncell, int W, int pad, int *ell) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)ncell * W;
+       i += (size_t)gridDim.x * blockDim.x)
+    ell[i] = pad;
+}
+
+__global__ void k_gl_place(int ne, int nb, const int *pecell, const int *pbecell, int W,
+                           int *cursor, int *ell) {
+  const int n = 2 * ne + nb;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int c = i < 2 * ne ? pecell[i] : pbecell[i - 2 * ne];
+    const int key = i < 2 * ne ? i : (ne + (i - 2 * ne)) << 1;
+    const int pos = atomicAdd(cursor + c, 1);
+    if (pos < W) ell[(size_t)c * W + pos] = key;
+  }
+}
+
+__global__ void k_gl_sort(int ncell, int W, int *ell) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+    int v[kMaxWidth];
+    for (int j = 0; j < W; j++) v[j] = ell[(size_t)c * W + j];
+    for (int j = 1; j < W; j++) {  // insertion sort, W <= 8
+      const int x = v[j];
+      int m = j - 1;
+      while (m >= 0 && v[m] > x) {
+        v[m + 1] = v[m];
+        m--;
+      }
+      v[m + 1] = x;
+    }
+    for (int j = 0; j < W; j++) ell[(size_t)c * W + j] = v[j];
+  }
+}
+
+// q = qinf and res = 0 on every cell; the padding value -0.0
+template <class T>
+__global__ void k_gl_init(int ncell, T *q, T *res, T *vals_pad, T q0, T q1, T q2, T q3) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+    const T v[4] = {q0, q1, q2, q3}, z[4] = {T(0), T(0), T(0), T(0)};
+    st4(q + 4 * (size_t)c, v);
+    st4(res + 4 * (size_t)c, z);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < 4) vals_pad[threadIdx.x] = T(-0.0);
+}
+
+// ---------------------------------------------------------------- host ----
+
+template <class T>
+void flow_state(double mach_d, double alpha_deg, T qinf[4], T c[4]);
+
+// airfoil/airfoil.cpp:134-149 in float, alpha added to the velocity
+template <>
+void flow_state<float>(double mach_d, double alpha_deg, float qinf[4], float c[4]) {
+  float gam = 1.4f, gm1 = gam - 1.0f, cfl = 0.9f, eps = 0.05f;
+  float mach = (float)mach_d;
+  float p = 1.0f, r = 1.0f;
+  float u = sqrtf(gam * p / r) * mach;
+  float e = p / (r * gm1) + 0.5f * u * u;
+  qinf[0] = r;
+  qinf[3] = r * e;
+  if (alpha_deg == 0.0) {
+    qinf[1] = r * u;
+    qinf[2] = 0.0f;
+  } else {
+    float a = (float)alpha_deg * (atanf(1.0f) / 45.0f);
+    qinf[1] = r * u * cosf(a);
+    qinf[2] = r * u * sinf(a);
+  }
+  c[0] = gam; c[1] = gm1; c[2] = cfl; c[3] = eps;
+}
+
+// the float->double variant of the same lines (float literals kept)
+template <>
+void flow_state<double>(double mach_d, double alpha_deg, double qinf[4], double c[4]) {
+  double gam = 1.4f, gm1 = gam - 1.0f, cfl = 0.9f, eps = 0.05f;
+  // the reference's float literals are kept in its FP64 variant (0.4f), so
+  // Mach and alpha enter rounded to float
+  double mach = (double)(float)mach_d;
+  double p = 1.0f, r = 1.0f;
+  double u = sqrt(gam * p / r) * mach;
+  double e = p / (r * gm1) + 0.5f * u * u;
+  qinf[0] = r;
+  qinf[3] = r * e;
+  if (alpha_deg == 0.0) {
+    qinf[1] = r * u;
+    qinf[2] = 0.0f;
+  } else {
+    double a = (double)(float)alpha_deg * (atan(1.0) / 45.0);
+    qinf[1] = r * u * cos(a);
+    qinf[2] = r * u * sin(a);
+  }
+  c[0] = gam; c[1] = gm1; c[2] = cfl; c[3] = eps;
+}
+
+size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+struct GroupBase {
+  virtual ~GroupBase() {}
+  virtual int add(const op2b_mesh *m, double mach, double alpha, int max_iter, double tol) = 0;
+  virtual int run(int niter) = 0;
+  virtual int poll(int *ids, int max) = 0;
+  virtual int sync() = 0;
+  virtual int iterations(int id) = 0;
+  virtual int history(int id, double *out, int max) = 0;
+  virtual int fetch_q(int id, void *q) = 0;
+  virtual int remove(int id) = 0;
+  virtual long long solve_bytes(int nn, int nc, int ne, int nb, int max_iter) = 0;
+  virtual long long device_bytes() = 0;
+  virtual int active() = 0;
+  virtual int set_edge_tile(int e) = 0;
+  virtual int edge_tile() = 0;
+  virtual int autotune(int iters) = 0;
+};
+
+template <class T>
+struct Group : GroupBase {
+  struct Solve {
+    int nnode = 0, ncell = 0, nedge = 0, nbedge = 0, max_iter = 0;
+    double tol = 0;
+    void *block = nullptr;
+    int *ell = nullptr;
+    size_t bytes = 0;
+    cudaEvent_t ready = nullptr;
+    bool joined = false, removed = false, done = false, reported = false;
+    long long join_epoch = 0;  // the first state mirror that includes this solve
+    SolveDev<T> dev;
+  };
+
+  cudaStream_t cs = nullptr, us = nullptr;  // iterations; admission
+  std::vector<Solve> solves;
+  SolveDev<T> *d_sd = nullptr;
+  SolveState *d_st = nullptr;
+  SolveState *h_st = nullptr;  // pinned mirror, filled after each run
+  int cap = 0;
+  Tile *d_ct = nullptr, *d_et = nullptr;
+  size_t ct_cap = 0, et_cap = 0;
+  int nct = 0, net = 0, nactive = 0;
+  int etile = 2048;
+  bool changed = true;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t mirror_ev = nullptr;
+  bool mirror_pending = false;
+  long long mirror_epoch = 0;  // state mirrors issued (run) so far
+  AirConsts<T> K;
+  bool ok = false;
+
+  Group() {
+    ensure_cuda();
+    if (error_pending()) return;
+    OP2B_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    OP2B_CUDA(cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking));
+    OP2B_CUDA(cudaEventCreateWithFlags(&mirror_ev, cudaEventDisableTiming));
+    T q[4], c[4];
+    flow_state<T>(0.4, 0.0, q, c);
+    memset(&K, 0, sizeof K);
+    K.gam = c[0]; K.gm1 = c[1]; K.cfl = c[2]; K.eps = c[3];
+    ok = !error_pending();
+  }
+
+  ~Group() override {
+    if (cs) cudaStreamSynchronize(cs);
+    if (us) cudaStreamSynchronize(us);
+    for (auto &s : solves) release(s);
+    if (exec) cudaGraphExecDestroy(exec);
+    cudaFree(d_sd);
+    cudaFree(d_st);
+    cudaFree(d_ct);
+    cudaFree(d_et);
+    if (h_st) cudaFreeHost(h_st);
+    if (mirror_ev) cudaEventDestroy(mirror_ev);
+    if (cs) cudaStreamDestroy(cs);
+    if (us) cudaStreamDestroy(us);
+  }
+
+  void release(Solve &s) {
+    if (s.removed) return;
+    if (s.block) cudaFreeAsync(s.block, s.joined ? cs : us);
+    if (s.ell) cudaFreeAsync(s.ell, s.joined ? cs : us);
+    if (s.ready) cudaEventDestroy(s.ready);
+    s.block = nullptr;
+    s.ell = nullptr;
+    s.ready = nullptr;
+    s.removed = true;
+  }
+
+  static size_t layout(int nn, int nc, int ne, int nb, int max_iter, size_t off[16]) {
+    const int ntiles = (nc + kCellTile - 1) / kCellTile;
+    const size_t sz[16] = {sizeof(T) * 2 * (size_t)nn,                 // x
+                           sizeof(T) * 4 * (size_t)nc,                 // q
+                           sizeof(T) * 4 * (size_t)nc,                 // qold
+                           sizeof(T) * (size_t)nc,                     // adt
+                           sizeof(T) * 4 * (size_t)nc,                 // res
+                           sizeof(T) * 4 * ((size_t)ne + nb + 1),      // vals
+                           sizeof(T) * (size_t)std::max(ntiles, 1),    // partials
+                           sizeof(T) * (size_t)std::max(max_iter, 1),  // hist
+                           sizeof(int) * 2 * (size_t)ne,               // pedge
+                           sizeof(int) * 2 * (size_t)ne,               // pecell
+                           sizeof(int) * 2 * (size_t)std::max(nb, 1),  // pbedge
+                           sizeof(int) * (size_t)std::max(nb, 1),      // pbecell
+                           sizeof(int) * (size_t)std::max(nb, 1),      // bound
+                           sizeof(int) * 4 * (size_t)nc,               // pcell
+                           sizeof(int) * ((size_t)nc + 1),             // list counts (build)
+                           0};
+    size_t tot = 0;
+    for (int i = 0; i < 16; i++) {
+      off[i] = tot;
+      tot += align256(sz[i]);
+    }
+    return tot;
+  }
+
+  long long solve_bytes(int nn, int nc, int ne, int nb, int max_iter) override {
+    size_t off[16];
+    return (long long)(layout(nn, nc, ne, nb, max_iter, off) + align256(sizeof(int) * 4 * (size_t)nc));
+  }
+
+  int add(const op2b_mesh *m, double mach, double alpha, int max_iter, double tol) override {
+    if (!ok || !m || m->ncell <= 0 || m->nedge <= 0 || m->nnode <= 0 || m->nbedge < 0 ||
+        max_iter <= 0) {
+      fail(-1, "op2b_group_add error -- bad mesh or max_iter\n");
+      return -1;
+    }
+    if ((long long)m->nedge + m->nbedge + 1 >= (1LL << 30)) {
+      fail(-1, "op2b_group_add error -- mesh too large for 32-bit value lists\n");
+      return -1;
+    }
+    Solve s;
+    s.nnode = m->nnode; s.ncell = m->ncell; s.nedge = m->nedge; s.nbedge = m->nbedge;
+    s.max_iter = max_iter;
+    s.tol = tol;
+    size_t off[16];
+    const size_t tot = layout(s.nnode, s.ncell, s.nedge, s.nbedge, max_iter, off);
+    if (cudaMallocAsync(&s.block, tot, us) != cudaSuccess) {
+      cudaGetLastError();
+      fail(-1, "op2b_group_add error -- out of device memory (%zu bytes)\n", tot);
+      return -1;
+    }
+    s.bytes = tot;
+    char *b = (char *)s.block;
+    SolveDev<T> &d = s.dev;
+    memset(&d, 0, sizeof d);
+    d.x = (const T *)(b + off[0]);
+    d.q = (T *)(b + off[1]); d.qold = (T *)(b + off[2]); d.adt = (T *)(b + off[3]);
+    d.res = (T *)(b + off[4]); d.vals = (T *)(b + off[5]); d.partials = (T *)(b + off[6]);
+    d.hist = (T *)(b + off[7]);
+    d.pedge = (const int *)(b + off[8]); d.pecell = (const int *)(b + off[9]);
+    d.pbedge = (const int *)(b + off[10]); d.pbecell = (const int *)(b + off[11]);
+    d.bound = (const int *)(b + off[12]); d.pcell = (const int *)(b + off[13]);
+    int *cnt = (int *)(b + off[14]);
+    d.ncell = s.ncell; d.nedge = s.nedge; d.nbedge = s.nbedge;
+    d.ntiles = (s.ncell + kCellTile - 1) / kCellTile;
+    T c4[4];
+    flow_state<T>(mach, alpha, d.qinf, c4);
+    const T *xh = (const T *)(sizeof(T) == 8 ? (const void *)m->x64 : (const void *)m->x32);
+    auto up = [&](const void *dst, const void *src, size_t n) {
+      if (n) OP2B_CUDA(cudaMemcpyAsync((void *)dst, src, n, cudaMemcpyHostToDevice, us));
+    };
+    up(d.x, xh, sizeof(T) * 2 * (size_t)s.nnode);
+    up(d.pedge, m->edge, sizeof(int) * 2 * (size_t)s.nedge);
+    up(d.pecell, m->ecell, sizeof(int) * 2 * (size_t)s.nedge);
+    up(d.pbedge, m->bedge, sizeof(int) * 2 * (size_t)s.nbedge);
+    up(d.pbecell, m->becell, sizeof(int) * (size_t)s.nbedge);
+    up(d.bound, m->bound, sizeof(int) * (size_t)s.nbedge);
+    up(d.pcell, m->cell, sizeof(int) * 4 * (size_t)s.ncell);
+    // contribution lists: count, width, place, sort
+    const int grid = rt().num_sms * 4;
+    OP2B_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)s.ncell + 1), us));
+    k_gl_count<<<grid, 256, 0, us>>>(s.nedge, s.nbedge, d.pecell, d.pbecell, cnt);
+    k_gl_max<<<grid, 256, 0, us>>>(cnt, s.ncell, cnt + s.ncell);
+    int W = 0;
+    OP2B_CUDA(cudaMemcpyAsync(&W, cnt + s.ncell, sizeof(int), cudaMemcpyDeviceToHost, us));
+    OP2B_CUDA(cudaStreamSynchronize(us));
+    if (W < 1 || W > kMaxWidth) {
+      cudaFreeAsync(s.block, us);
+      fail(-1, "op2b_group_add error -- a cell has %d contributions (at most %d)\n", W,
+           kMaxWidth);
+      return -1;
+    }
+    d.W = W;
+    if (cudaMallocAsync((void **)&s.ell, sizeof(int) * W * (size_t)s.ncell, us) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFreeAsync(s.block, us);
+      fail(-1, "op2b_group_add error -- out of device memory\n");
+      return -1;
+    }
+    s.bytes += align256(sizeof(int) * W * (size_t)s.ncell);
+    d.ell = s.ell;
+    k_gl_pad<<<grid, 256, 0, us>>>(s.ncell, W, (s.nedge + s.nbedge) << 1, s.ell);
+    OP2B_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)s.ncell, us));
+    k_gl_place<<<grid, 256, 0, us>>>(s.nedge, s.nbedge, d.pecell, d.pbecell, W, cnt, s.ell);
+    k_gl_sort<<<grid, 256, 0, us>>>(s.ncell, W, s.ell);
+    OP2B_CUDA(cudaMemsetAsync(d.qold, 0, sizeof(T) * 4 * (size_t)s.ncell, us));
+    OP2B_CUDA(cudaMemsetAsync(d.adt, 0, sizeof(T) * (size_t)s.ncell, us));
+    k_gl_init<T><<<grid, 256, 0, us>>>(s.ncell, d.q, d.res, d.vals + 4 * ((size_t)s.nedge + s.nbedge),
+                                       d.qinf[0], d.qinf[1], d.qinf[2], d.qinf[3]);
+    OP2B_CUDA(cudaEventCreateWithFlags(&s.ready, cudaEventDisableTiming));
+    OP2B_CUDA(cudaEventRecord(s.ready, us));
+    if (error_pending()) return -1;
+    solves.push_back(s);
+    return (int)solves.size() - 1;
+  }
+
+  // device arrays of solve views and states, at least n entries
+  void reserve(int n) {
+    if (n <= cap) return;
+    int nc = std::max(64, cap);
+    while (nc < n) nc *= 2;
+    SolveDev<T> *sd = nullptr;
+    SolveState *st = nullptr, *hs = nullptr;
+    OP2B_CUDA(cudaMallocAsync((void **)&sd, sizeof(SolveDev<T>) * nc, cs));
+    OP2B_CUDA(cudaMallocAsync((void **)&st, sizeof(SolveState) * nc, cs));
+    OP2B_CUDA(cudaMallocHost((void **)&hs, sizeof(SolveState) * nc));
+    OP2B_CUDA(cudaMemsetAsync(st, 0, sizeof(SolveState) * nc, cs));
+    if (cap) {
+      OP2B_CUDA(cudaMemcpyAsync(sd, d_sd, sizeof(SolveDev<T>) * cap, cudaMemcpyDeviceToDevice, cs));
+      OP2B_CUDA(cudaMemcpyAsync(st, d_st, sizeof(SolveState) * cap, cudaMemcpyDeviceToDevice, cs));
+      OP2B_CUDA(cudaFreeAsync(d_sd, cs));
+      OP2B_CUDA(cudaFreeAsync(d_st, cs));
+    }
+    if (h_st) {
+      OP2B_CUDA(cudaStreamSynchronize(cs));  // the mirror may be the target of a copy
+      memcpy(hs, h_st, sizeof(SolveState) * cap);
+      cudaFreeHost(h_st);
+    } else {
+      memset(hs, 0, sizeof(SolveState) * nc);
+    }
+    d_sd = sd;
+    d_st = st;
+    h_st = hs;
+    cap = nc;
+    changed = true;
+  }
+
+  void upload_tiles(Tile *&dptr, size_t &dcap, const std::vector<Tile> &h) {
+    const size_t need = std::max<size_t>(h.size(), 1);
+    if (need > dcap) {
+      if (dptr) OP2B_CUDA(cudaFreeAsync(dptr, cs));
+      OP2B_CUDA(cudaMallocAsync((void **)&dptr, sizeof(Tile) * need, cs));
+      dcap = need;
+    }
+    if (!h.empty())
+      OP2B_CUDA(cudaMemcpyAsync(dptr, h.data(), sizeof(Tile) * h.size(), cudaMemcpyHostToDevice, cs));
+  }
+
+  void rebuild() {
+    std::vector<Tile> ct, et;
+    nactive = 0;
+    for (int id = 0; id < (int)solves.size(); id++) {
+      const Solve &s = solves[id];
+      if (!s.joined || s.removed || s.done) continue;
+      nactive++;
+      for (int a = 0, l = 0; a < s.ncell; a += kCellTile, l++)
+        ct.push_back(Tile{id, a, std::min(kCellTile, s.ncell - a), l});
+      const int nv = s.nedge + s.nbedge;
+      for (int a = 0, l = 0; a < nv; a += etile, l++)
+        et.push_back(Tile{id, a, std::min(etile, nv - a), l});
+    }
+    upload_tiles(d_ct, ct_cap, ct);
+    upload_tiles(d_et, et_cap, et);
+    nct = (int)ct.size();
+    net = (int)et.size();
+    if (exec) {
+      cudaGraphExecDestroy(exec);
+      exec = nullptr;
+    }
+    if (nactive == 0) return;
+    cudaGraph_t graph = nullptr;
+    OP2B_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    iteration();
+    OP2B_CUDA(cudaStreamEndCapture(cs, &graph));
+    if (graph) {
+      OP2B_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+      cudaGraphDestroy(graph);
+    }
+    changed = false;
+  }
+
+  void iteration() {
+    launch_pdl(k_grp_save_adt<T>, nct, kThreads, 0, cs, (const Tile *)d_ct,
+               (const SolveDev<T> *)d_sd, (const SolveState *)d_st, K);
+    launch_pdl(k_grp_flux<T>, net, kThreads, 0, cs, (const Tile *)d_et, (const SolveDev<T> *)d_sd,
+               (const SolveState *)d_st, K);
+    launch_pdl(k_grp_fold<T, true>, nct, kThreads, 0, cs, (const Tile *)d_ct,
+               (const SolveDev<T> *)d_sd, d_st, K);
+    launch_pdl(k_grp_flux<T>, net, kThreads, 0, cs, (const Tile *)d_et, (const SolveDev<T> *)d_sd,
+               (const SolveState *)d_st, K);
+    launch_pdl(k_grp_fold<T, false>, nct, kThreads, 0, cs, (const Tile *)d_ct,
+               (const SolveDev<T> *)d_sd, d_st, K);
+  }
+
+  int join_pending() {
+    int joined = 0;
+    for (int id = 0; id < (int)solves.size(); id++) {
+      Solve &s = solves[id];
+      if (s.joined || s.removed) continue;
+      reserve(id + 1);
+      OP2B_CUDA(cudaStreamWaitEvent(cs, s.ready, 0));
+      SolveState st0;
+      memset(&st0, 0, sizeof st0);
+      st0.active = 1;
+      st0.max_iter = s.max_iter;
+      st0.tol = s.tol;
+      OP2B_CUDA(cudaMemcpyAsync(d_sd + id, &s.dev, sizeof(SolveDev<T>), cudaMemcpyHostToDevice, cs));
+      OP2B_CUDA(cudaMemcpyAsync(d_st + id, &st0, sizeof(SolveState), cudaMemcpyHostToDevice, cs));
+      s.join_epoch = mirror_epoch + 1;
+      s.joined = true;
+      joined++;
+    }
+    if (joined) changed = true;
+    return joined;
+  }
+
+  int run(int niter) override {
+    if (!ok || niter < 0) return -1;
+    if (!solves.empty()) reserve((int)solves.size());  // the state mirror covers every id
+    join_pending();
+    if (error_pending()) return -1;
+    if (changed) rebuild();
+    if (error_pending()) return -1;
+    if (exec)
+      for (int i = 0; i < niter; i++) OP2B_CUDA(cudaGraphLaunch(exec, cs));
+    if ((int)solves.size() > 0 && cap > 0) {
+      OP2B_CUDA(cudaMemcpyAsync(h_st, d_st, sizeof(SolveState) * solves.size(),
+                                cudaMemcpyDeviceToHost, cs));
+      OP2B_CUDA(cudaEventRecord(mirror_ev, cs));
+      mirror_pending = true;
+      mirror_epoch++;
+    }
+    return error_pending() ? -1 : nactive;
+  }
+
+  int sync() override {
+    if (!ok) return -1;
+    OP2B_CUDA(cudaStreamSynchronize(cs));
+    OP2B_CUDA(cudaStreamSynchronize(us));
+    mirror_pending = false;
+    return error_pending() ? -1 : 0;
+  }
+
+  int poll(int *ids, int max) override {
+    if (!ok) return -1;
+    if (mirror_pending) {
+      OP2B_CUDA(cudaEventSynchronize(mirror_ev));
+      mirror_pending = false;
+    }
+    int n = 0;
+    for (int id = 0; id < (int)solves.size(); id++) {
+      Solve &s = solves[id];
+      if (!s.joined || s.removed || s.reported || s.join_epoch > mirror_epoch || h_st[id].active)
+        continue;
+      s.done = true;
+      changed = true;
+      if (n < max && ids) {
+        ids[n++] = id;
+        s.reported = true;
+      }
+    }
+    return error_pending() ? -1 : n;
+  }
+
+  Solve *get(int id) {
+    if (id < 0 || id >= (int)solves.size() || solves[id].removed) {
+      fail(-1, "op2b_group error -- no solve %d\n", id);
+      return nullptr;
+    }
+    return &solves[id];
+  }
+
+  int iterations(int id) override {
+    Solve *s = get(id);
+    if (!s) return -1;
+    if (!s->joined) return 0;
+    sync();
+    SolveState st;
+    OP2B_CUDA(cudaMemcpy(&st, d_st + id, sizeof st, cudaMemcpyDeviceToHost));
+    return st.iter;
+  }
+
+  int history(int id, double *out, int max) override {
+    Solve *s = get(id);
+    if (!s) return -1;
+    int n = iterations(id);
+    if (n <= 0) return n;
+    n = std::min(n, max);
+    std::vector<T> h(n);
+    OP2B_CUDA(cudaMemcpy(h.data(), s->dev.hist, sizeof(T) * n, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; i++) out[i] = (double)h[i];
+    return error_pending() ? -1 : n;
+  }
+
+  int fetch_q(int id, void *q) override {
+    Solve *s = get(id);
+    if (!s) return -1;
+    sync();
+    OP2B_CUDA(cudaMemcpy(q, s->dev.q, sizeof(T) * 4 * (size_t)s->ncell, cudaMemcpyDeviceToHost));
+    return error_pending() ? -1 : 0;
+  }
+
+  int remove(int id) override {
+    Solve *s = get(id);
+    if (!s) return -1;
+    release(*s);
+    changed = true;
+    return error_pending() ? -1 : 0;
+  }
+
+  long long device_bytes() override {
+    long long b = 0;
+    for (auto &s : solves)
+      if (!s.removed) b += (long long)s.bytes;
+    return b + (long long)cap * (sizeof(SolveDev<T>) + sizeof(SolveState)) +
+           (long long)(ct_cap + et_cap) * sizeof(Tile);
+  }
+
+  int active() override { return nactive; }
+
+  int set_edge_tile(int e) override {
+    if (e < kThreads || e > 8192 || e % kThreads) {
+      fail(-1, "op2b_group error -- edge tile %d: a multiple of %d in [%d, 8192]\n", e, kThreads,
+           kThreads);
+      return -1;
+    }
+    if (e != etile) changed = true;
+    etile = e;
+    return 0;
+  }
+  int edge_tile() override { return etile; }
+
+  // time each candidate edge tile on the active solves, restoring their
+  // state after each trial (the tile does not change results)
+  int autotune(int iters) override {
+    if (!ok) return -1;
+    join_pending();
+    if (changed) rebuild();
+    if (nactive == 0 || iters <= 0) return etile;
+    // snapshot of everything an iteration writes
+    std::vector<std::pair<void *, size_t>> regions;
+    for (auto &s : solves) {
+      if (!s.joined || s.removed || s.done) continue;
+      regions.push_back({s.dev.q, sizeof(T) * 4 * (size_t)s.ncell});
+      regions.push_back({s.dev.qold, sizeof(T) * 4 * (size_t)s.ncell});
+      regions.push_back({s.dev.adt, sizeof(T) * (size_t)s.ncell});
+      regions.push_back({s.dev.res, sizeof(T) * 4 * (size_t)s.ncell});
+    }
+    regions.push_back({d_st, sizeof(SolveState) * (size_t)solves.size()});
+    size_t tot = 0;
+    for (auto &r : regions) tot += align256(r.second);
+    void *snap = nullptr;
+    if (cudaMallocAsync(&snap, tot, cs) != cudaSuccess) {
+      cudaGetLastError();
+      return etile;  // no room to snapshot: keep the current tile
+    }
+    auto copy = [&](bool save) {
+      size_t o = 0;
+      for (auto &r : regions) {
+        char *sp = (char *)snap + o;
+        OP2B_CUDA(cudaMemcpyAsync(save ? sp : r.first, save ? r.first : sp, r.second,
+                                  cudaMemcpyDeviceToDevice, cs));
+        o += align256(r.second);
+      }
+    };
+    copy(true);
+    cudaEvent_t e0, e1;
+    OP2B_CUDA(cudaEventCreate(&e0));
+    OP2B_CUDA(cudaEventCreate(&e1));
+    const int cands[] = {512, 1024, 2048, 4096, 8192};
+    int best = etile;
+    float best_ms = 1e30f;
+    for (int c : cands) {
+      etile = c;
+      rebuild();
+      OP2B_CUDA(cudaGraphLaunch(exec, cs));  // warm
+      OP2B_CUDA(cudaEventRecord(e0, cs));
+      for (int i = 0; i < iters; i++) OP2B_CUDA(cudaGraphLaunch(exec, cs));
+      OP2B_CUDA(cudaEventRecord(e1, cs));
+      OP2B_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      OP2B_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = c;
+      }
+      copy(false);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    OP2B_CUDA(cudaFreeAsync(snap, cs));
+    etile = best;
+    rebuild();
+    OP2B_CUDA(cudaStreamSynchronize(cs));
+    return error_pending() ? -1 : best;
+  }
+};
+
+}  // namespace
+}  // namespace op2b
+
+using namespace op2b;
+
+struct op2b_group_s {
+  std::unique_ptr<GroupBase> impl;
+};
+
+extern "C" {
+
+int op2b_flow_qinf(double mach, double alpha_deg, int fp64, void *qinf4, void *consts4) {
+  if (!qinf4) return -1;
+  if (fp64) {
+    double q[4], c[4];
+    flow_state<double>(mach, alpha_deg, q, c);
+    memcpy(qinf4, q, sizeof q);
+    if (consts4) memcpy(consts4, c, sizeof c);
+  } else {
+    float q[4], c[4];
+    flow_state<float>(mach, alpha_deg, q, c);
+    memcpy(qinf4, q, sizeof q);
+    if (consts4) memcpy(consts4, c, sizeof c);
+  }
+  return 0;
+}
+
+op2b_group op2b_group_create(int fp64) {
+  op2b_group g = new op2b_group_s;
+  if (fp64) g->impl.reset(new Group<double>());
+  else g->impl.reset(new Group<float>());
+  if (error_pending()) {
+    delete g;
+    return nullptr;
+  }
+  return g;
+}
+
+void op2b_group_destroy(op2b_group g) { delete g; }
+
+#define GROUP_CALL(expr) \
+  do {                   \
+    if (!g) return -1;   \
+    return g->impl->expr; \
+  } while (0)
+
+int op2b_group_add(op2b_group g, const op2b_mesh *m, double mach, double alpha_deg, int max_iter,
+                   double rel_tol) {
+  GROUP_CALL(add(m, mach, alpha_deg, max_iter, rel_tol));
+}
+int op2b_group_run(op2b_group g, int niter) { GROUP_CALL(run(niter)); }
+int op2b_group_poll(op2b_group g, int *ids, int max) { GROUP_CALL(poll(ids, max)); }
+int op2b_group_sync(op2b_group g) { GROUP_CALL(sync()); }
+int op2b_group_iterations(op2b_group g, int id) { GROUP_CALL(iterations(id)); }
+int op2b_group_history(op2b_group g, int id, double *rms, int max) {
+  GROUP_CALL(history(id, rms, max));
+}
+int op2b_group_fetch_q(op2b_group g, int id, void *q) { GROUP_CALL(fetch_q(id, q)); }
+int op2b_group_remove(op2b_group g, int id) { GROUP_CALL(remove(id)); }
+long long op2b_group_solve_bytes(op2b_group g, int nnode, int ncell, int nedge, int nbedge,
+                                 int max_iter) {
+  GROUP_CALL(solve_bytes(nnode, ncell, nedge, nbedge, max_iter));
+}
+long long op2b_group_device_bytes(op2b_group g) { GROUP_CALL(device_bytes()); }
+int op2b_group_active(op2b_group g) { GROUP_CALL(active()); }
+int op2b_group_set_edge_tile(op2b_group g, int e) { GROUP_CALL(set_edge_tile(e)); }
+int op2b_group_edge_tile(op2b_group g) { GROUP_CALL(edge_tile()); }
+int op2b_group_autotune(op2b_group g, int iters) { GROUP_CALL(autotune(iters)); }
+
+}  // extern "C"

@@ -61,20 +61,32 @@ def naca0012(I, J, scramble=False, seed=SEED):
         lib.op2b_mesh_free(C.byref(m))
 
 
-def write_grid(mesh, path):
-    """Write new_grid.dat (naca0012.m:328-351) for the reference apps."""
-    lib = _lib.load()
+def as_struct(mesh):
+    """An op2b_mesh view of an AirfoilMesh's arrays; returns (struct, keep),
+    where `keep` must outlive every use of the struct."""
     m = _lib.op2b_mesh()
     keep = []
 
-    def ptr(a, ct):
-        a = np.ascontiguousarray(a)
+    def ptr(a, ct, dt):
+        a = np.ascontiguousarray(a, dtype=dt)
         keep.append(a)
         return a.ctypes.data_as(C.POINTER(ct))
     m.nnode, m.ncell, m.nedge, m.nbedge = mesh.nnode, mesh.ncell, mesh.nedge, mesh.nbedge
-    m.cell, m.edge, m.ecell = ptr(mesh.cell, C.c_int), ptr(mesh.edge, C.c_int), ptr(mesh.ecell, C.c_int)
-    m.bedge, m.becell, m.bound = ptr(mesh.bedge, C.c_int), ptr(mesh.becell, C.c_int), ptr(mesh.bound, C.c_int)
-    m.x64, m.x32 = ptr(mesh.x64, C.c_double), ptr(mesh.x32, C.c_float)
+    m.cell = ptr(mesh.cell, C.c_int, np.int32)
+    m.edge = ptr(mesh.edge, C.c_int, np.int32)
+    m.ecell = ptr(mesh.ecell, C.c_int, np.int32)
+    m.bedge = ptr(mesh.bedge, C.c_int, np.int32)
+    m.becell = ptr(mesh.becell, C.c_int, np.int32)
+    m.bound = ptr(mesh.bound, C.c_int, np.int32)
+    m.x64 = ptr(mesh.x64, C.c_double, np.float64)
+    m.x32 = ptr(mesh.x32, C.c_float, np.float32)
+    return m, keep
+
+
+def write_grid(mesh, path):
+    """Write new_grid.dat (naca0012.m:328-351) for the reference apps."""
+    lib = _lib.load()
+    m, keep = as_struct(mesh)
     if lib.op2b_mesh_write(C.byref(m), str(path).encode()) != 0:
         raise IOError("cannot write %s" % path)
 

@@ -14,7 +14,7 @@ from oplus2_matlab_b200 import _lib
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 INCLUDE = os.path.join(ROOT, "include")
-HEADERS = ["op_lib_core.h", "op_lib.h", "op2b.h", "op2b_mesh.h"]
+HEADERS = ["op_lib_core.h", "op_lib.h", "op2b.h", "op2b_mesh.h", "op2b_group.h"]
 
 
 def declared_functions(header):
