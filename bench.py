@@ -64,6 +64,20 @@ def parse():
     ap.add_argument("--e2e-iters", type=int, default=1000)
     ap.add_argument("--tune", action="append", default=[],
                     help="kernel-variant knob key=value (op2b_set_tuning)")
+    ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"],
+                    help="plain: the 720k single-mesh iteration (default); batched: many "
+                         "instances per launch; served: a Poisson request stream")
+    ap.add_argument("--instances", type=int, default=64, help="batched: instances")
+    ap.add_argument("--iters", type=int, default=500, help="batched: iterations per instance")
+    ap.add_argument("--requests", type=int, default=10000, help="served: requests")
+    ap.add_argument("--rate", type=float, default=200.0, help="served: mean arrivals per second")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="served: HBM budget")
+    ap.add_argument("--max-iter", type=int, default=2000, help="served: iteration cap")
+    ap.add_argument("--rel-tol", type=float, default=1e-6, help="served: rms tolerance")
+    ap.add_argument("--iters-per-step", type=int, default=10,
+                    help="served: iterations between completion checks")
+    ap.add_argument("--plain-sample", type=int, default=16,
+                    help="served: requests re-solved with the plain path for its rate")
     return ap.parse_args()
 
 
@@ -513,12 +527,192 @@ def cpu_baseline(mesh, fp64):
                       "sum of its op_timing_output)" % niter}
 
 
+# ------------------------------------------------------ batched / served ----
+
+def warm_paths(dt):
+    """Untimed: create the CUDA context and load the kernels of both paths
+    (lazy module loading) on a tiny mesh, so neither timed region pays the
+    process's one-time start-up."""
+    from oplus2_matlab_b200 import group as G
+    from oplus2_matlab_b200 import mesh as M
+    tiny = M.naca0012(10, 15)
+    g = G.Group(dt)
+    g.add(tiny, 0.5, 1.0, 3)
+    g.autotune(1)
+    g.run(3)
+    g.sync()
+    g.close()
+    G.plain_solve(tiny, 0.5, 1.0, 3, dt)
+
+
+def impl_batched(args, dist):
+    """64 seeded instances (20k-720k cells, Mach 0.3-0.7, alpha -2..6 deg),
+    `iters` iterations each: the group engine (every loop one launch over all
+    instances, edge tile autotuned) against the same instances solved one
+    after another through the plain C API.  Both timed end to end: host
+    arrays in, rms histories and q out; mesh generation (the input) is not
+    timed.  N ranks share the instances by greedy cell balance."""
+    from oplus2_matlab_b200 import group as G
+    from oplus2_matlab_b200 import mesh as M
+    from oplus2_matlab_b200 import serve as S
+    from oplus2_matlab_b200 import api
+    dt = np.float64 if args.fp64 else np.float32
+    inst = G.draw_instances(args.instances, cmin=20000, cmax=720000)
+    cells = [3 * I * J for I, J, _, _ in inst]
+    mine = S.shard_by_cells(cells, dist.world)[dist.rank]
+    meshes = {}
+    for i in mine:
+        I, J = inst[i][:2]
+        if (I, J) not in meshes:
+            meshes[(I, J)] = M.naca0012(I, J)
+    api.set_error_mode(api.ERRORS_RETURN)
+    warm_paths(dt)
+    n = args.iters
+
+    dist.barrier()
+    t0 = time.perf_counter()
+    g = G.Group(dt)
+    ids = [g.add(meshes[inst[i][:2]], inst[i][2], inst[i][3], n) for i in mine]
+    tile = g.autotune(3)
+    ti = time.perf_counter()
+    g.run(n)
+    g.sync()
+    t_iter = time.perf_counter() - ti
+    hist = [g.history(s) for s in ids]
+    qg = [g.fetch_q(s) for s in ids]
+    t_group = dist.max(time.perf_counter() - t0)
+    gbytes = g.device_bytes()
+    g.close()
+
+    dist.barrier()
+    t0 = time.perf_counter()
+    plain = [G.plain_solve(meshes[inst[i][:2]], inst[i][2], inst[i][3], n, dt) for i in mine]
+    t_plain = dist.max(time.perf_counter() - t0)
+
+    exact = sum(int(a.tobytes() == p[0].astype(dt).tobytes()) for a, p in zip(qg, plain))
+    rel = max(float(np.max(np.abs(h - p[1]) / np.abs(p[1]))) for h, p in zip(hist, plain))
+    s = 8 if args.fp64 else 4
+    my_bytes = sum(iteration_bytes(meshes[inst[i][:2]], s) for i in mine) * n
+    total = len(inst)
+    line = {
+        "metric": "batched airfoil solves/s", "value": total / t_group, "unit": "solves/s",
+        "n_gpus": dist.world, "steps": n, "warmup": 0, "ms_per_step": 1e3 * t_group / n,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f64" if args.fp64 else "f32",
+        "data": "synthetic: %d seeded NACA0012 C-meshes, cells log-uniform 20k-720k, "
+                "Mach U[0.3,0.7], alpha U[-2,6] deg (splitmix64 seed %d)" % (total, M.SEED),
+        "config": {"workload": "airfoil batched: %d instances x %d iterations, %d cells in all"
+                               % (total, n, sum(cells)),
+                   "instances": total, "iterations": n, "cells_total": sum(cells),
+                   "timing": "wall clock, host arrays in to rms histories and q out, "
+                             "mesh generation excluded",
+                   "parallelism": "instances sharded by cells over %d GPU(s)" % dist.world},
+        "group": {"seconds": t_group, "iterate_seconds_rank0": t_iter,
+                  "edge_tile_autotuned": tile, "device_bytes_rank0": gbytes,
+                  "iteration_gbs_rank0": my_bytes / t_iter / 1e9},
+        "plain_back_to_back": {"seconds": t_plain, "solves_per_s": total / t_plain,
+                               "path": "op2b_airfoil_app_flow per instance (op_par_loop, "
+                                       "rms to the host after every update)"},
+        "speedup_vs_plain": t_plain / t_group,
+        "parity_rank0": {"q_bit_identical": "%d/%d" % (exact, len(mine)),
+                         "max_rms_rel_diff": rel},
+        "gpu_launches": 5 * n,
+    }
+    if dist.rank == 0:
+        print(json.dumps(line))
+
+
+def impl_served(args, dist):
+    """A Poisson request stream (rate, seeded) of meshes of 10k-720k cells,
+    each solved until rms < rel_tol x its first rms or max_iter iterations,
+    through the continuous-batching server under an HBM budget; p50/p99
+    latency from arrival to result and solves/s.  Against: the same
+    requests' solves through the plain C API, one after another, timed on a
+    sample and scaled.  Ranks take every N-th request."""
+    from oplus2_matlab_b200 import group as G
+    from oplus2_matlab_b200 import mesh as M
+    from oplus2_matlab_b200 import serve as S
+    from oplus2_matlab_b200 import api
+    dt = np.float64 if args.fp64 else np.float32
+    inst = G.draw_instances(args.requests, seed=M.SEED + 1, cmin=10000, cmax=720000)
+    rng = np.random.default_rng(M.SEED)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, args.requests))
+    mine = list(range(dist.rank, args.requests, dist.world))
+    meshes = {}
+    for i in mine:
+        I, J = inst[i][:2]
+        if (I, J) not in meshes:
+            meshes[(I, J)] = M.naca0012(I, J)
+    api.set_error_mode(api.ERRORS_RETURN)
+    warm_paths(dt)
+    srv = S.Server(dt, budget_bytes=args.budget_gb * 1e9, iters_per_step=args.iters_per_step)
+    reqs = [S.Request(i, meshes[inst[i][:2]], inst[i][2], inst[i][3], args.max_iter,
+                      args.rel_tol, float(arrivals[i])) for i in mine]
+    dist.barrier()
+    t0 = time.perf_counter()
+    srv.clock = lambda: time.perf_counter() - t0
+    nxt = 0
+    while nxt < len(reqs) or not srv.idle():
+        now = srv.clock()
+        while nxt < len(reqs) and reqs[nxt].arrival <= now:
+            srv.submit(reqs[nxt])
+            nxt += 1
+        if srv.idle() and nxt < len(reqs):
+            time.sleep(max(0.0, min(reqs[nxt].arrival - srv.clock(), 0.01)))
+            continue
+        srv.step()
+    wall = dist.max(time.perf_counter() - t0)
+    stats = S.latency_stats(srv.done)
+    iters = np.array([r.iterations for r in srv.done])
+    max_active = srv.max_active
+    srv.close()
+
+    # the plain path on a sample of the same requests, same iteration counts
+    sample = srv.done[:max(1, min(args.plain_sample, len(srv.done)))]
+    t0 = time.perf_counter()
+    for r in sample:
+        G.plain_solve(r.mesh, r.mach, r.alpha, r.iterations, dt)
+    t_sample = time.perf_counter() - t0
+    frac = sum(r.iterations * r.mesh.ncell for r in sample) / max(
+        1, sum(r.iterations * r.mesh.ncell for r in srv.done))
+    plain_serial_s = t_sample / max(frac, 1e-12)  # the whole stream, scaled by cell-iterations
+    line = {
+        "metric": "served airfoil solves/s", "value": args.requests / wall, "unit": "solves/s",
+        "n_gpus": dist.world, "steps": args.requests, "warmup": 0,
+        "ms_per_step": 1e3 * wall / args.requests, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64" if args.fp64 else "f32",
+        "data": "synthetic: Poisson(%g/s) arrivals, seeded NACA0012 meshes 10k-720k cells, "
+                "Mach U[0.3,0.7], alpha U[-2,6] deg" % args.rate,
+        "config": {"workload": "airfoil served: %d requests, stop at rms < %g x first or %d "
+                               "iterations, %g GB budget" % (args.requests, args.rel_tol,
+                                                              args.max_iter, args.budget_gb),
+                   "iters_per_step": args.iters_per_step,
+                   "parallelism": "requests dealt round-robin over %d GPU(s)" % dist.world},
+        "latency": stats,
+        "wall_seconds": wall,
+        "iterations": {"mean": float(iters.mean()), "min": int(iters.min()),
+                       "max": int(iters.max())},
+        "max_active_solves_rank0": max_active,
+        "plain_serial": {"sample": len(sample), "sample_seconds": t_sample,
+                         "estimated_seconds": plain_serial_s,
+                         "solves_per_s": args.requests / plain_serial_s,
+                         "scaled_by": "cell-iterations of the sample over the stream"},
+        "speedup_vs_plain": plain_serial_s / wall,
+    }
+    if dist.rank == 0:
+        print(json.dumps(line))
+
+
 def main():
     args = parse()
     dist = Dist()
     try:
         if args.impl == "reference":
             impl_reference(args, dist)
+        elif args.mode == "batched":
+            impl_batched(args, dist)
+        elif args.mode == "served":
+            impl_served(args, dist)
         else:
             impl_ours(args, dist)
     finally:
