@@ -47,6 +47,11 @@ enum { OP2B_REDUCE_TREE = 0, OP2B_REDUCE_SEQ = 1 };
  *   "unroll"        elements per thread in the direct loops (1, 2, 4) */
 int op2b_set_tuning(const char *key, int value);
 
+/* op_decl_const of include/op_seq.h (the sequential API's unnamed form,
+ * op_lib.h:177-182): declares the constant under the name written in `expr`,
+ * the app's argument expression ("&gam" -> "gam", "qinf" -> "qinf"). */
+void op2b_decl_const_named(int dim, const char *type, int size, char *dat, const char *expr);
+
 /* Errors: EXIT (default, like the reference: print and exit) or RETURN
  * (print, remember the message, return NULL / do nothing). */
 enum { OP2B_ERRORS_EXIT = 0, OP2B_ERRORS_RETURN = 1 };

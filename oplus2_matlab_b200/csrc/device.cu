@@ -242,6 +242,23 @@ void op_decl_const_char(int dim, char const *type, int size, char *dat, char con
   rt().consts_version++;
 }
 
+// op_seq.h's unnamed op_decl_const(dim, type, ptr): the name is the
+// expression the app wrote ("&gam", "qinf", "& alpha"), without the address
+// operator, blanks and enclosing parentheses
+void op2b_decl_const_named(int dim, char const *type, int size, char *dat, char const *expr) {
+  std::string e = expr ? expr : "";
+  std::string n;
+  for (char ch : e)
+    if (ch != ' ' && ch != '\t' && ch != '(' && ch != ')') n += ch;
+  while (!n.empty() && n[0] == '&') n.erase(0, 1);
+  if (n.empty()) {
+    fail(-1, "op_decl_const error -- cannot name the constant passed as \"%s\"\n",
+         expr ? expr : "(null)");
+    return;
+  }
+  op_decl_const_char(dim, type, size, dat, n.c_str());
+}
+
 // common/op_lib.cu:116-121: device -> the caller's original array
 void op_fetch_data(op_dat dat) {
   flush_pending();

@@ -1,9 +1,11 @@
-"""Drop-in: the reference's unchanged generated mains linked against this
-library.
+"""Drop-in: the reference's unchanged app mains linked against this library.
 
-oracle/Makefile (target `dropin`) compiles airfoil/airfoil_op.cpp,
-jac1/jac_op.cpp and jac2/jac_op.cpp, exactly as the reference ships them,
-against include/ and libop2b200.so (no generated CUDA stubs).  Here: every
+oracle/Makefile (target `dropin`) compiles, exactly as the reference ships
+them, against include/ and libop2b200.so (no generated CUDA stubs):
+  - the generated mains airfoil/airfoil_op.cpp, jac1/jac_op.cpp,
+    jac2/jac_op.cpp (op_par_loop_<name> entry points), and
+  - the un-generated mains airfoil/airfoil.cpp, jac1/jac.cpp, jac2/jac.cpp
+    (the template op_par_loop of op_seq.h, here include/op_seq.h).  Here: every
 OP2 symbol those binaries import must come from the library, and on the GPU
 their printed results must match the reference's own sequential build
 (the goldens made from it): airfoil's rms every 100 iterations (printed
@@ -23,7 +25,7 @@ from oplus2_matlab_b200 import mesh as M
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DROPIN = os.path.join(ROOT, "oracle", "_ref", "dropin")
-APPS = ["airfoil_op", "jac1_op", "jac2_op"]
+APPS = ["airfoil_op", "jac1_op", "jac2_op", "airfoil_seqapi", "jac1_seqapi", "jac2_seqapi"]
 
 
 def binary(name):
@@ -43,7 +45,9 @@ def dynsyms(path, flag):
 def test_dropin_imports_every_op2_symbol_from_the_library(app):
     path = binary(app)
     need = {s for s in dynsyms(path, "--undefined-only") if s.startswith(("op_", "OP_"))}
-    assert "op_par_loop_update" in need and "op_init" in need
+    assert "op_init" in need
+    assert "op_par_loop_update" in need or "op2b_par_loop" in dynsyms(path, "--undefined-only")
+    need |= {s for s in dynsyms(path, "--undefined-only") if s.startswith("op2b_")}
     have = dynsyms(_lib.LIB_PATH, "--defined-only")
     assert need <= have, sorted(need - have)
     ldd = subprocess.run(["ldd", path], capture_output=True, text=True).stdout
@@ -57,8 +61,9 @@ def run(path, cwd):
 
 
 @pytest.mark.gpu
-def test_dropin_airfoil_matches_reference_rms():
-    path = binary("airfoil_op")
+@pytest.mark.parametrize("app", ["airfoil_op", "airfoil_seqapi"])
+def test_dropin_airfoil_matches_reference_rms(app):
+    path = binary(app)
     gold = load_golden("airfoil_40x60_f32")
     d = scratch_dir()
     M.write_grid(M.naca0012(40, 60), os.path.join(d, "new_grid.dat"))
@@ -73,7 +78,8 @@ def test_dropin_airfoil_matches_reference_rms():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("app,case", [("jac1_op", "jac1_nn6"), ("jac2_op", "jac2_nn6")])
+@pytest.mark.parametrize("app,case", [("jac1_op", "jac1_nn6"), ("jac2_op", "jac2_nn6"),
+                                      ("jac1_seqapi", "jac1_nn6"), ("jac2_seqapi", "jac2_nn6")])
 def test_dropin_jac_matches_reference(app, case):
     path = binary(app)
     gold = load_golden(case)
