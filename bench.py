@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--e2e-iters", type=int, default=1000)
     ap.add_argument("--tune", action="append", default=[],
                     help="kernel-variant knob key=value (op2b_set_tuning)")
+    ap.add_argument("--mesh", default="400x600",
+                    help="plain mode: IxJ of the NACA0012 C-mesh (3IJ cells); a trailing 's' "
+                         "renumbers cells, nodes, edges and bedges from the seed (scrambled)")
     ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"],
                     help="plain: the 720k single-mesh iteration (default); batched: many "
                          "instances per launch; served: a Poisson request stream")
@@ -294,6 +297,23 @@ def impl_reference(args, dist):
 
 # ------------------------------------------------------------------ ours ----
 
+def plain_mesh(args):
+    from oplus2_matlab_b200 import mesh as M
+    spec = args.mesh.lower()
+    scramble = spec.endswith("s")
+    I, J = (int(v) for v in spec.rstrip("s").split("x"))
+    return M.naca0012(I, J, scramble=scramble)
+
+
+def workload_name(mesh, args):
+    if args.mesh == "400x600":
+        return ("airfoil 720k cells (I=400, J=600: 720,000 cells, 1,438,600 edges, "
+                "721,801 nodes, 2,800 bedges), one outer iteration per step")
+    return ("airfoil %s (%s%d cells, %d edges, %d nodes, %d bedges), one outer iteration per step"
+            % (args.mesh, "scrambled numbering, " if args.mesh.endswith("s") else "",
+               mesh.ncell, mesh.nedge, mesh.nnode, mesh.nbedge))
+
+
 def impl_ours(args, dist):
     from oplus2_matlab_b200 import api, apps
     from oplus2_matlab_b200 import mesh as M
@@ -302,7 +322,7 @@ def impl_ours(args, dist):
     dt = np.float64 if args.fp64 else np.float32
     s = 8 if args.fp64 else 4
 
-    mesh = M.naca0012(I_MESH, J_MESH)
+    mesh = plain_mesh(args)
     api.set_error_mode(api.ERRORS_RETURN)
     api.op_init([], 0)
     api.set_strategy(api.STRATEGY_GATHER if args.strategy == "gather" else api.STRATEGY_COLOURED)
@@ -425,8 +445,7 @@ def impl_ours(args, dist):
         "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.fp64 else "f32",
         "data": "synthetic: NACA0012 C-mesh from the reference's generator, free-stream start",
-        "config": {"workload": "airfoil 720k cells (I=400, J=600: 720,000 cells, 1,438,600 edges, "
-                               "721,801 nodes, 2,800 bedges), one outer iteration per step",
+        "config": {"workload": workload_name(mesh, args),
                    "cells": mesh.ncell, "edges": mesh.nedge, "strategy": args.strategy,
                    "reduction": "tree", "l2": "flushed before every step (untimed read-only sweep of 3x the 126 MB L2)",
                    "timing": "CUDA events around each graph launch on the library stream",
