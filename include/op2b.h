@@ -47,6 +47,21 @@ enum { OP2B_REDUCE_TREE = 0, OP2B_REDUCE_SEQ = 1 };
  *   "unroll"        elements per thread in the direct loops (1, 2, 4) */
 int op2b_set_tuning(const char *key, int value);
 
+/* Renumber every set for locality of the indirect gathers (off by default).
+ * Call before the first loop; the first loop call then orders the sets
+ * (Cuthill-McKee on the set most maps point to, the others following through
+ * the maps), stores every dataset in the new order on the device and maps in
+ * the new numbering.  op_fetch_data returns data in the app's order, and
+ * results are the same as without renumbering (contributions still follow
+ * the app's element order); plans from op_plan_get describe the renumbered
+ * sets, and TREE-mode global sums are summed in another order.  Returns 0,
+ * or -1 when turning it off after it has been applied. */
+int op2b_set_renumber(int on);
+/* The new -> old order renumbering would give `set` (computed from the sets
+ * and maps declared so far; host only).  Returns 1 if the set is reordered,
+ * 0 if it keeps its numbering (new2old = identity), -1 on bad arguments. */
+int op2b_renumber_order(op_set set, int *new2old);
+
 /* op_decl_const of include/op_seq.h (the sequential API's unnamed form,
  * op_lib.h:177-182): declares the constant under the name written in `expr`,
  * the app's argument expression ("&gam" -> "gam", "qinf" -> "qinf"). */

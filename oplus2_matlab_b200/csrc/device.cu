@@ -12,6 +12,8 @@
 
 #include "internal.h"
 
+void op2b_release_plans();  // plan.cu
+
 namespace op2b {
 
 void release_fused_plans();  // airfoil.cu
@@ -65,11 +67,25 @@ const int *map_dev(op_map m) {
     size_t bytes = sizeof(int) * (size_t)m->dim * m->from->size;
     md.d = (int *)dev_alloc(bytes);
     if (md.d) {
-      OP2B_CUDA(cudaMemcpyAsync(md.d, m->map, bytes, cudaMemcpyHostToDevice, R.stream));
+      // renumbered sets: rows in the from-set's new order, values in the
+      // to-set's new numbering
+      std::vector<int> rn = renumbered_map(m);
+      OP2B_CUDA(cudaMemcpyAsync(md.d, rn.empty() ? (const int *)m->map : rn.data(), bytes,
+                                cudaMemcpyHostToDevice, R.stream));
       OP2B_CUDA(cudaStreamSynchronize(R.stream));
     }
   }
   return md.d;
+}
+
+// device copies of maps and every plan, rebuilt on next use
+void release_plans_and_maps() {
+  ::op2b_release_plans();
+  release_fused_plans();
+  for (auto &m : rt().maps) {
+    dev_free(m.d);
+    m.d = nullptr;
+  }
 }
 
 static bool capturing() {
@@ -220,6 +236,7 @@ op_dat op_decl_dat_char(op_set set, int dim, char const *type, int size, char *d
   if (data) OP2B_CUDA(cudaMemcpyAsync(dat->data_d, data, bytes, cudaMemcpyHostToDevice, R.stream));
   else OP2B_CUDA(cudaMemsetAsync(dat->data_d, 0, bytes, R.stream));
   OP2B_CUDA(cudaStreamSynchronize(R.stream));
+  permute_dat_in_place(dat);  // when its set has been renumbered
   return dat;
 }
 
@@ -265,6 +282,7 @@ void op_fetch_data(op_dat dat) {
   if (!dat || !dat->data_d) return;
   Runtime &R = rt();
   deliver_deferred();
+  if (fetch_unpermuted(dat, dat->data)) return;  // renumbered set: the app's order back
   OP2B_CUDA(cudaMemcpyAsync(dat->data, dat->data_d, (size_t)dat->size * dat->set->size,
                             cudaMemcpyDeviceToHost, R.stream));
   OP2B_CUDA(cudaStreamSynchronize(R.stream));
@@ -281,6 +299,7 @@ void op_exit(void) {
   }
   op2b_release_plans();
   release_fused_plans();
+  renumber_reset();
   for (auto &m : R.maps) dev_free(m.d);
   R.maps.clear();
   for (int i = 0; i < OP_dat_index; i++) dev_free(OP_dat_list[i]->data_d);

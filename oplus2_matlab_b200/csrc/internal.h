@@ -148,6 +148,16 @@ struct PhaseScope {
 int const_get_f32(char const *name, float *out, int n);
 int const_get_f64(char const *name, double *out, int n);
 
+// renumbering of the sets for locality (renumber.cu)
+bool renumber_enabled();
+void renumber_apply();                 // first loop call: order the sets, move the data
+void renumber_reset();                 // op_exit
+const int *perm_new2old_dev(op_set s);  // device permutation, nullptr when not renumbered
+const int *perm_old2new_dev(op_set s);
+void permute_dat_in_place(op_dat d);   // a dataset declared after renumbering
+bool fetch_unpermuted(op_dat d, void *host);  // false: not renumbered, nothing done
+std::vector<int> renumbered_map(op_map m);    // empty: map unchanged
+
 // global reductions: device slot management (reduce.cu)
 void deliver_deferred();
 

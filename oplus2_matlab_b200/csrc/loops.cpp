@@ -320,6 +320,10 @@ void op2b_par_loop(char const *name, op_set set, int nargs, const op_arg *args) 
     ensure_cuda();
     if (error_pending()) return;
   }
+  if (renumber_enabled()) {
+    renumber_apply();  // once, at the first loop: order the sets, move the data
+    if (error_pending()) return;
+  }
   // the checks op_seq.h runs when OP_diags > 0 (common/op_seq.h:37-39); a
   // device loop always runs them, since bad arguments would fault the GPU
   int ninds = 0;

@@ -1055,6 +1055,15 @@ __global__ void k_sort_long_rows(const int *row, const int *long_rows, int *keys
   for (int i = threadIdx.x; i < len; i += blockDim.x) keys[a + i] = s[i];
 }
 
+// key = element * nslots + slot -> perm[element] * nslots + slot
+__global__ void k_keys_through(int *keys, long long n, int nslots, const int *perm) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int k = keys[i];
+    keys[i] = perm[k / nslots] * nslots + k % nslots;
+  }
+}
+
 GatherPlan *get_gather_plan(op_set set, const op_arg *args, const std::vector<int> &slots) {
   for (auto &up : g_gather) {
     GatherPlan &g = *up;
@@ -1120,6 +1129,11 @@ GatherPlan *get_gather_plan(op_set set, const op_arg *args, const std::vector<in
   OP2B_CUDA(cudaMemcpyAsync(cursor, g.d_row, sizeof(int) * ((size_t)g.nactive + 1),
                             cudaMemcpyDeviceToDevice, s));
   k_gather_scatter<<<grid, 256, 0, s>>>(sm, g.nslots, n, slot_of_target, cursor, g.d_keys);
+  // renumbered loop set: order each row by the app's element numbers (the
+  // order of op_seq.h), then turn the keys back into device numbers below
+  const int *to_orig = perm_new2old_dev(set), *to_dev = perm_old2new_dev(set);
+  if (to_orig && nkeys)
+    k_keys_through<<<grid, 256, 0, s>>>(g.d_keys, nkeys, g.nslots, to_orig);
   OP2B_CUDA(cudaMallocAsync((void **)&long_rows, sizeof(int) * std::max(1, g.nactive), s));
   OP2B_CUDA(cudaMallocAsync((void **)&nlong, sizeof(int) * 2, s));
   maxlen = nlong + 1;
@@ -1144,6 +1158,7 @@ GatherPlan *get_gather_plan(op_set set, const op_arg *args, const std::vector<in
     allow_smem(k_sort_long_rows);
     k_sort_long_rows<<<h[0], 1024, sizeof(int) * P, s>>>(g.d_row, long_rows, g.d_keys);
   }
+  if (to_dev && nkeys) k_keys_through<<<grid, 256, 0, s>>>(g.d_keys, nkeys, g.nslots, to_dev);
   OP2B_CUDA(cudaFreeAsync(cnt, s));
   OP2B_CUDA(cudaFreeAsync(flags, s));
   OP2B_CUDA(cudaFreeAsync(pos, s));

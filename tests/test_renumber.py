@@ -1,0 +1,97 @@
+"""Renumbering for locality (op2b_set_renumber).
+
+On the host: the orders are permutations, and on a scrambled mesh they bring
+the two cells of an edge, and an edge and its cells, close together again.
+On the device: with renumbering on, the scrambled airfoil's final fields are
+still bit-identical to the reference's sequential build (contributions keep
+the app's element order) and come back from op_fetch_data in the app's
+order; the TREE rms stays within its summation tolerance; jac is unchanged.
+"""
+import ctypes as C
+import hashlib
+import os
+import subprocess
+import sys
+import textwrap
+
+import numpy as np
+import pytest
+
+from conftest import load_golden
+from oplus2_matlab_b200 import _lib, apps
+from oplus2_matlab_b200 import mesh as M
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def test_orders_are_permutations_that_restore_locality():
+    code = textwrap.dedent("""
+        import sys, ctypes as C, numpy as np
+        sys.path.insert(0, %r)
+        from oplus2_matlab_b200 import api, _lib, mesh as M
+        L = _lib.load()
+        m = M.naca0012(40, 60, scramble=True)
+        nodes = api.op_decl_set(m.nnode, "nodes"); edges = api.op_decl_set(m.nedge, "edges")
+        bedges = api.op_decl_set(m.nbedge, "bedges"); cells = api.op_decl_set(m.ncell, "cells")
+        api.op_decl_map(edges, nodes, 2, m.edge, "pedge")
+        api.op_decl_map(edges, cells, 2, m.ecell, "pecell")
+        api.op_decl_map(bedges, nodes, 2, m.bedge, "pbedge")
+        api.op_decl_map(bedges, cells, 1, m.becell, "pbecell")
+        api.op_decl_map(cells, nodes, 4, m.cell, "pcell")
+        P = {}
+        for name, s, n in (("nodes", nodes, m.nnode), ("edges", edges, m.nedge),
+                           ("bedges", bedges, m.nbedge), ("cells", cells, m.ncell)):
+            p = np.zeros(n, np.int32)
+            assert L.op2b_renumber_order(s, p.ctypes.data_as(C.POINTER(C.c_int))) == 1
+            assert np.array_equal(np.sort(p), np.arange(n)), name
+            P[name] = p
+        Qc = np.argsort(P["cells"]); Qn = np.argsort(P["nodes"])
+        # spread of an edge's two cells, and of consecutive edges' cells
+        before = np.abs(m.ecell[:, 0] - m.ecell[:, 1]).mean()
+        after = np.abs(Qc[m.ecell[:, 0]] - Qc[m.ecell[:, 1]]).mean()
+        e_new = m.ecell[P["edges"]]
+        jump_before = np.abs(np.diff(m.ecell[:, 0])).mean()
+        jump_after = np.abs(np.diff(Qc[e_new[:, 0]])).mean()
+        print(before, after, jump_before, jump_after)
+        assert after < before / 20 and jump_after < jump_before / 20
+        nodes_after = np.abs(Qn[m.cell[P["cells"]][:, 0]] - np.arange(m.ncell)).mean()
+        assert nodes_after < m.nnode / 20
+    """ % ROOT)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["airfoil_40x60s_f32", "airfoil_40x60_f32"])
+def test_renumbered_airfoil_fields_bit_identical(op2, case):
+    g = load_golden(case)
+    m = M.naca0012(g["I"], g["J"], scramble=g["scramble"])
+    op2.set_strategy(op2.STRATEGY_GATHER)
+    op2.set_reduction(op2.REDUCE_TREE)
+    assert _lib.load().op2b_set_renumber(1) == 0
+    A = apps.Airfoil(m, np.float32)
+    rms = A.iterate(g["niter"])
+    st = A.fetch()
+    assert op2.last_error() == ""
+    for f, key in (("p_q", "q"), ("p_qold", "qold"), ("p_res", "res"), ("p_adt", "adt")):
+        assert sha(st[key]) == g["final"][f]["sha256"], f
+    ref = np.array([v for _, v in g["rms"]])
+    assert np.max(np.abs(rms - ref) / ref) < 5e-5
+
+
+@pytest.mark.gpu
+def test_renumbered_jac1_matches_reference(op2):
+    g = load_golden("jac1_nn64")
+    op2.set_strategy(op2.STRATEGY_GATHER)
+    op2.set_reduction(op2.REDUCE_TREE)
+    assert _lib.load().op2b_set_renumber(1) == 0
+    jm = M.jac(g["NN"], g["variant"])
+    J = apps.Jac(jm, g["variant"])
+    J.iterate(g["niter"])
+    u = J.fetch()
+    assert op2.last_error() == ""
+    assert sha(u) == g["u_sha256"]
