@@ -9,6 +9,7 @@
 // direct loops stream 16-byte vectors per thread, which coalesces fully.
 
 #include <stdio.h>
+#include <stdlib.h>
 
 #include "internal.h"
 
@@ -28,6 +29,15 @@ void ensure_cuda() {
          err == cudaSuccess ? "0 devices" : cudaGetErrorString(err));
     return;
   }
+  // Host waits spin rather than yield: the drop-in API returns every global
+  // reduction to the caller before the loop call returns, so each update is
+  // a host round trip and its wake-up latency is GPU idle time.  This is a
+  // flag of this process's context (set before it exists; ignored if the
+  // process created it already); OP2B_SYNC_YIELD=1 keeps the default.
+  const char *yield = getenv("OP2B_SYNC_YIELD");
+  if (!(yield && yield[0] == '1') &&
+      cudaSetDeviceFlags(cudaDeviceScheduleSpin | cudaDeviceMapHost) != cudaSuccess)
+    cudaGetLastError();
   OP2B_CUDA(cudaGetDevice(&R.device));
   cudaDeviceProp prop;
   OP2B_CUDA(cudaGetDeviceProperties(&prop, R.device));

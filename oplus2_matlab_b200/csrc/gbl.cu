@@ -7,6 +7,8 @@
 // when the loop call returns.  In deferred mode the device results wait in
 // slots until op2b_sync / op_fetch_data, so no call blocks.
 
+#include <string.h>
+
 #include <algorithm>
 
 #include "loops.h"
@@ -16,8 +18,10 @@ namespace op2b {
 namespace {
 constexpr int kSlots = 4096;
 struct RedState {
-  char *dev = nullptr;  // [2 x kMaxRedBlocks x 8] partials | ticket (256 B) | slots
-  char *host = nullptr; // pinned mirror of the slots
+  char *dev = nullptr;  // [2 x kMaxRedBlocks x 8] partials | ticket (256 B)
+  // result slots in mapped pinned host memory: the last block of a reduction
+  // stores the result where the host reads it, so delivery needs no copy
+  char *host = nullptr;
   int next_slot = 0;
   int graph_slots = 0;  // slots baked into captured graphs stay reserved
   void *seq = nullptr;
@@ -33,10 +37,11 @@ size_t off_slots() { return off_ticket() + 256; }
 void ensure_red() {
   RedState &S = rs();
   if (S.dev) return;
-  size_t bytes = off_slots() + (size_t)kSlots * 8;
+  size_t bytes = off_slots();
   S.dev = (char *)dev_alloc(bytes);
   OP2B_CUDA(cudaMemset(S.dev, 0, bytes));
-  OP2B_CUDA(cudaMallocHost((void **)&S.host, (size_t)kSlots * 8));
+  OP2B_CUDA(cudaHostAlloc((void **)&S.host, (size_t)kSlots * 8, cudaHostAllocMapped));
+  memset(S.host, 0, (size_t)kSlots * 8);
 }
 
 template <class T>
@@ -58,9 +63,9 @@ void deliver(const std::vector<GblRequest> &reqs) {
     lo = std::min(lo, r.slot);
     hi = std::max(hi, r.slot);
   }
-  OP2B_CUDA(cudaMemcpyAsync(S.host + (size_t)lo * 8, S.dev + off_slots() + (size_t)lo * 8,
-                            (size_t)(hi - lo + 1) * 8, cudaMemcpyDeviceToHost, rt().stream));
-  OP2B_CUDA(cudaStreamSynchronize(rt().stream));
+  (void)lo;
+  (void)hi;
+  OP2B_CUDA(cudaStreamSynchronize(rt().stream));  // the slots are host memory
   for (auto &r : reqs) {
     const char *p = S.host + (size_t)r.slot * 8;
     if (r.type == GBL_F64) combine<double>(r.host, *(const double *)p, r.acc, r.assign);
@@ -86,7 +91,7 @@ unsigned *red_ticket() {
 
 void *red_slot_ptr(int slot) {
   ensure_red();
-  return rs().dev + off_slots() + (size_t)slot * 8;
+  return rs().host + (size_t)slot * 8;  // a mapped host address (unified addressing)
 }
 
 int red_new_slot() {
