@@ -48,6 +48,16 @@ void op2b_mesh_free(op2b_mesh *m);
 int  op2b_mesh_write(const op2b_mesh *m, const char *path);
 int  op2b_mesh_read(const char *path, op2b_mesh *out);
 
+/* Binary mesh files: the arrays of an op2b_mesh with a header and a hash of
+ * the payload (reading a damaged file fails).  op2b_mesh_read_cached reads
+ * text_path through a binary cache: when cache_path holds a valid cache of
+ * the same text file (same size and modification time) it is read instead
+ * of parsing the text; otherwise the text is parsed and the cache written.
+ * Returns 0 on success. */
+int  op2b_mesh_write_bin(const op2b_mesh *m, const char *path);
+int  op2b_mesh_read_bin(const char *path, op2b_mesh *out);
+int  op2b_mesh_read_cached(const char *text_path, const char *cache_path, op2b_mesh *out);
+
 /* The jac1 / jac2 test problem (jac1/jac.cpp:65-117): an (NN-1)^2 interior
  * grid stored unstructured, one self edge (A = -1) per node and one edge per
  * interior 4-neighbour (A = 0.25), boundary neighbours adding 0.25 to r.

@@ -144,6 +144,9 @@ PROTOTYPES = [
     ("op2b_mesh_free", None, [C.POINTER(op2b_mesh)]),
     ("op2b_mesh_write", C.c_int, [C.POINTER(op2b_mesh), C.c_char_p]),
     ("op2b_mesh_read", C.c_int, [C.c_char_p, C.POINTER(op2b_mesh)]),
+    ("op2b_mesh_write_bin", C.c_int, [C.POINTER(op2b_mesh), C.c_char_p]),
+    ("op2b_mesh_read_bin", C.c_int, [C.c_char_p, C.POINTER(op2b_mesh)]),
+    ("op2b_mesh_read_cached", C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(op2b_mesh)]),
     ("op2b_jac_sizes", C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("op2b_mesh_jac1", C.c_int, [C.c_int, _P, _P, _P]),
     ("op2b_mesh_jac2", C.c_int, [C.c_int, _P, _P, _P]),

@@ -11,6 +11,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <string>
+#include <sys/stat.h>
 #include <vector>
 
 namespace {
@@ -302,7 +304,94 @@ extern "C" int op2b_mesh_write(const op2b_mesh *m, const char *path) {
   return fclose(fp) == 0 ? 0 : 2;
 }
 
+// Text input, fast path: the whole file in memory, integers parsed by hand,
+// coordinates by strtod / strtof on the same tokens (so values equal the
+// reference reader's, airfoil/airfoil.cpp:80-129).  Returns -1 when the text
+// does not have the expected shape, so the caller can fall back to fscanf.
+namespace {
+
+bool slurp(const char *path, std::vector<char> &buf) {
+  FILE *fp = fopen(path, "rb");
+  if (!fp) return false;
+  fseek(fp, 0, SEEK_END);
+  long n = ftell(fp);
+  fseek(fp, 0, SEEK_SET);
+  if (n < 0) { fclose(fp); return false; }
+  buf.resize((size_t)n + 1);
+  size_t got = fread(buf.data(), 1, (size_t)n, fp);
+  fclose(fp);
+  buf[got] = 0;
+  buf.resize(got + 1);
+  return true;
+}
+
+struct Cursor {
+  const char *p, *end;
+  void skip() { while (p < end && (*p == ' ' || *p == '\n' || *p == '\r' || *p == '\t')) p++; }
+  bool integer(int &v) {
+    skip();
+    bool neg = false;
+    if (p < end && (*p == '-' || *p == '+')) neg = *p++ == '-';
+    if (p >= end || *p < '0' || *p > '9') return false;
+    long long x = 0;
+    while (p < end && *p >= '0' && *p <= '9') {
+      x = x * 10 + (*p++ - '0');
+      if (x > 2147483648LL) return false;
+    }
+    if (p < end && *p != ' ' && *p != '\n' && *p != '\r' && *p != '\t') return false;
+    v = (int)(neg ? -x : x);
+    return true;
+  }
+  bool real(double &d, float &f) {
+    skip();
+    const char *t = p;
+    while (p < end && *p != ' ' && *p != '\n' && *p != '\r' && *p != '\t') p++;
+    if (p == t || p - t > 127) return false;
+    char tok[128];
+    memcpy(tok, t, p - t);
+    tok[p - t] = 0;
+    char *e1, *e2;
+    d = strtod(tok, &e1);
+    f = strtof(tok, &e2);
+    return *e1 == 0 && *e2 == 0;
+  }
+};
+
+int parse_text(const char *path, op2b_mesh *m) {
+  std::vector<char> buf;
+  if (!slurp(path, buf)) return 1;
+  Cursor c{buf.data(), buf.data() + buf.size() - 1};
+  if (!c.integer(m->nnode) || !c.integer(m->ncell) || !c.integer(m->nedge) ||
+      !c.integer(m->nbedge) || m->nnode <= 0 || m->ncell <= 0 || m->nedge <= 0 ||
+      m->nbedge <= 0)
+    return -1;
+  if (!alloc_mesh(m)) return 3;
+  for (int n = 0; n < m->nnode; n++)
+    for (int k = 0; k < 2; k++)
+      if (!c.real(m->x64[2 * (size_t)n + k], m->x32[2 * (size_t)n + k])) return -1;
+  for (size_t i = 0; i < 4 * (size_t)m->ncell; i++)
+    if (!c.integer(m->cell[i])) return -1;
+  for (int n = 0; n < m->nedge; n++)
+    if (!c.integer(m->edge[2 * (size_t)n]) || !c.integer(m->edge[2 * (size_t)n + 1]) ||
+        !c.integer(m->ecell[2 * (size_t)n]) || !c.integer(m->ecell[2 * (size_t)n + 1]))
+      return -1;
+  for (int n = 0; n < m->nbedge; n++)
+    if (!c.integer(m->bedge[2 * (size_t)n]) || !c.integer(m->bedge[2 * (size_t)n + 1]) ||
+        !c.integer(m->becell[n]) || !c.integer(m->bound[n]))
+      return -1;
+  return 0;
+}
+
+}  // namespace
+
 extern "C" int op2b_mesh_read(const char *path, op2b_mesh *m) {
+  memset(m, 0, sizeof(*m));
+  const int fast = parse_text(path, m);
+  if (fast >= 0) {
+    if (fast) op2b_mesh_free(m);
+    return fast;
+  }
+  op2b_mesh_free(m);  // unexpected layout: the reference's own scanf reading
   memset(m, 0, sizeof(*m));
   FILE *fp = fopen(path, "r");
   if (!fp) return 1;
@@ -332,6 +421,132 @@ extern "C" int op2b_mesh_read(const char *path, op2b_mesh *m) {
                &m->becell[n], &m->bound[n]) != 4) rc = 2;
   fclose(fp);
   if (rc) op2b_mesh_free(m);
+  return rc;
+}
+
+// ------------------------------------------------------ binary mesh cache --
+// "OP2BMSH1" header, the four sizes, the size and modification time of the
+// text file it was made from, an FNV-1a hash of the payload, then the arrays
+// (cell, edge, ecell, bedge, becell, bound, x64, x32) in host byte order.
+
+namespace {
+
+struct BinHeader {
+  char magic[8];
+  int32_t version, nnode, ncell, nedge, nbedge, pad;
+  int64_t src_size, src_mtime_ns;
+  uint64_t hash;
+};
+
+struct Part {
+  void *p;
+  size_t bytes;
+};
+
+std::vector<Part> parts(const op2b_mesh *m) {
+  return {{m->cell, sizeof(int) * 4 * (size_t)m->ncell},
+          {m->edge, sizeof(int) * 2 * (size_t)m->nedge},
+          {m->ecell, sizeof(int) * 2 * (size_t)m->nedge},
+          {m->bedge, sizeof(int) * 2 * (size_t)m->nbedge},
+          {m->becell, sizeof(int) * (size_t)m->nbedge},
+          {m->bound, sizeof(int) * (size_t)m->nbedge},
+          {m->x64, sizeof(double) * 2 * (size_t)m->nnode},
+          {m->x32, sizeof(float) * 2 * (size_t)m->nnode}};
+}
+
+// FNV-1a over 8-byte words (then the tail bytes)
+uint64_t fnv1a(const std::vector<Part> &ps) {
+  uint64_t h = 0xcbf29ce484222325ull;
+  for (const Part &q : ps) {
+    const unsigned char *b = (const unsigned char *)q.p;
+    size_t i = 0;
+    for (; i + 8 <= q.bytes; i += 8) {
+      uint64_t w;
+      memcpy(&w, b + i, 8);
+      h = (h ^ w) * 0x100000001b3ull;
+    }
+    for (; i < q.bytes; i++) h = (h ^ b[i]) * 0x100000001b3ull;
+  }
+  return h;
+}
+
+bool file_stamp(const char *path, int64_t &size, int64_t &mtime_ns) {
+  struct stat st;
+  if (!path || stat(path, &st) != 0) return false;
+  size = (int64_t)st.st_size;
+  mtime_ns = (int64_t)st.st_mtim.tv_sec * 1000000000LL + st.st_mtim.tv_nsec;
+  return true;
+}
+
+int write_bin(const op2b_mesh *m, const char *path, int64_t src_size, int64_t src_mtime) {
+  BinHeader h;
+  memset(&h, 0, sizeof h);
+  memcpy(h.magic, "OP2BMSH1", 8);
+  h.version = 1;
+  h.nnode = m->nnode; h.ncell = m->ncell; h.nedge = m->nedge; h.nbedge = m->nbedge;
+  h.src_size = src_size;
+  h.src_mtime_ns = src_mtime;
+  std::vector<Part> ps = parts(m);
+  h.hash = fnv1a(ps);
+  std::string tmp = std::string(path) + ".tmp";
+  FILE *fp = fopen(tmp.c_str(), "wb");
+  if (!fp) return 1;
+  bool ok = fwrite(&h, sizeof h, 1, fp) == 1;
+  for (const Part &q : ps) ok = ok && fwrite(q.p, 1, q.bytes, fp) == q.bytes;
+  ok = (fclose(fp) == 0) && ok;
+  if (!ok || rename(tmp.c_str(), path) != 0) {
+    remove(tmp.c_str());
+    return 2;
+  }
+  return 0;
+}
+
+// 0 ok; 1 missing; 2 bad or stale (want_size >= 0: must match the stamp)
+int read_bin(const char *path, op2b_mesh *m, int64_t want_size, int64_t want_mtime) {
+  memset(m, 0, sizeof(*m));
+  FILE *fp = fopen(path, "rb");
+  if (!fp) return 1;
+  BinHeader h;
+  if (fread(&h, sizeof h, 1, fp) != 1 || memcmp(h.magic, "OP2BMSH1", 8) != 0 || h.version != 1 ||
+      h.nnode <= 0 || h.ncell <= 0 || h.nedge <= 0 || h.nbedge <= 0 ||
+      (want_size >= 0 && (h.src_size != want_size || h.src_mtime_ns != want_mtime))) {
+    fclose(fp);
+    return 2;
+  }
+  m->nnode = h.nnode; m->ncell = h.ncell; m->nedge = h.nedge; m->nbedge = h.nbedge;
+  if (!alloc_mesh(m)) {
+    fclose(fp);
+    op2b_mesh_free(m);
+    return 3;
+  }
+  std::vector<Part> ps = parts(m);
+  bool ok = true;
+  for (const Part &q : ps) ok = ok && fread(q.p, 1, q.bytes, fp) == q.bytes;
+  fclose(fp);
+  if (!ok || fnv1a(ps) != h.hash) {
+    op2b_mesh_free(m);
+    return 2;
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int op2b_mesh_write_bin(const op2b_mesh *m, const char *path) {
+  return write_bin(m, path, -1, -1);
+}
+
+extern "C" int op2b_mesh_read_bin(const char *path, op2b_mesh *out) {
+  return read_bin(path, out, -1, -1);
+}
+
+extern "C" int op2b_mesh_read_cached(const char *text_path, const char *cache_path,
+                                     op2b_mesh *out) {
+  int64_t size = 0, mtime = 0;
+  if (!file_stamp(text_path, size, mtime)) return 1;
+  if (cache_path && read_bin(cache_path, out, size, mtime) == 0) return 0;
+  int rc = op2b_mesh_read(text_path, out);
+  if (rc == 0 && cache_path) write_bin(out, cache_path, size, mtime);  // best effort
   return rc;
 }
 

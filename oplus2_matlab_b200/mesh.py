@@ -137,3 +137,20 @@ def jac(NN, variant=1):
     if rc != nedge:
         raise RuntimeError("jac mesh generation failed")
     return JacMesh(NN=NN, nnode=nnode, nedge=nedge, pp=pp, A=A, r=r)
+
+
+def read_grid(path, cache=None):
+    """Read new_grid.dat (airfoil/airfoil.cpp:80-129); with `cache`, through a
+    binary cache of the same file (op2b_mesh_read_cached)."""
+    lib = _lib.load()
+    m = _lib.op2b_mesh()
+    if cache:
+        rc = lib.op2b_mesh_read_cached(str(path).encode(), str(cache).encode(), C.byref(m))
+    else:
+        rc = lib.op2b_mesh_read(str(path).encode(), C.byref(m))
+    if rc != 0:
+        raise IOError("cannot read %s (rc %d)" % (path, rc))
+    try:
+        return AirfoilMesh(I=0, J=0, **_take(m))
+    finally:
+        lib.op2b_mesh_free(C.byref(m))

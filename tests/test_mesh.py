@@ -66,3 +66,70 @@ def test_jac_grid():
     assert abs(float(j.r.sum()) - 0.25 * 4 * 5) < 1e-6
     j2 = M.jac(6, 2)
     assert j2.A.shape == (105, 3) and np.array_equal(j2.A[:, 0].astype(np.float32), j.A)
+
+
+# ---------------------------------------------------------- mesh files ----
+
+def _read(fn, *paths):
+    import ctypes as C
+    from oplus2_matlab_b200 import _lib
+    L = _lib.load()
+    s = _lib.op2b_mesh()
+    rc = getattr(L, fn)(*[p.encode() for p in paths], C.byref(s))
+    if rc != 0:
+        return rc, None
+    try:
+        return 0, M._take(s)
+    finally:
+        L.op2b_mesh_free(C.byref(s))
+
+
+def _same(a, b):
+    for k in ("cell", "edge", "ecell", "bedge", "becell", "bound", "x64", "x32"):
+        assert np.array_equal(a[k], getattr(b, k) if not isinstance(b, dict) else b[k]), k
+
+
+def test_text_binary_and_cached_reads_agree(tmp_path):
+    import ctypes as C
+    import os
+    from oplus2_matlab_b200 import _lib
+    m = M.naca0012(40, 60)
+    txt, binp, cache = str(tmp_path / "g.dat"), str(tmp_path / "g.bin"), str(tmp_path / "g.cache")
+    M.write_grid(m, txt)
+    rc, t = _read("op2b_mesh_read", txt)
+    assert rc == 0
+    _same(t, m)  # the fast text reader gives the generator's values bit for bit
+    s, keep = M.as_struct(m)
+    assert _lib.load().op2b_mesh_write_bin(C.byref(s), binp.encode()) == 0
+    rc, b = _read("op2b_mesh_read_bin", binp)
+    assert rc == 0
+    _same(b, m)
+    rc, c1 = _read("op2b_mesh_read_cached", txt, cache)  # parses, writes the cache
+    assert rc == 0 and os.path.exists(cache)
+    _same(c1, m)
+    stamp = os.stat(cache).st_mtime_ns
+    rc, c2 = _read("op2b_mesh_read_cached", txt, cache)  # reads the cache
+    assert rc == 0 and os.stat(cache).st_mtime_ns == stamp
+    _same(c2, m)
+
+
+def test_damaged_or_stale_cache_is_not_used(tmp_path):
+    import os
+    m = M.naca0012(20, 30)
+    txt, cache = str(tmp_path / "g.dat"), str(tmp_path / "g.cache")
+    M.write_grid(m, txt)
+    assert _read("op2b_mesh_read_cached", txt, cache)[0] == 0
+    with open(cache, "r+b") as f:  # flip one payload byte
+        f.seek(os.path.getsize(cache) - 5)
+        b = f.read(1)
+        f.seek(-1, 1)
+        f.write(bytes([b[0] ^ 0xFF]))
+    assert _read("op2b_mesh_read_bin", cache)[0] == 2
+    rc, c = _read("op2b_mesh_read_cached", txt, cache)  # falls back to the text, rewrites
+    assert rc == 0
+    _same(c, m)
+    assert _read("op2b_mesh_read_bin", cache)[0] == 0
+    m2 = M.naca0012(21, 30)  # a new text file: the old cache is stale
+    M.write_grid(m2, txt)
+    rc, c = _read("op2b_mesh_read_cached", txt, cache)
+    assert rc == 0 and c["ncell"] == m2.ncell
