@@ -62,6 +62,21 @@ int op2b_set_renumber(int on);
  * 0 if it keeps its numbering (new2old = identity), -1 on bad arguments. */
 int op2b_renumber_order(op_set set, int *new2old);
 
+/* Checkpointing (doc/dev.tex:1080-1087 proposes it; the reference has no
+ * implementation).  op2b_checkpoint_file(path) names the checkpoint file;
+ * call it after op_init, before the first loop.  If the file holds a
+ * checkpoint, the run fast-forwards: loop calls do not run but return the
+ * global reduction values recorded in the file, until the op_checkpoint call
+ * at which it was saved, which restores every dataset (matched by name) and
+ * resumes.  Returns 1 when resuming, 0 when starting fresh, -1 on error.
+ * op_checkpoint() saves every dataset and every reduction value returned so
+ * far (atomically: written to path.tmp, then renamed); returns 1 when saved,
+ * 2 where a fast-forwarded run resumed, 0 for an earlier checkpoint passed
+ * while fast-forwarding, -1 on error.  Needs reductions returned at each loop
+ * call (not op2b_set_gbl_deferred). */
+int op2b_checkpoint_file(const char *path);
+int op_checkpoint(void);
+
 /* op_decl_const of include/op_seq.h (the sequential API's unnamed form,
  * op_lib.h:177-182): declares the constant under the name written in `expr`,
  * the app's argument expression ("&gam" -> "gam", "qinf" -> "qinf"). */

@@ -129,6 +129,8 @@ PROTOTYPES = [
     ("op2b_set_tuning", C.c_int, [C.c_char_p, C.c_int]),
     ("op2b_update_noalloc", C.c_int, [C.c_int, _P, _P, _P, _P, _P, _P]),
     ("op2b_set_renumber", C.c_int, [C.c_int]),
+    ("op2b_checkpoint_file", C.c_int, [C.c_char_p]),
+    ("op_checkpoint", C.c_int, []),
     ("op2b_renumber_order", C.c_int, [op_set, C.POINTER(C.c_int)]),
     ("op2b_decl_const_named", None, [C.c_int, C.c_char_p, C.c_int, _P, C.c_char_p]),
     ("op2b_capture_begin", C.c_int, [C.c_int]),

@@ -158,6 +158,13 @@ void permute_dat_in_place(op_dat d);   // a dataset declared after renumbering
 bool fetch_unpermuted(op_dat d, void *host);  // false: not renumbered, nothing done
 std::vector<int> renumbered_map(op_map m);    // empty: map unchanged
 
+// op_checkpoint (checkpoint.cpp): fast-forward of a restarted run, and the
+// log of reduction values returned to the app
+bool checkpoint_fast_forward();
+bool checkpoint_before_loop(char const *name, int nargs, const op_arg *args);  // true: skip
+void checkpoint_after_loop(int nargs, const op_arg *args);
+void checkpoint_reset();  // op_exit
+
 // global reductions: device slot management (reduce.cu)
 void deliver_deferred();
 

@@ -309,9 +309,19 @@ void flush_pending() {
 }
 }  // namespace op2b
 
-extern "C" {
+namespace {
+void par_loop_run(char const *name, op_set set, int nargs, const op_arg *args);
+}
 
-void op2b_par_loop(char const *name, op_set set, int nargs, const op_arg *args) {
+extern "C" void op2b_par_loop(char const *name, op_set set, int nargs, const op_arg *args) {
+  // a restarted run before its checkpoint: hand back the saved values
+  if (checkpoint_fast_forward() && checkpoint_before_loop(name, nargs, args)) return;
+  par_loop_run(name, set, nargs, args);
+  if (!error_pending()) checkpoint_after_loop(nargs, args);
+}
+
+namespace {
+void par_loop_run(char const *name, op_set set, int nargs, const op_arg *args) {
   if (set == nullptr) {
     fail(1, "error: invalid set in kernel \"%s\"\n", name ? name : "(null)");
     return;
@@ -359,6 +369,9 @@ void op2b_par_loop(char const *name, op_set set, int nargs, const op_arg *args) 
   }
   run_kind(k, v, name, set, args);
 }
+}  // namespace
+
+extern "C" {
 
 // the per-loop entry points of the generated app mains
 // (airfoil/airfoil_op.cpp:64-99, jac1/jac_op.cpp:58-73)
