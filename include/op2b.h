@@ -111,8 +111,12 @@ int   op2b_set_gbl_deferred(int on);
 /* Per-loop device time in seconds and call count, by loop name (CUDA events
  * around each loop; summed lazily).  Returns -1 if the name is unknown. */
 double op2b_loop_time(char const *name, int *count);
-/* Turn per-loop event timing on (default) or off; returns the old value. */
-int    op2b_set_timing(int on);
+/* Per-loop device timing for op_timing_output / op2b_loop_time: 0 off,
+ * 1 sampled (default: a loop's first call and every 16th call are timed with
+ * events, the total is estimated from them; each event pair costs host time
+ * on every timed call), 2 every call.  Call counts are always exact.
+ * Returns the old mode. */
+int    op2b_set_timing(int mode);
 
 /* CUDA graphs.  op2b_capture_begin() starts capturing the library stream;
  * the op_par_loop calls that follow are recorded, not run, with their global

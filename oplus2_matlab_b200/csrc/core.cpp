@@ -97,9 +97,9 @@ int op2b_set_tuning(const char *key, int value) {
   return old;
 }
 
-int op2b_set_timing(int on) {
+int op2b_set_timing(int mode) {
   int old = rt().timing;
-  rt().timing = on != 0;
+  rt().timing = mode < 0 ? 0 : (mode > 2 ? 2 : mode);
   return old;
 }
 

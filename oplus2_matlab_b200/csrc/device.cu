@@ -132,6 +132,8 @@ LoopScope::LoopScope(char const *name, double transfer, double transfer2) {
     return;
   }
   if (!R.timing) return;
+  first = T.count == 1;
+  if (R.timing == 1 && !first && (T.count - 1) % kTimingSample != 0) return;
   if (T.pending.size() > 512) flush_timers();
   if (T.free_pairs.empty()) {
     cudaEvent_t a, b;
@@ -149,7 +151,7 @@ LoopScope::~LoopScope() {
   if (captured) cudaEventRecordWithFlags(ev.second, rt().stream, cudaEventRecordExternal);
   else cudaEventRecord(ev.second, rt().stream);
   if (captured) rt().capture_events.push_back({t->name, ev.first, ev.second});
-  else t->pending.push_back(ev);
+  else t->pending.push_back(LoopTimer::Timed{ev, first});
 }
 
 PhaseScope::PhaseScope(const std::string &name) : name_(name) {
@@ -170,17 +172,26 @@ void flush_timers() {
   Runtime &R = rt();
   for (auto &kv : R.timers) {
     LoopTimer &T = kv.second;
+    if (T.pending.empty()) continue;
     for (auto &p : T.pending) {
       float ms = 0.f;
-      if (cudaEventSynchronize(p.second) == cudaSuccess &&
-          cudaEventElapsedTime(&ms, p.first, p.second) == cudaSuccess) {
-        T.seconds += ms * 1e-3;
-        if (T.kernel_index >= 0 && T.kernel_index < OP_kern_max)
-          OP_kernels[T.kernel_index].time += ms * 1e-3f;
+      if (cudaEventSynchronize(p.ev.second) == cudaSuccess &&
+          cudaEventElapsedTime(&ms, p.ev.first, p.ev.second) == cudaSuccess) {
+        if (p.first) {
+          T.first_s = ms * 1e-3;
+        } else {
+          T.sampled_s += ms * 1e-3;
+          T.sampled_n++;
+        }
       }
-      T.free_pairs.push_back(p);
+      T.free_pairs.push_back(p.ev);
     }
     T.pending.clear();
+    // every call after the first at the sampled mean
+    const double rest = T.sampled_n ? T.sampled_s / T.sampled_n * (T.count - 1) : 0.0;
+    T.seconds = T.first_s + rest;
+    if (T.kernel_index >= 0 && T.kernel_index < OP_kern_max)
+      OP_kernels[T.kernel_index].time = (float)T.seconds;
   }
 }
 

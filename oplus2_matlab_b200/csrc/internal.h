@@ -38,12 +38,23 @@ struct DatDev {
 };
 
 // per-loop timing record (op_kernel of the reference plus device events)
+// per-loop timing record (op_kernel of the reference plus device events).
+// Sampled timing (the default) times a loop's first call and every
+// kTimingSample-th call after it; the total is the first call's time plus
+// the sampled mean times the other calls.
+constexpr int kTimingSample = 16;
 struct LoopTimer {
   std::string name;
   int kernel_index = -1;  // slot in OP_kernels
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+  struct Timed {
+    std::pair<cudaEvent_t, cudaEvent_t> ev;
+    bool first;
+  };
+  std::vector<Timed> pending;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> free_pairs;
-  double seconds = 0.0;
+  double seconds = 0.0;   // estimated total device time
+  double first_s = 0.0, sampled_s = 0.0;
+  long long sampled_n = 0;
   int count = 0;
 };
 
@@ -56,7 +67,7 @@ struct Runtime {
   int reduction = OP2B_REDUCE_TREE;
   int error_mode = OP2B_ERRORS_EXIT;
   bool gbl_deferred = false;
-  bool timing = true;
+  int timing = 1;  // 0 off, 1 sampled (every kTimingSample-th call), 2 every call
   int num_sms = 148;
 
   std::vector<MapDev> maps;  // by op_map index
@@ -126,7 +137,7 @@ void ensure_cuda();  // op_init's device part, also run lazily
 struct LoopScope {
   LoopTimer *t = nullptr;
   std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
-  bool captured = false;
+  bool captured = false, first = false;
   LoopScope(char const *name, double transfer, double transfer2);
   ~LoopScope();
 };
