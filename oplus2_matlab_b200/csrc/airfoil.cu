@@ -810,7 +810,23 @@ __global__ void k_update(int n, const T *__restrict__ qold, T *__restrict__ q,
 // ------------------------------------------------------------ host side ---
 
 template <class T>
+static AirConsts<T> air_consts_lookup();
+
+// the constants by name, looked up again only when a constant was declared
+template <class T>
 static AirConsts<T> air_consts() {
+  static AirConsts<T> cached;
+  static unsigned version = ~0u;
+  if (version != rt().consts_version) {
+    cached = air_consts_lookup<T>();
+    if (error_pending()) return cached;
+    version = rt().consts_version;
+  }
+  return cached;
+}
+
+template <class T>
+static AirConsts<T> air_consts_lookup() {
   AirConsts<T> K;
   memset(&K, 0, sizeof K);
   T v[4];

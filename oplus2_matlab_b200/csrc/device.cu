@@ -334,6 +334,7 @@ void op_exit(void) {
   }
   R.timers.clear();
   R.consts.clear();
+  R.consts_version++;  // constants cached by the loops are stale now
   op_exit_core();
 }
 

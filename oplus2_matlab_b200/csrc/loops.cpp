@@ -24,15 +24,19 @@ int effective_strategy(char const *loop_name) {
 }
 
 double compulsory_bytes(op_set set, int nargs, const op_arg *args) {
-  std::set<const void *> maps_seen;
-  std::set<const void *> dats_seen;
+  // every distinct map and dataset once (no allocation: this runs per call)
   double bytes = 0;
   for (int m = 0; m < nargs; m++) {
     const op_arg &a = args[m];
     if (a.argtype != OP_ARG_DAT || !a.dat) continue;
-    if (a.map && maps_seen.insert(a.map).second)
-      bytes += 4.0 * a.map->dim * (double)set->size;
-    if (dats_seen.insert(a.dat).second) {
+    bool map_new = a.map != nullptr, dat_new = true;
+    for (int j = 0; j < m; j++) {
+      if (args[j].argtype != OP_ARG_DAT) continue;
+      if (a.map && args[j].map == a.map) map_new = false;
+      if (args[j].dat == a.dat) dat_new = false;
+    }
+    if (map_new) bytes += 4.0 * a.map->dim * (double)set->size;
+    if (dat_new) {
       double fac = (a.acc == OP_READ || a.acc == OP_WRITE) ? 1.0 : 2.0;
       bytes += fac * a.dat->size * (double)a.dat->set->size;
     }
