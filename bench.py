@@ -69,7 +69,8 @@ def parse():
                          "renumbers cells, nodes, edges and bedges from the seed (scrambled)")
     ap.add_argument("--renumber", action="store_true",
                     help="plain mode: renumber the sets for locality (op2b_set_renumber)")
-    ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"],
+    ap.add_argument("--nn", type=int, default=512, help="jac mode: NN (grid of (NN-1)^2 nodes)")
+    ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served", "jac"],
                     help="plain: the 720k single-mesh iteration (default); batched: many "
                          "instances per launch; served: a Poisson request stream")
     ap.add_argument("--instances", type=int, default=64, help="batched: instances")
@@ -727,6 +728,124 @@ def impl_served(args, dist):
         print(json.dumps(line))
 
 
+def run_reference_jac(NN, niter, threads=None):
+    """The reference's OpenMP jac1 (oracle/_ref/jac1_op) at NN, niter; returns
+    (iterations/s from its own op_timing_output, seconds, cores) or None."""
+    binary = os.path.join(ROOT, "oracle", "_ref", "jac1_op")
+    if not os.path.exists(binary):
+        return None
+    cores = threads or os.cpu_count()
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_PROC_BIND="close",
+               OP2REF_NN=str(NN), OP2REF_NITER=str(niter))
+    r = subprocess.run([binary], env=env, capture_output=True, text=True, timeout=1800)
+    if r.returncode != 0:
+        return None
+    tot = 0.0
+    for line in r.stdout.splitlines():
+        f = line.split()
+        if len(f) >= 4 and f[0].isdigit() and f[-1] in ("res", "update"):
+            tot += float(f[1])
+    return (niter / tot if tot > 0 else None), tot, cores
+
+
+def impl_jac(args, dist):
+    """jac1 (config 0 of the reference's apps): an (NN-1)^2-node Jacobi grid
+    stored unstructured, 100 iterations of res (indirect OP_INC) + update
+    (direct, sum and max reductions).  value: one iteration per CUDA-graph
+    launch, reductions deferred, L2 flushed before each; e2e: the same
+    iterations through the C API with both reductions returned to the host
+    every iteration; cpu_baseline: the reference's OpenMP jac1_op."""
+    from oplus2_matlab_b200 import api, apps
+    from oplus2_matlab_b200 import mesh as M
+    lib = api.lib()
+    cr = cudart()
+    NN, niter = args.nn, max(args.steps, 1)
+    jm = M.jac(NN, 1)
+    api.set_error_mode(api.ERRORS_RETURN)
+    api.op_init([], 0)
+    api.set_strategy(api.STRATEGY_GATHER)
+    api.set_reduction(api.REDUCE_TREE)
+    J = apps.Jac(jm, 1)
+    J.iterate(max(3, args.warmup))
+    api.sync()
+    # e2e first: every iteration returns u_sum and u_max to the host
+    t0 = time.perf_counter()
+    J.iterate(niter)
+    e2e_s = time.perf_counter() - t0
+    # device: one iteration per graph launch, reductions deferred
+    api.set_gbl_deferred(1)
+    assert lib.op2b_capture_begin(0) == 1, api.last_error()
+    J.iteration()
+    g = lib.op2b_capture_end()
+    assert g, api.last_error()
+    nk = lib.op2b_graph_nkernels(g)
+    stream = lib.op2b_get_stream()
+    assert lib.op2b_l2_flush() == 0
+    ev = []
+    for _ in range(2 * niter):
+        e = C.c_void_p()
+        cr.cudaEventCreate(C.byref(e))
+        ev.append(e)
+    for _ in range(3):
+        lib.op2b_graph_launch(g)
+    clocks = Clocks(dist.local)
+    dist.barrier()
+    cr.cudaStreamSynchronize(stream)
+    for k in range(niter):
+        lib.op2b_l2_flush()
+        cr.cudaEventRecord(ev[2 * k], stream)
+        lib.op2b_graph_launch(g)
+        cr.cudaEventRecord(ev[2 * k + 1], stream)
+    cr.cudaStreamSynchronize(stream)
+    clk = clocks.stop()
+    ms = []
+    for k in range(niter):
+        m = C.c_float()
+        cr.cudaEventElapsedTime(C.byref(m), ev[2 * k], ev[2 * k + 1])
+        ms.append(m.value)
+    total = dist.max(sum(ms) * 1e-3)
+    lib.op2b_graph_destroy(g)
+    api.sync()
+    api.set_gbl_deferred(0)
+    u = J.fetch().copy()
+    ok = bool(np.isfinite(u).all())
+    api.op_exit()
+    value = dist.world * niter / total
+    # compulsory bytes per iteration: res = 12 per edge + 12 per node (A, the
+    # map pair, u read, du read+write), update = 20 per node (r, du rw, u rw)
+    it_bytes = 12.0 * jm.nedge + 12.0 * jm.nnode + 20.0 * jm.nnode
+    peak, peak_kind = measured_peak()
+    cpu = None
+    if not args.no_cpu_baseline and dist.rank == 0 and dist.world == 1:
+        r = run_reference_jac(NN, min(niter, 100))
+        if r and r[0]:
+            cpu = {"value": r[0], "unit": "iters/s", "cores": r[2], "kind": "reference",
+                   "sample": "%d iterations at NN=%d (reference jac1_op, OpenMP, sum of its "
+                             "op_timing_output)" % (min(niter, 100), NN)}
+    line = {
+        "metric": "jac1 iters/s", "value": value, "unit": "iters/s", "n_gpus": dist.world,
+        "steps": niter, "warmup": max(3, args.warmup), "ms_per_step": 1e3 * total / niter,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: the reference's jac1 grid generator (jac1/jac.cpp:65-117)",
+        "config": {"workload": "jac1 NN=%d: %d nodes, %d edges, one iteration (res + update) "
+                               "per step" % (NN, jm.nnode, jm.nedge),
+                   "l2": "flushed before every step", "parallelism": "single GPU"},
+        "roofline": {"bound": "hbm", "kernel": "res + update (one iteration)",
+                     "achieved": it_bytes * value / dist.world / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": it_bytes * value / dist.world / 1e9 / peak,
+                     "traffic": None, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": it_bytes},
+        "e2e": {"value": niter / e2e_s, "unit": "iters/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 8,
+                "path": "Python Jac app over the C API, u_sum and u_max to the host every "
+                        "iteration"},
+        "gpu_launches": nk * niter, "kernels_per_step": nk,
+        "finite": ok, "cpu_baseline": cpu, "clocks": clk,
+    }
+    if dist.rank == 0:
+        print(json.dumps(line))
+
+
 def main():
     args = parse()
     dist = Dist()
@@ -737,6 +856,8 @@ def main():
             impl_batched(args, dist)
         elif args.mode == "served":
             impl_served(args, dist)
+        elif args.mode == "jac":
+            impl_jac(args, dist)
         else:
             impl_ours(args, dist)
     finally:
