@@ -76,36 +76,32 @@ __device__ __forceinline__ AirConsts<T> with_qinf(AirConsts<T> K, const SolveDev
   return K;
 }
 
-// save_soln + adt_calc over one tile of one solve's cells
+// save_soln + adt_calc over one tile of one solve's cells (a thread's cells
+// one after another, the next cell's nodes fetched while this one computes)
 template <class T>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 6 : 4)
     k_grp_save_adt(const Tile *__restrict__ tiles, const SolveDev<T> *__restrict__ sd,
                    const SolveState *st, AirConsts<T> K) {
   const Tile t = tiles[blockIdx.x];
   const SolveDev<T> *d = sd + t.solve;
   const int4 *pcell = reinterpret_cast<const int4 *>(d->pcell);
-  int4 nd[kCellsPerThread];
-#pragma unroll
-  for (int j = 0; j < kCellsPerThread; j++) {  // map entries: read-only
-    const int i = threadIdx.x + j * kThreads;
-    if (i < t.count) nd[j] = __ldg(pcell + t.start + i);
-  }
+  int4 nd = make_int4(0, 0, 0, 0);
+  if ((int)threadIdx.x < t.count) nd = __ldg(pcell + t.start + threadIdx.x);  // read-only
   pdl_wait();
   pdl_trigger();
   if (!solve_active(st, t.solve)) return;
   const T *x = d->x, *q = d->q;
   T *qold = d->qold, *adt = d->adt;
-#pragma unroll
-  for (int j = 0; j < kCellsPerThread; j++) {
-    const int i = threadIdx.x + j * kThreads;
-    if (i >= t.count) continue;
+#pragma unroll 1
+  for (int i = threadIdx.x; i < t.count; i += kThreads) {
     const int c = t.start + i;
     T qq[4], a[2], b[2], e[2], f[2];
     ld4(q + 4 * (size_t)c, qq);
-    ld2(x + 2 * (size_t)nd[j].x, a);
-    ld2(x + 2 * (size_t)nd[j].y, b);
-    ld2(x + 2 * (size_t)nd[j].z, e);
-    ld2(x + 2 * (size_t)nd[j].w, f);
+    ld2(x + 2 * (size_t)nd.x, a);
+    ld2(x + 2 * (size_t)nd.y, b);
+    ld2(x + 2 * (size_t)nd.z, e);
+    ld2(x + 2 * (size_t)nd.w, f);
+    if (i + kThreads < t.count) nd = __ldg(pcell + c + kThreads);
     st4(qold + 4 * (size_t)c, qq);
     adt[c] = adt_calc(a, b, e, f, qq, K);
   }
@@ -114,7 +110,7 @@ __global__ void __launch_bounds__(kThreads)
 // res_calc's flux per edge and bres_calc's increment per boundary edge, over
 // one tile of one solve's values (edges first, then boundary edges)
 template <class T>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 8 : 4)
     k_grp_flux(const Tile *__restrict__ tiles, const SolveDev<T> *__restrict__ sd,
                const SolveState *st, AirConsts<T> K0) {
   const Tile t = tiles[blockIdx.x];
@@ -166,7 +162,7 @@ __global__ void __launch_bounds__(kThreads)
 // update (airfoil/update.h:1-12); FIRST: then adt_calc on the new q, no rms;
 // otherwise: the rms partial, and the solve's last CTA ends the iteration
 template <class T, bool FIRST>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? (FIRST ? 3 : 4) : 2)
     k_grp_fold(const Tile *__restrict__ tiles, const SolveDev<T> *__restrict__ sd,
                SolveState *st, AirConsts<T> K) {
   const Tile t = tiles[blockIdx.x];
@@ -174,14 +170,13 @@ __global__ void __launch_bounds__(kThreads)
   const int W = d->W;
   const int *ell = d->ell;
   const int4 *pcell = reinterpret_cast<const int4 *>(d->pcell);
-  int k[kCellsPerThread][4];
-  int4 nd[kCellsPerThread];
-#pragma unroll
-  for (int j = 0; j < kCellsPerThread; j++) {  // list heads and nodes: read-only
-    const int i = threadIdx.x + j * kThreads;
-    if (i >= t.count) continue;
-    list_head(ell, W, t.start + i, k[j]);
-    if (FIRST) nd[j] = __ldg(pcell + t.start + i);
+  // a thread's cells one after another; the next cell's list head and nodes
+  // (read-only) are fetched while this cell gathers
+  int k[4];
+  int4 nd = make_int4(0, 0, 0, 0);
+  if ((int)threadIdx.x < t.count) {
+    list_head(ell, W, t.start + threadIdx.x, k);
+    if (FIRST) nd = __ldg(pcell + t.start + threadIdx.x);
   }
   pdl_wait();
   pdl_trigger();
@@ -190,10 +185,8 @@ __global__ void __launch_bounds__(kThreads)
   const T *x = d->x, *qold = d->qold, *vals = d->vals;
   T *q = d->q, *res = d->res, *adt = d->adt;
   T rms = T(0);
-#pragma unroll
-  for (int j = 0; j < kCellsPerThread; j++) {
-    const int i = threadIdx.x + j * kThreads;
-    if (i >= t.count) continue;
+#pragma unroll 1
+  for (int i = threadIdx.x; i < t.count; i += kThreads) {
     const int c = t.start + i;
     T r[4], qo[4], f[4][4], xs[4][2];
     ldw4(res + 4 * (size_t)c, r);
@@ -201,15 +194,20 @@ __global__ void __launch_bounds__(kThreads)
     const T ad = adt[c];
 #pragma unroll
     for (int m = 0; m < 4; m++)
-      if (k[j][m] >= 0) ld4(vals + 4 * (size_t)(k[j][m] >> 1), f[m]);
+      if (k[m] >= 0) ld4(vals + 4 * (size_t)(k[m] >> 1), f[m]);
     if (FIRST) {
-      ld2(x + 2 * (size_t)nd[j].x, xs[0]);
-      ld2(x + 2 * (size_t)nd[j].y, xs[1]);
-      ld2(x + 2 * (size_t)nd[j].z, xs[2]);
-      ld2(x + 2 * (size_t)nd[j].w, xs[3]);
+      ld2(x + 2 * (size_t)nd.x, xs[0]);
+      ld2(x + 2 * (size_t)nd.y, xs[1]);
+      ld2(x + 2 * (size_t)nd.z, xs[2]);
+      ld2(x + 2 * (size_t)nd.w, xs[3]);
+    }
+    int kc[4] = {k[0], k[1], k[2], k[3]};
+    if (i + kThreads < t.count) {
+      list_head(ell, W, c + kThreads, k);
+      if (FIRST) nd = __ldg(pcell + c + kThreads);
     }
 #pragma unroll
-    for (int m = 0; m < 4; m++) add_listed(r, k[j][m], f[m]);
+    for (int m = 0; m < 4; m++) add_listed(r, kc[m], f[m]);
     for (int m = 4; m < W; m++) {  // lists longer than 4
       const int kk = __ldg(ell + (size_t)c * W + m);
       T g[4];
