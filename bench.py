@@ -634,6 +634,7 @@ def impl_batched(args, dist):
                    "parallelism": "instances sharded by cells over %d GPU(s)" % dist.world},
         "group": {"seconds": t_group, "iterate_seconds_rank0": t_iter,
                   "edge_tile_autotuned": tile, "device_bytes_rank0": gbytes,
+                  "autotuned": "edge tile and L2 block size",
                   "iteration_gbs_rank0": my_bytes / t_iter / 1e9},
         "plain_back_to_back": {"seconds": t_plain, "solves_per_s": total / t_plain,
                                "path": "op2b_airfoil_app_flow per instance (op_par_loop, "

@@ -6,9 +6,10 @@
  * A group holds any number of independent solves, each a mesh plus a flow
  * condition, with its datasets, maps and contribution lists resident in HBM.
  * Every loop of the outer iteration (save_soln + adt_calc, then twice
- * res_calc + bres_calc + update [+ adt_calc]) runs as ONE launch over all
- * active solves: a tile table lists tiles of one solve's elements, and each
- * CTA works on one tile.  The per-element arithmetic is the plain path's
+ * res_calc + bres_calc + update [+ adt_calc]) runs as one launch over a
+ * whole block of active solves (all of them, or as many as keep the block's
+ * intermediate values in L2): a tile table lists tiles of one solve's
+ * elements, and each CTA works on one tile.  The per-element arithmetic is the plain path's
  * (same device functions, same contribution order), so a solve's flow field
  * q is bit-identical to the plain op_par_loop solve of the same mesh and
  * flow.  Each solve's rms is folded from its own tiles' partials, in tile
@@ -78,12 +79,21 @@ long long op2b_group_solve_bytes(op2b_group g, int nnode, int ncell, int nedge, 
 long long op2b_group_device_bytes(op2b_group g);
 int op2b_group_active(op2b_group g); /* solves in the launches (joined, not stopped) */
 
+/* An iteration runs block by block over the solves (in id order), each
+ * block's five launches together, so that a block's flux values -- written
+ * by one launch, read by the next -- stay in L2: a block holds up to `bytes`
+ * of values (<= 0, the default: all solves in one block).  Results do not
+ * depend on it. */
+int op2b_group_set_block_bytes(op2b_group g, long long bytes);
+
 /* Launch shape of the flux pass: edges per tile (multiple of 256, 256..8192).
  * Results do not depend on it; op2b_group_autotune picks it by timing. */
 int op2b_group_set_edge_tile(op2b_group g, int edges_per_tile);
 int op2b_group_edge_tile(op2b_group g);
-/* Time `iters` iterations at each candidate edge tile on the current active
- * solves, put their state back as it was, keep the fastest; returns it. */
+/* Time `iters` iterations at each candidate edge tile, then at each block
+ * size (24, 48, 96 MiB, one block), on the current active solves, putting
+ * their state back after each trial; keeps the fastest of each and returns
+ * the edge tile. */
 int op2b_group_autotune(op2b_group g, int iters);
 
 #ifdef __cplusplus

@@ -184,5 +184,9 @@ class Group:
     def edge_tile(self, e):
         self._check(self.lib.op2b_group_set_edge_tile(self.h, int(e)), "op2b_group_set_edge_tile")
 
+    def set_block_bytes(self, nbytes):
+        self._check(self.lib.op2b_group_set_block_bytes(self.h, int(nbytes)),
+                    "op2b_group_set_block_bytes")
+
     def autotune(self, iters=5):
         return self._check(self.lib.op2b_group_autotune(self.h, int(iters)), "op2b_group_autotune")
