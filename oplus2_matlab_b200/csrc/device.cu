@@ -18,6 +18,7 @@ void op2b_release_plans();  // plan.cu
 namespace op2b {
 
 void release_fused_plans();  // airfoil.cu
+void release_jac_pairs();    // jac.cu
 
 void ensure_cuda() {
   Runtime &R = rt();
@@ -92,6 +93,7 @@ const int *map_dev(op_map m) {
 void release_plans_and_maps() {
   ::op2b_release_plans();
   release_fused_plans();
+  release_jac_pairs();
   for (auto &m : rt().maps) {
     dev_free(m.d);
     m.d = nullptr;
@@ -320,6 +322,7 @@ void op_exit(void) {
   }
   op2b_release_plans();
   release_fused_plans();
+  release_jac_pairs();
   renumber_reset();
   checkpoint_reset();
   for (auto &m : R.maps) dev_free(m.d);

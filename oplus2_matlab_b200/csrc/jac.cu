@@ -11,6 +11,10 @@
 #include <math.h>
 #include <string.h>
 
+#include <algorithm>
+#include <vector>
+
+#include "launch.cuh"
 #include "loops.h"
 #include "reduce.cuh"
 
@@ -49,18 +53,62 @@ __global__ void k_jac_res_gather(int nrows, const int *__restrict__ active,
                                  const typename JacLayout<V>::AT *__restrict__ A,
                                  const float *__restrict__ u, float *__restrict__ du, float beta) {
   typedef JacLayout<V> L;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int n = 0, k0 = 0, k1 = 0;
+  if (t < nrows) {  // plan arrays: read-only, fetched before the wait
+    n = active ? active[t] : t;
+    k0 = row[t];
+    k1 = row[t + 1];
+  }
+  pdl_wait();
+  pdl_trigger();
   if (t >= nrows) return;
-  int n = active ? active[t] : t;
   float d = du[(size_t)n * L::DU];
-  int k1 = row[t + 1];
-  for (int k = row[t]; k < k1; k++) {
+  for (int k = k0; k < k1; k++) {
     int e = __ldg(keys + k);
     typename L::AT a = __ldg(A + (size_t)jat(mA, e) * L::A);
     float uu = __ldg(u + (size_t)jat(mu, e) * L::U);
     d = jac_inc<V>(d, beta, a, uu);
   }
   du[(size_t)n * L::DU] = d;
+}
+
+// res, GATHER over precomputed (edge, u element) pairs per contribution:
+// row -> pair -> (A, u) instead of row -> key -> map entry -> u
+template <int V>
+__global__ void k_jac_res_pairs(int nrows, const int *__restrict__ active,
+                                const int *__restrict__ row, const int2 *__restrict__ pairs,
+                                const typename JacLayout<V>::AT *__restrict__ A,
+                                const float *__restrict__ u, float *__restrict__ du, float beta) {
+  typedef JacLayout<V> L;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int n = 0, k0 = 0, k1 = 0;
+  if (t < nrows) {  // plan arrays: read-only, fetched before the wait
+    n = active ? active[t] : t;
+    k0 = row[t];
+    k1 = row[t + 1];
+  }
+  pdl_wait();
+  pdl_trigger();
+  if (t >= nrows) return;
+  float d = du[(size_t)n * L::DU];
+  for (int k = k0; k < k1; k++) {
+    const int2 p = __ldg(pairs + k);
+    typename L::AT a = __ldg(A + (size_t)p.x * L::A);
+    float uu = __ldg(u + (size_t)p.y * L::U);
+    d = jac_inc<V>(d, beta, a, uu);
+  }
+  du[(size_t)n * L::DU] = d;
+}
+
+// pairs[k] = (A element, u element) of gather key k (slot 0 of the group)
+__global__ void k_jac_pairs(long long nkeys, const int *__restrict__ keys, IdxMap mA, IdxMap mu,
+                            int2 *pairs) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nkeys;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int e = keys[k];
+    pairs[k] = make_int2(jat(mA, e), jat(mu, e));
+  }
 }
 
 struct JacPlanView {
@@ -116,6 +164,8 @@ __global__ void k_jac_update(int n, const float *__restrict__ r, float *__restri
                              float *__restrict__ u, float alpha, float *seq,
                              RedSlot<float> s_sum, RedSlot<float> s_max, unsigned *ticket) {
   typedef JacLayout<V> L;
+  pdl_wait();
+  pdl_trigger();
   float sum = 0.0f, mx = -INFINITY;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float *up = u + (size_t)i * L::U;
@@ -134,6 +184,36 @@ __global__ void k_jac_update(int n, const float *__restrict__ r, float *__restri
 }
 
 static const int kJacResInds[4] = {-1, 0, 1, -1};
+
+// the pair arrays, by gather plan and the A / u maps they were made for
+struct JacPairs {
+  const GatherPlan *g;
+  op_map mA, mu;
+  int iA, iu;
+  int2 *d;
+};
+static std::vector<JacPairs> g_jac_pairs;
+
+static int2 *jac_pairs(const GatherPlan *g, const op_arg *args, cudaStream_t s) {
+  if (!tuning("jac_pairs", 1)) return nullptr;
+  for (auto &p : g_jac_pairs)
+    if (p.g == g && p.mA == args[0].map && p.mu == args[1].map && p.iA == args[0].idx &&
+        p.iu == args[1].idx)
+      return p.d;
+  JacPairs p{g, args[0].map, args[1].map, args[0].idx, args[1].idx, nullptr};
+  p.d = (int2 *)dev_alloc(sizeof(int2) * (size_t)std::max(1LL, g->nkeys));
+  if (!p.d) return nullptr;
+  if (g->nkeys)
+    k_jac_pairs<<<rt().num_sms * 8, 256, 0, s>>>(g->nkeys, g->d_keys, idx_map(args[0]),
+                                                 idx_map(args[1]), p.d);
+  g_jac_pairs.push_back(p);
+  return p.d;
+}
+
+void release_jac_pairs() {
+  for (auto &p : g_jac_pairs) dev_free(p.d);
+  g_jac_pairs.clear();
+}
 
 template <int V>
 static void jac_res_t(char const *name, op_set set, const op_arg *args) {
@@ -164,10 +244,18 @@ static void jac_res_t(char const *name, op_set set, const op_arg *args) {
   if (!g) return;
   LoopScope ls(name, compulsory_bytes(set, 4, args), 0);
   if (g->nactive == 0) return;
-  k_jac_res_gather<V><<<(g->nactive + 255) / 256, 256, 0, s>>>(
-      g->nactive, g->d_active, g->d_row, g->d_keys, idx_map(args[0]), idx_map(args[1]),
-      (const typename L::AT *)args[0].dat->data_d, (const float *)args[1].dat->data_d,
-      (float *)args[2].dat->data_d, beta);
+  // (edge, u element) per contribution, built once per plan and map pair
+  int2 *pairs = jac_pairs(g, args, s);
+  if (pairs)
+    launch_pdl(k_jac_res_pairs<V>, (unsigned)((g->nactive + 255) / 256), 256, 0, s, g->nactive,
+               (const int *)g->d_active, (const int *)g->d_row, (const int2 *)pairs,
+               (const typename L::AT *)args[0].dat->data_d, (const float *)args[1].dat->data_d,
+               (float *)args[2].dat->data_d, beta);
+  else
+    launch_pdl(k_jac_res_gather<V>, (unsigned)((g->nactive + 255) / 256), 256, 0, s, g->nactive,
+               (const int *)g->d_active, (const int *)g->d_row, (const int *)g->d_keys,
+               idx_map(args[0]), idx_map(args[1]), (const typename L::AT *)args[0].dat->data_d,
+               (const float *)args[1].dat->data_d, (float *)args[2].dat->data_d, beta);
 }
 
 void run_jac_res(char const *name, op_set set, const op_arg *args, int variant) {
@@ -192,10 +280,9 @@ static void jac_update_t(char const *name, op_set set, const op_arg *args) {
     float *seqbuf = seq ? (float *)red_seq_buffer(sizeof(float) * (size_t)n) : nullptr;
     const int threads = 256, grid = red_grid(n, threads);
     RedSlot<float> ss{(float *)red_partials(0), r_sum}, sm{(float *)red_partials(1), r_max};
-    k_jac_update<V><<<grid, threads, 0, s>>>(n, (const float *)args[0].dat->data_d,
-                                             (float *)args[1].dat->data_d,
-                                             (float *)args[2].dat->data_d, alpha, seqbuf, ss, sm,
-                                             red_ticket());
+    launch_pdl(k_jac_update<V>, grid, threads, 0, s, n, (const float *)args[0].dat->data_d,
+               (float *)args[1].dat->data_d, (float *)args[2].dat->data_d, alpha, seqbuf, ss, sm,
+               red_ticket());
     if (seq) k_seq_sum<float><<<1, 32, 0, s>>>(seqbuf, n, *(const float *)args[3].data, r_sum);
   }
   red_finish({GblRequest{args[3].data, slot_sum, OP_INC, GBL_F32, seq},
