@@ -83,6 +83,10 @@ def parse():
     ap.add_argument("--rel-tol", type=float, default=1e-6, help="served: rms tolerance")
     ap.add_argument("--iters-per-step", type=int, default=10,
                     help="served: iterations between completion checks")
+    ap.add_argument("--max-active", type=int, default=0,
+                    help="served: cap on solves iterated together (0: memory budget only)")
+    ap.add_argument("--policy", default="fifo", choices=["fifo", "shortest"],
+                    help="served: admission order")
     ap.add_argument("--plain-sample", type=int, default=16,
                     help="served: requests re-solved with the plain path for its rate")
     return ap.parse_args()
@@ -692,7 +696,8 @@ def impl_served(args, dist):
             meshes[(I, J)] = M.naca0012(I, J)
     api.set_error_mode(api.ERRORS_RETURN)
     warm_paths(dt)
-    srv = S.Server(dt, budget_bytes=args.budget_gb * 1e9, iters_per_step=args.iters_per_step)
+    srv = S.Server(dt, budget_bytes=args.budget_gb * 1e9, iters_per_step=args.iters_per_step,
+                   max_active=args.max_active, policy=args.policy)
     reqs = [S.Request(i, meshes[inst[i][:2]], inst[i][2], inst[i][3], args.max_iter,
                       args.rel_tol, float(arrivals[i])) for i in mine]
     dist.barrier()
@@ -711,7 +716,7 @@ def impl_served(args, dist):
     wall = dist.max(time.perf_counter() - t0)
     stats = S.latency_stats(srv.done)
     iters = np.array([r.iterations for r in srv.done])
-    max_active = srv.max_active
+    max_active = srv.peak_active
     srv.close()
 
     # the plain path on a sample of the same requests, same iteration counts
@@ -733,7 +738,8 @@ def impl_served(args, dist):
         "config": {"workload": "airfoil served: %d requests, stop at rms < %g x first or %d "
                                "iterations, %g GB budget" % (args.requests, args.rel_tol,
                                                               args.max_iter, args.budget_gb),
-                   "iters_per_step": args.iters_per_step,
+                   "iters_per_step": args.iters_per_step, "policy": args.policy,
+                   "max_active": args.max_active,
                    "parallelism": "requests dealt round-robin over %d GPU(s)" % dist.world},
         "latency": stats,
         "wall_seconds": wall,

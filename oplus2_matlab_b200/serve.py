@@ -2,8 +2,9 @@
 
 Requests (mesh + flow condition + stopping rule) arrive at any time.  The
 server keeps every admitted solve's state resident in HBM (op2b_group),
-admits queued requests first-come first-served while the group's device
-bytes plus the request's stay under the memory budget, and advances all
+admits queued requests (first-come first-served, or least work first) while
+the group's device bytes plus the request's stay under the memory budget
+(and, optionally, while fewer than max_active solves run), and advances all
 admitted solves together: each `step` enqueues a few outer iterations of
 every active solve as one launch per loop, admits newly arrived requests
 while those run on the GPU (their uploads and list builds go on the group's
@@ -55,16 +56,23 @@ class Server:
     """Admit, iterate and retire solves on one GPU."""
 
     def __init__(self, dtype=np.float32, budget_bytes=150 * 10**9, iters_per_step=10,
-                 keep_q=False, clock=time.perf_counter):
+                 keep_q=False, clock=time.perf_counter, max_active=0, policy="fifo"):
+        """max_active > 0 caps the solves iterated together (0: memory budget
+        only); policy "fifo" admits in arrival order, "shortest" admits the
+        queued request with the least work (cells x iteration cap) first."""
+        if policy not in ("fifo", "shortest"):
+            raise ValueError("policy must be 'fifo' or 'shortest'")
         self.group = G.Group(dtype)
         self.budget = int(budget_bytes)
         self.k = int(iters_per_step)
         self.keep_q = keep_q
         self.clock = clock
+        self.max_active = int(max_active)
+        self.policy = policy
         self.queue = deque()
         self.active = {}  # sid -> Request
         self.done = []
-        self.max_active = 0
+        self.peak_active = 0
         self.steps = 0
 
     def submit(self, req):
@@ -72,16 +80,21 @@ class Server:
 
     def _admit(self, now):
         g = self.group
+        if self.policy == "shortest" and len(self.queue) > 1:
+            self.queue = deque(sorted(self.queue, key=lambda q: (q.mesh.ncell * q.max_iter,
+                                                                 q.arrival)))
         while self.queue:
+            if self.max_active and len(self.active) >= self.max_active:
+                break
             r = self.queue[0]
             need = g.solve_bytes(r.mesh, r.max_iter)
             if self.active and g.device_bytes() + need > self.budget:
-                break  # head of the queue waits for memory (FIFO)
+                break  # the head of the queue waits for memory
             self.queue.popleft()
             r.sid = g.add(r.mesh, r.mach, r.alpha, r.max_iter, r.rel_tol)
             r.admitted = now
             self.active[r.sid] = r
-        self.max_active = max(self.max_active, len(self.active))
+        self.peak_active = max(self.peak_active, len(self.active))
 
     def step(self):
         """One round: admit, run k iterations, retire; returns the requests

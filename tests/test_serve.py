@@ -84,7 +84,7 @@ def test_served_answers_equal_alone_answers(op2):
         srv.submit(S.Request(k, meshes[ij], mach, alpha, n, 0.0, 0.0))
     while not srv.idle():
         srv.step()
-    assert srv.max_active < len(specs)  # the budget made requests queue
+    assert srv.peak_active < len(specs)  # the budget made requests queue
     assert sorted(r.rid for r in srv.done) == list(range(len(specs)))
     for r in srv.done:
         ij, mach, alpha, n = specs[r.rid]
@@ -95,4 +95,19 @@ def test_served_answers_equal_alone_answers(op2):
         assert r.q.tobytes() == g.fetch_q(sid).tobytes()
         assert r.rms.tobytes() == g.history(sid).tobytes()
         g.close()
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_concurrency_cap_and_shortest_first_policy(op2):
+    sizes = [(40, 60), (20, 30), (30, 45), (20, 30)]
+    meshes = {ij: M.naca0012(*ij) for ij in sizes}
+    srv = S.Server(iters_per_step=5, clock=lambda: 0.0, max_active=1, policy="shortest")
+    for k, ij in enumerate(sizes):
+        srv.submit(S.Request(k, meshes[ij], 0.5, 0.0, 10, 0.0, 0.0))
+    while not srv.idle():
+        srv.step()
+    assert srv.peak_active == 1
+    # one at a time, least work first (ties in arrival order)
+    assert [r.rid for r in srv.done] == [1, 3, 2, 0]
     srv.close()
