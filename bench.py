@@ -11,7 +11,12 @@ stream (Mach 0.4) -- the reference ships no mesh, so this is its generator.
 
 value   device throughput: W untimed warm-up iterations build the plans, then
         one iteration is captured as a CUDA graph (op2b_capture_*) and K
-        launches are timed with CUDA events on the library stream; L2 is
+        launches are timed with CUDA events on the library stream.  The
+        captured iteration is the app's, rotated by two loop calls: res_calc,
+        bres_calc, update, adt_calc, res_calc, bres_calc, update, then the
+        next iteration's save_soln and adt_calc (run once before the first
+        launch), so those two fuse with the update before them; every launch
+        is still one whole outer iteration's loops.  L2 is
         flushed before every step by an untimed read-only sweep of 3x its
         size (op2b_l2_flush; a memset would leave dirty lines whose
         write-back the next step would pay).
@@ -350,16 +355,21 @@ def impl_ours(args, dist):
     assert api.last_error() == "", api.last_error()
 
     # one outer iteration as a CUDA graph: a plain one for the timed steps,
-    # and one with event nodes around every loop for the per-loop times
+    # and one with event nodes around every loop for the per-loop times.
+    # Rotated: the iteration's first save_soln + adt_calc run once here, and
+    # each graph ends with the next iteration's, fused with the last update
+    A.loop("save_soln")
+    A.loop("adt_calc")
+    api.sync()
+    rotated = ("res_calc", "bres_calc", "update", "adt_calc", "res_calc", "bres_calc", "update",
+               "save_soln", "adt_calc")
+
     def capture(profile):
         assert lib.op2b_capture_begin(profile) == 1, api.last_error()
-        A.loop("save_soln")
-        for _ in range(2):
-            A.loop("adt_calc")
-            A.loop("res_calc")
-            A.loop("bres_calc")
-            A.rms[0] = 0
-            A.loop("update")
+        for nm in rotated:
+            if nm == "update":
+                A.rms[0] = 0
+            A.loop(nm)
         h = lib.op2b_capture_end()
         assert h, api.last_error()
         return h
@@ -419,7 +429,7 @@ def impl_ours(args, dist):
     # roofline is taken over the launches that carry the first res_calc of
     # the step, against the compulsory bytes of the loops they run
     chains = [n for n in names if n.split("+")[0] == "res_calc" and ":" not in n]
-    res_key = max(chains, key=lambda n: n.count("+"))
+    res_key = chains[0]
     profiled_launch_s = loop_tot[res_key] / max(1, loop_cnt[res_key])
     # the chain's own launch time: a graph holding only its loop calls
     # (res_calc, bres_calc, update[, adt_calc] -- the same fused launches as in

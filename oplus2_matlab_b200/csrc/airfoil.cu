@@ -500,14 +500,17 @@ struct CellNodes {  // adt_calc's four x arguments through pcell
 };
 // U cells per thread: every index load of the U cells, then every data
 // load, then the arithmetic, so up to U cells' gathers are in flight at
-// once; MINB is the launch-bounds occupancy target (register cap)
-template <class T, bool ADT, int U, int MINB>
+// once; MINB is the launch-bounds occupancy target (register cap).  SAVE:
+// save_soln follows update (the next outer iteration's first loop), so the
+// new q is also stored to qsave -- usually qold itself, which update read at
+// the same cell first, hence the plain (coherent) load of qold
+template <class T, bool ADT, int U, int MINB, bool SAVE = false>
 __global__ void __launch_bounds__(256, MINB)
     k_fold_update(int n, const int *__restrict__ ell, int W, const T *__restrict__ vals,
-                  const T *__restrict__ qold, T *__restrict__ q, T *__restrict__ res,
+                  const T *qold, T *__restrict__ q, T *__restrict__ res,
                   T *__restrict__ adt, CellNodes N, const T *__restrict__ x0,
                   const T *__restrict__ x1, const T *__restrict__ x2, const T *__restrict__ x3,
-                  AirConsts<T> K, T *seq, RedSlot<T> slot, unsigned *ticket) {
+                  AirConsts<T> K, T *seq, RedSlot<T> slot, unsigned *ticket, T *qsave) {
   const bool quad = N.m0.map && N.m0.map == N.m1.map && N.m0.map == N.m2.map &&
                     N.m0.map == N.m3.map && N.m0.dim == 4 && N.m0.idx == 0 && N.m1.idx == 1 &&
                     N.m2.idx == 2 && N.m3.idx == 3;
@@ -544,7 +547,8 @@ __global__ void __launch_bounds__(256, MINB)
       const int c = base + u * stride;
       if (c >= n) continue;
       ldw4(res + 4 * (size_t)c, r[u]);
-      ld4(qold + 4 * (size_t)c, qo[u]);
+      if (SAVE) ldw4(qold + 4 * (size_t)c, qo[u]);
+      else ld4(qold + 4 * (size_t)c, qo[u]);
       ad[u] = adt[c];
 #pragma unroll
       for (int j = 0; j < 4; j++)
@@ -579,6 +583,7 @@ __global__ void __launch_bounds__(256, MINB)
         rms += sq[d];
       }
       st4(q + 4 * (size_t)c, qn);
+      if (SAVE) st4(qsave + 4 * (size_t)c, qn);  // airfoil/save_soln.h:1-3
       const T z[4] = {T(0), T(0), T(0), T(0)};
       st4(res + 4 * (size_t)c, z);
       if (seq) st4(seq + 4 * (size_t)c, sq);
@@ -591,6 +596,107 @@ __global__ void __launch_bounds__(256, MINB)
         k[u][j] = kn[u][j];
         nd[u][j] = ndn[u][j];
       }
+  }
+  if (seq) return;
+  const T v[1] = {rms}, id[1] = {T(0)};
+  RedSlot<T> sl[1] = {slot};
+  grid_finish<T, OpSum, OpSum, 1>(v, id, OpSum(), OpSum(), sl, ticket);
+}
+
+// One cell per thread, with the cell's own streams (res, qold, adt) fetched
+// a cell ahead together with its list and node indices: the next cell's
+// DRAM loads are in flight while this cell's gathers return and its
+// arithmetic runs, so a pass waits on the (mostly L2) gathers alone.  The
+// arithmetic and its order are k_fold_update's.  Reading the next cell's
+// res/qold/adt before this cell's stores is safe: every cell belongs to one
+// thread.
+template <class T, bool ADT, int MINB, bool SAVE>
+__global__ void __launch_bounds__(256, MINB)
+    k_fold_update_pf(int n, const int *__restrict__ ell, int W, const T *__restrict__ vals,
+                     const T *qold, T *__restrict__ q, T *__restrict__ res, T *__restrict__ adt,
+                     CellNodes N, const T *__restrict__ x0, const T *__restrict__ x1,
+                     const T *__restrict__ x2, const T *__restrict__ x3, AirConsts<T> K, T *seq,
+                     RedSlot<T> slot, unsigned *ticket, T *qsave) {
+  const bool quad = N.m0.map && N.m0.map == N.m1.map && N.m0.map == N.m2.map &&
+                    N.m0.map == N.m3.map && N.m0.dim == 4 && N.m0.idx == 0 && N.m1.idx == 1 &&
+                    N.m2.idx == 2 && N.m3.idx == 3;
+  const int stride = gridDim.x * blockDim.x;
+  T rms = T(0);
+  auto indices = [&](int c, int (&kk)[4], int (&nn)[4]) {
+    list_head(ell, W, c, kk);
+    if (ADT) {
+      if (quad) {
+        int4 v = __ldg(reinterpret_cast<const int4 *>(N.m0.map) + c);
+        nn[0] = v.x; nn[1] = v.y; nn[2] = v.z; nn[3] = v.w;
+      } else {
+        nn[0] = at(N.m0, c); nn[1] = at(N.m1, c); nn[2] = at(N.m2, c); nn[3] = at(N.m3, c);
+      }
+    }
+  };
+  auto streams = [&](int c, T (&r)[4], T (&qo)[4], T &ad) {
+    ldw4(res + 4 * (size_t)c, r);
+    if (SAVE) ldw4(qold + 4 * (size_t)c, qo);
+    else ld4(qold + 4 * (size_t)c, qo);
+    ad = adt[c];
+  };
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  int k[4] = {-1, -1, -1, -1}, nd[4] = {0, 0, 0, 0};
+  if (c < n) indices(c, k, nd);  // before the previous kernel has finished
+  pdl_wait();
+  pdl_trigger();
+  T r[4], qo[4], ad = T(1);
+  if (c < n) streams(c, r, qo, ad);
+  for (; c < n; c += stride) {
+    T f[4][4], xs[4][2];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (k[j] >= 0) ld4(vals + 4 * (size_t)(k[j] >> 1), f[j]);
+    if (ADT) {
+      ld2(x0 + 2 * (size_t)nd[0], xs[0]);
+      ld2(x1 + 2 * (size_t)nd[1], xs[1]);
+      ld2(x2 + 2 * (size_t)nd[2], xs[2]);
+      ld2(x3 + 2 * (size_t)nd[3], xs[3]);
+    }
+    const int cn = c + stride;
+    int kn[4] = {-1, -1, -1, -1}, ndn[4] = {0, 0, 0, 0};
+    T rn[4], qon[4], adn = T(1);
+    if (cn < n) {
+      indices(cn, kn, ndn);
+      streams(cn, rn, qon, adn);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) add_listed(r, k[j], f[j]);
+    for (int j = 4; j < W; j++) {  // lists longer than 4
+      const int kk = __ldg(ell + (size_t)c * W + j);
+      T g[4];
+      ld4(vals + 4 * (size_t)(kk >> 1), g);
+      add_listed(r, kk, g);
+    }
+    // airfoil/update.h:1-12
+    T adti = rcp(ad);
+    T qn[4], sq[4];
+    for (int d = 0; d < 4; d++) {
+      T del = adti * r[d];
+      qn[d] = qo[d] - del;
+      sq[d] = del * del;
+      rms += sq[d];
+    }
+    st4(q + 4 * (size_t)c, qn);
+    if (SAVE) st4(qsave + 4 * (size_t)c, qn);  // airfoil/save_soln.h:1-3
+    const T z[4] = {T(0), T(0), T(0), T(0)};
+    st4(res + 4 * (size_t)c, z);
+    if (seq) st4(seq + 4 * (size_t)c, sq);
+    if (ADT) adt[c] = adt_calc(xs[0], xs[1], xs[2], xs[3], qn, K);
+    if (cn < n) {
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        k[j] = kn[j];
+        nd[j] = ndn[j];
+        r[j] = rn[j];
+        qo[j] = qon[j];
+      }
+      ad = adn;
+    }
   }
   if (seq) return;
   const T v[1] = {rms}, id[1] = {T(0)};
@@ -948,7 +1054,7 @@ static void res_calc_t(char const *name, op_set set, const op_arg *args) {
   GatherPlan *g = get_gather_plan(set, args, {6, 7});
   if (!g) return;
   if (tuning("gather_flux", 1) && tuning("gather_slots", 1) &&
-      run_res_chain(name, set, args, nullptr, nullptr, nullptr, nullptr))
+      run_res_chain(name, set, args, nullptr, nullptr, nullptr, nullptr, nullptr))
     return;
   LoopScope ls(name, compulsory_bytes(set, 8, args), 0);
   if (g->nactive == 0) return;
@@ -1342,7 +1448,7 @@ static bool res_bres_t(op_set rset, const op_arg *ra, op_set bset, const op_arg 
 
 bool run_res_bres(op_set rset, const op_arg *ra, op_set bset, const op_arg *ba) {
   if (tuning("gather_slots", 1) &&
-      run_res_chain(nullptr, rset, ra, bset, ba, nullptr, nullptr))
+      run_res_chain(nullptr, rset, ra, bset, ba, nullptr, nullptr, nullptr))
     return true;
   return is_double(ra[0]) ? res_bres_t<double>(rset, ra, bset, ba)
                           : res_bres_t<float>(rset, ra, bset, ba);
@@ -1353,7 +1459,10 @@ bool run_res_bres(op_set rset, const op_arg *ra, op_set bset, const op_arg *ba) 
 // update follows, applies it (and adt_calc) to the cell before storing
 template <class T>
 static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op_set bset,
-                        const op_arg *ba, const op_arg *ua, const op_arg *aa) {
+                        const op_arg *ba, const op_arg *ua, const op_arg *aa, const op_arg *sa) {
+  // save_soln rides on the one-cell-per-thread fold + update + adt_calc forms
+  const int fvar = tuning("fold_variant", 0);
+  if (sa && (!ua || !aa || (fvar != 0 && fvar != 4 && fvar != 5))) return false;
   AirConsts<T> K = air_consts<T>();
   if (error_pending()) return true;
   cudaStream_t s = rt().stream;
@@ -1379,6 +1488,7 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
   double bytes = compulsory_bytes(rset, 8, ra);
   if (ba) name += "+bres_calc", bytes += compulsory_bytes(bset, 6, ba);
   if (ua) name += "+update", bytes += compulsory_bytes(ra[6].dat->set, 5, ua);
+  if (sa) name += "+save_soln", bytes += compulsory_bytes(ra[6].dat->set, 2, sa);
   if (aa) name += "+adt_calc", bytes += compulsory_bytes(ra[6].dat->set, 6, aa);
   const bool seq = ua && rt().reduction == OP2B_REDUCE_SEQ;
   int rslot_id = ua ? red_new_slot() : -1;
@@ -1433,15 +1543,21 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
                  (const int *)sp->d_ell, W, (const T *)vals, res);
     } else {
       T *seqbuf = seq ? (T *)red_seq_buffer(sizeof(T) * 4 * (size_t)ncell) : nullptr;
-      // a few waves of grid-stride CTAs (fewer, longer CTAs beat one cell
-      // per thread: each CTA ends with a block reduction and a ticket):
-      // measured best at 4 CTAs per SM for the fold + update (one wave at
-      // its occupancy) and 6 with adt_calc; fixed by ncell, so sums
-      // reproduce.  0: one cell per thread
-      long long gw = (ncell + 255LL) / 256;
-      const int per_sm = aa ? tuning("fold_adt_ctas_per_sm", 6) : tuning("fold_ctas_per_sm", 4);
-      long long gcap = per_sm > 0 ? (long long)rt().num_sms * per_sm : (long long)kMaxRedBlocks;
-      const int grid = (int)std::max(1LL, std::min(gw, std::min(gcap, (long long)kMaxRedBlocks)));
+      // one wave of grid-stride CTAs: as many as the kernel keeps resident
+      // on every SM at once (fewer, longer CTAs beat one cell per thread --
+      // each CTA ends with a block reduction and a ticket -- and a second
+      // wave of CTAs starting late leaves SMs idle at the end: measured
+      // 25.6 -> 21.3 us for the fold + update + adt_calc at 720k cells).
+      // The grid depends only on ncell and the kernel, so sums reproduce.
+      // Knob > 0: that many CTAs per SM; 0: one cell per thread
+      const long long gw = (ncell + 255LL) / 256;
+      const int per_sm = aa ? tuning("fold_adt_ctas_per_sm", -1) : tuning("fold_ctas_per_sm", -1);
+      auto grid_of = [&](const void *kernel) {
+        long long per = per_sm;
+        if (per < 0) per = resident_ctas(kernel, 256);
+        long long gcap = per > 0 ? (long long)rt().num_sms * per : (long long)kMaxRedBlocks;
+        return (int)std::max(1LL, std::min(gw, std::min(gcap, (long long)kMaxRedBlocks)));
+      };
       T *result = (T *)red_slot_ptr(rslot_id);
       RedSlot<T> rslot{(T *)red_partials(0), result};
       const T *qold = (const T *)ua[0].dat->data_d;
@@ -1453,25 +1569,37 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
         N = CellNodes{idx_map(aa[0]), idx_map(aa[1]), idx_map(aa[2]), idx_map(aa[3])};
         for (int i = 0; i < 4; i++) xs[i] = (const T *)aa[i].dat->data_d;
       }
-      // fold_variant: 0 one cell per thread at >= 4 CTAs per SM (3 with
-      // adt_calc); 1 the same at >= 6; 2 two cells per thread; 3 two cells
-      // at >= 3 CTAs per SM
+      // fold_variant: 0 one cell per thread at >= 5 CTAs per SM (4 with
+      // adt_calc; FP64 2), measured best; 1 the same at >= 6; 2 two cells
+      // per thread; 3 two cells at >= 3 CTAs per SM; 4 one cell per thread
+      // at >= 4 (3 with adt_calc; FP64 3); 5 one cell per thread, the
+      // cell's own streams fetched a cell ahead
+      T *qsave = sa ? (T *)sa[1].dat->data_d : nullptr;
       auto launch = [&](auto kernel) {
-        launch_pdl(kernel, grid, 256, 0, s, ncell, (const int *)sp->d_ell, W, (const T *)vals,
+        launch_pdl(kernel, grid_of((const void *)kernel), 256, 0, s, ncell,
+                   (const int *)sp->d_ell, W, (const T *)vals,
                    qold, q, res, adt, N, xs[0], xs[1], xs[2], xs[3], K, seqbuf, rslot,
-                   red_ticket());
+                   red_ticket(), qsave);
       };
-      const int fv = tuning("fold_variant", 0);
-      if (aa) {
+      const int fv = fvar;
+      if (sa) {
+        if (fv == 4) launch(k_fold_update<T, true, 1, 3, true>);
+        else if (fv == 5) launch(k_fold_update_pf<T, true, sizeof(T) == 4 ? 3 : 2, true>);
+        else launch(k_fold_update<T, true, 1, sizeof(T) == 4 ? 4 : 2, true>);
+      } else if (aa) {
         if (fv == 1) launch(k_fold_update<T, true, 1, 6>);
         else if (fv == 2) launch(k_fold_update<T, true, 2, 1>);
         else if (fv == 3) launch(k_fold_update<T, true, 2, 3>);
-        else launch(k_fold_update<T, true, 1, sizeof(T) == 4 ? 3 : 2>);
+        else if (fv == 4) launch(k_fold_update<T, true, 1, 3>);
+        else if (fv == 5) launch(k_fold_update_pf<T, true, sizeof(T) == 4 ? 3 : 2, false>);
+        else launch(k_fold_update<T, true, 1, sizeof(T) == 4 ? 4 : 2>);
       } else {
         if (fv == 1) launch(k_fold_update<T, false, 1, 6>);
         else if (fv == 2) launch(k_fold_update<T, false, 2, 1>);
         else if (fv == 3) launch(k_fold_update<T, false, 2, 3>);
-        else launch(k_fold_update<T, false, 1, sizeof(T) == 4 ? 4 : 2>);
+        else if (fv == 4) launch(k_fold_update<T, false, 1, sizeof(T) == 4 ? 4 : 3>);
+        else if (fv == 5) launch(k_fold_update_pf<T, false, sizeof(T) == 4 ? 4 : 2, false>);
+        else launch(k_fold_update<T, false, 1, sizeof(T) == 4 ? 5 : 2>);
       }
       if (seq) {
         T init = *(const T *)ua[4].data;
@@ -1485,9 +1613,9 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
 }
 
 bool run_res_chain(char const *name, op_set rset, const op_arg *ra, op_set bset,
-                   const op_arg *ba, const op_arg *ua, const op_arg *aa) {
-  return is_double(ra[0]) ? res_chain_t<double>(name, rset, ra, bset, ba, ua, aa)
-                          : res_chain_t<float>(name, rset, ra, bset, ba, ua, aa);
+                   const op_arg *ba, const op_arg *ua, const op_arg *aa, const op_arg *sa) {
+  return is_double(ra[0]) ? res_chain_t<double>(name, rset, ra, bset, ba, ua, aa, sa)
+                          : res_chain_t<float>(name, rset, ra, bset, ba, ua, aa, sa);
 }
 
 }  // namespace op2b

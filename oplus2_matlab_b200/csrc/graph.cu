@@ -36,6 +36,7 @@ int op2b_capture_begin(int profile) {
   ensure_cuda();
   if (error_pending()) return 0;
   Runtime &R = rt();
+  flush_pending();  // loops held back before the capture run outside the graph
   deliver_deferred();
   g_pending_mark = red_pending_count();
   R.capture_events.clear();

@@ -18,6 +18,7 @@
 
 #include <cuda_runtime.h>
 
+#include <unordered_map>
 #include <utility>
 
 #include "internal.h"
@@ -45,6 +46,21 @@ inline void launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, 
   cfg.attrs = attr;
   cfg.numAttrs = tuning("pdl", 1) ? 1 : 0;
   OP2B_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+}
+
+// CTAs of `threads` threads (no dynamic shared memory) that one SM keeps
+// resident at once for `kernel`: the size of one wave of a grid-stride
+// grid is that times the SM count.  Cached per kernel (the host-side query
+// costs microseconds; a loop call should not pay it each time).
+inline int resident_ctas(const void *kernel, int threads) {
+  static std::unordered_map<const void *, int> cache;
+  auto it = cache.find(kernel);
+  if (it != cache.end()) return it->second;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0) != cudaSuccess || n < 1)
+    n = 1;
+  cache.emplace(kernel, n);
+  return n;
 }
 
 }  // namespace op2b

@@ -161,7 +161,8 @@ void run_kind(Kind k, int variant, char const *name, op_set set, const op_arg *a
 }
 
 // The loops held back in case the next call can be fused with them: one of
-// save_soln, update, res_calc; res_calc+bres_calc; res_calc+bres_calc+update.
+// save_soln, update, res_calc; res_calc+bres_calc; res_calc+bres_calc+update;
+// res_calc+bres_calc+update+save_soln.
 struct Held {
   Kind kind = K_NONE;
   std::string name;
@@ -203,6 +204,14 @@ bool update_follows_res(const op_arg *r, op_set set, const op_arg *u) {
          u[3].dat != res;
 }
 
+// save_soln(q -> qold') after update(qold, q, res, adt) on the same set: it
+// copies the q update just wrote, at the same cell, to a dataset that is
+// none of q, res, adt (update's qold is allowed: update reads it at the cell
+// before the copy overwrites it)
+bool save_follows_update(const op_arg *u, op_set uset, op_set set, const op_arg *sv) {
+  return set == uset && sv[0].dat == u[1].dat && !dat_in(sv[1].dat, {u[1].dat, u[2].dat, u[3].dat});
+}
+
 // the update may wait for the next call only when its reduction need not
 // reach the host before its own call returns
 bool update_holdable() { return rt().gbl_deferred && rt().reduction == OP2B_REDUCE_TREE; }
@@ -213,6 +222,16 @@ bool res_holdable() {
 
 // run a chain, fused as far as the kernels allow
 void run_chain(const std::vector<Held> &ch, const Held *adt) {
+  if (ch.size() == 4) {  // res_calc, bres_calc, update, save_soln
+    const Held &sv = ch[3];
+    if (adt && tuning("gather_slots", 1) &&
+        run_res_chain(nullptr, ch[0].set, ch[0].args.data(), ch[1].set, ch[1].args.data(),
+                      ch[2].args.data(), adt->args.data(), sv.args.data()))
+      return;
+    run_chain(std::vector<Held>(ch.begin(), ch.begin() + 3), nullptr);
+    run_chain(std::vector<Held>{sv}, adt);
+    return;
+  }
   const Held &h0 = ch[0];
   const op_arg *a0 = h0.args.data();
   if (ch.size() == 1) {
@@ -284,6 +303,20 @@ bool extend_chain(Kind k, char const *name, op_set set, int nargs, const op_arg 
     return true;
   }
   if (n == 3 && k == K_ADT && adt_follows_update(g_chain[2].args.data(), g_chain[2].set, set, a)) {
+    Held adt = make_held(k, name, set, nargs, a);
+    std::vector<Held> ch;
+    std::swap(ch, g_chain);
+    run_chain(ch, &adt);
+    return true;
+  }
+  // the next outer iteration's save_soln, then its adt_calc, join the update
+  if (n == 3 && k == K_SAVE && tuning("fuse_save", 1) &&
+      save_follows_update(g_chain[2].args.data(), g_chain[2].set, set, a)) {
+    g_chain.push_back(make_held(k, name, set, nargs, a));
+    return true;
+  }
+  if (n == 4 && k == K_ADT && adt_follows_update(g_chain[2].args.data(), g_chain[2].set, set, a) &&
+      !dat_in(g_chain[3].args[1].dat, {a[0].dat, a[1].dat, a[2].dat, a[3].dat})) {
     Held adt = make_held(k, name, set, nargs, a);
     std::vector<Held> ch;
     std::swap(ch, g_chain);
