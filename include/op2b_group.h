@@ -9,7 +9,9 @@
  * res_calc + bres_calc + update [+ adt_calc]) runs as one launch over a
  * whole block of active solves (all of them, or as many as keep the block's
  * intermediate values in L2): a tile table lists tiles of one solve's
- * elements, and each CTA works on one tile.  The per-element arithmetic is the plain path's
+ * elements, and each CTA works on one tile.  The iteration is rotated: the
+ * next iteration's save_soln + adt_calc run in the second update's launch,
+ * and a solve's first ones in a launch before its first iteration.  The per-element arithmetic is the plain path's
  * (same device functions, same contribution order), so a solve's flow field
  * q is bit-identical to the plain op_par_loop solve of the same mesh and
  * flow.  Each solve's rms is folded from its own tiles' partials, in tile
@@ -80,7 +82,7 @@ long long op2b_group_device_bytes(op2b_group g);
 int op2b_group_active(op2b_group g); /* solves in the launches (joined, not stopped) */
 
 /* An iteration runs block by block over the solves (in id order), each
- * block's five launches together, so that a block's flux values -- written
+ * block's launches together, so that a block's flux values -- written
  * by one launch, read by the next -- stay in L2: a block holds up to `bytes`
  * of values (<= 0, the default: all solves in one block).  Results do not
  * depend on it. */

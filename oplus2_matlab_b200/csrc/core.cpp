@@ -160,17 +160,25 @@ op_map op_decl_map(op_set from, op_set to, int dim, int *imap, char const *name)
     fail(-1, "op_decl_map error -- negative/zero dimension for map %s\n", name);
     return nullptr;
   }
-  for (int d = 0; d < dim; d++)
-    for (int n = 0; n < from->size; n++) {
-      int v = imap[d + (size_t)n * dim];
-      if (v < 0 || v >= to->size) {
-        fail(-1,
-             "op_decl_map error -- invalid data for map %s\n"
-             "element = %d, dimension = %d, map = %d\n",
-             name, n, d, v);
-        return nullptr;
+  // one contiguous, vectorisable pass decides whether any entry is out of
+  // range; only then the reference's dimension-major scan finds the first
+  // bad entry for the message
+  const size_t nent = (size_t)dim * from->size;
+  const unsigned lim = (unsigned)to->size;
+  unsigned bad = 0;
+  for (size_t i = 0; i < nent; i++) bad |= (unsigned)((unsigned)imap[i] >= lim);
+  if (bad)
+    for (int d = 0; d < dim; d++)
+      for (int n = 0; n < from->size; n++) {
+        int v = imap[d + (size_t)n * dim];
+        if (v < 0 || v >= to->size) {
+          fail(-1,
+               "op_decl_map error -- invalid data for map %s\n"
+               "element = %d, dimension = %d, map = %d\n",
+               name, n, d, v);
+          return nullptr;
+        }
       }
-    }
   if (!grow(&OP_map_list, OP_map_index, &OP_map_max)) {
     fail(-1, " op_decl_map error -- error reallocating memory\n");
     return nullptr;

@@ -43,6 +43,7 @@ void ensure_cuda() {
   cudaDeviceProp prop;
   OP2B_CUDA(cudaGetDeviceProperties(&prop, R.device));
   R.num_sms = prop.multiProcessorCount;
+  R.device_name = prop.name;
   if (prop.major < 10)
     fail(-1, "op2b error: device %s is sm_%d%d; this library is built for sm_100a\n", prop.name,
          prop.major, prop.minor);
@@ -238,9 +239,7 @@ void op_init(int argc, char **argv, int diags) {
   op_init_core(argc, argv, diags);
   ensure_cuda();
   if (!rt().cuda_ready) return;
-  cudaDeviceProp prop;
-  cudaGetDeviceProperties(&prop, rt().device);
-  printf("\n Using CUDA device: %s\n", prop.name);
+  printf("\n Using CUDA device: %s\n", rt().device_name.c_str());
 }
 
 // common/op_lib.cu:145-153: registry entry + device copy (synchronous, so

@@ -3,12 +3,16 @@
 //
 // Each solve keeps its own datasets, maps and contribution lists in HBM (one
 // stream-ordered allocation per solve).  One outer iteration of every active
-// solve is five launches, the same five as the plain path's fused chains:
-//   k_grp_save_adt      save_soln + adt_calc              (cell tiles)
+// solve is four launches, the plain path's fused chains with the iteration
+// rotated so that save_soln + adt_calc ride on the last update:
 //   k_grp_flux          res_calc flux + bres_calc values  (edge tiles)
-//   k_grp_fold<true>    fold + update + adt_calc          (cell tiles)
+//   k_grp_fold<0>       fold + update + adt_calc          (cell tiles)
 //   k_grp_flux
-//   k_grp_fold<false>   fold + update + rms               (cell tiles)
+//   k_grp_fold<2>       fold + update + rms, then the next iteration's
+//                       save_soln + adt_calc              (cell tiles)
+// A solve's first save_soln + adt_calc (k_grp_save_adt) is a launch of its
+// own before its first iteration.  With the "group_rotate" knob at 0 the
+// iteration is k_grp_save_adt, flux, fold<0>, flux, fold<1> (no save).
 // A tile is a run of one solve's elements; a launch's grid is its tile table,
 // so one launch covers many solves, whatever their sizes: a block of solves
 // whose intermediate flux values fit L2 together (Group::rebuild).  The device
@@ -160,12 +164,17 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 8 : 4)
 }
 
 // the cell pass: fold each cell's listed values onto res in list order, then
-// update (airfoil/update.h:1-12); FIRST: then adt_calc on the new q, no rms;
-// otherwise: the rms partial, and the solve's last CTA ends the iteration
-template <class T, bool FIRST>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? (FIRST ? 3 : 4) : 2)
+// update (airfoil/update.h:1-12).  MODE 0 (the iteration's first update):
+// then adt_calc on the new q, no rms.  MODE 1 (its second): the rms partial,
+// and the solve's last CTA ends the iteration.  MODE 2: MODE 1 plus the next
+// iteration's save_soln and adt_calc on the new q (qold = q, then adt), so
+// that iteration starts at its res_calc; update reads qold at the cell
+// before the copy overwrites it, hence the coherent load
+template <class T, int MODE>
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? (MODE == 1 ? 4 : 3) : 2)
     k_grp_fold(const Tile *__restrict__ tiles, const SolveDev<T> *__restrict__ sd,
                SolveState *st, AirConsts<T> K) {
+  constexpr bool FIRST = MODE == 0, ADT = MODE != 1, SAVE = MODE == 2;
   const Tile t = tiles[blockIdx.x];
   const SolveDev<T> *d = sd + t.solve;
   const int W = d->W;
@@ -177,7 +186,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? (FIRST ? 3 : 4) : 2
   int4 nd = make_int4(0, 0, 0, 0);
   if ((int)threadIdx.x < t.count) {
     list_head(ell, W, t.start + threadIdx.x, k);
-    if (FIRST) nd = __ldg(pcell + t.start + threadIdx.x);
+    if (ADT) nd = __ldg(pcell + t.start + threadIdx.x);
   }
   pdl_wait();
   pdl_trigger();
@@ -191,12 +200,13 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? (FIRST ? 3 : 4) : 2
     const int c = t.start + i;
     T r[4], qo[4], f[4][4], xs[4][2];
     ldw4(res + 4 * (size_t)c, r);
-    ld4(qold + 4 * (size_t)c, qo);
+    if (SAVE) ldw4(qold + 4 * (size_t)c, qo);
+    else ld4(qold + 4 * (size_t)c, qo);
     const T ad = adt[c];
 #pragma unroll
     for (int m = 0; m < 4; m++)
       if (k[m] >= 0) ld4(vals + 4 * (size_t)(k[m] >> 1), f[m]);
-    if (FIRST) {
+    if (ADT) {
       ld2(x + 2 * (size_t)nd.x, xs[0]);
       ld2(x + 2 * (size_t)nd.y, xs[1]);
       ld2(x + 2 * (size_t)nd.z, xs[2]);
@@ -205,7 +215,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? (FIRST ? 3 : 4) : 2
     int kc[4] = {k[0], k[1], k[2], k[3]};
     if (i + kThreads < t.count) {
       list_head(ell, W, c + kThreads, k);
-      if (FIRST) nd = __ldg(pcell + c + kThreads);
+      if (ADT) nd = __ldg(pcell + c + kThreads);
     }
 #pragma unroll
     for (int m = 0; m < 4; m++) add_listed(r, kc[m], f[m]);
@@ -223,9 +233,10 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? (FIRST ? 3 : 4) : 2
       rms += del * del;
     }
     st4(q + 4 * (size_t)c, qn);
+    if (SAVE) st4(d->qold + 4 * (size_t)c, qn);  // airfoil/save_soln.h:1-3
     const T z[4] = {T(0), T(0), T(0), T(0)};
     st4(res + 4 * (size_t)c, z);
-    if (FIRST) adt[c] = adt_calc(xs[0], xs[1], xs[2], xs[3], qn, K);
+    if (ADT) adt[c] = adt_calc(xs[0], xs[1], xs[2], xs[3], qn, K);
   }
   if (FIRST) return;
   __shared__ T ws[32];
@@ -401,6 +412,9 @@ struct Group : GroupBase {
     size_t bytes = 0;
     cudaEvent_t ready = nullptr;
     bool joined = false, removed = false, done = false, reported = false;
+    // its qold and adt hold the next iteration's save_soln + adt_calc (done
+    // by the previous iteration's last launch, or by the priming launch)
+    bool primed = false;
     long long join_epoch = 0;  // the first state mirror that includes this solve
     SolveDev<T> dev;
   };
@@ -411,9 +425,13 @@ struct Group : GroupBase {
   SolveState *d_st = nullptr;
   SolveState *h_st = nullptr;  // pinned mirror, filled after each run
   int cap = 0;
-  Tile *d_ct = nullptr, *d_et = nullptr;
-  size_t ct_cap = 0, et_cap = 0;
-  int nct = 0, net = 0, nactive = 0;
+  Tile *d_ct = nullptr, *d_et = nullptr, *d_pt = nullptr;
+  size_t ct_cap = 0, et_cap = 0, pt_cap = 0;
+  int nct = 0, net = 0, npt = 0, nactive = 0;
+  // rotated iteration: res_calc ... update, update + the next iteration's
+  // save_soln + adt_calc -- four launches; a solve's very first save_soln +
+  // adt_calc is a priming launch of its own (pt: the unprimed solves' tiles)
+  bool rotate = true;
   int etile = 2048;
   bool changed = true;
   cudaGraphExec_t exec = nullptr;
@@ -445,6 +463,7 @@ struct Group : GroupBase {
     cudaFree(d_st);
     cudaFree(d_ct);
     cudaFree(d_et);
+    cudaFree(d_pt);
     if (h_st) cudaFreeHost(h_st);
     if (mirror_ev) cudaEventDestroy(mirror_ev);
     if (cs) cudaStreamDestroy(cs);
@@ -637,14 +656,18 @@ struct Group : GroupBase {
   size_t block_bytes = ~(size_t)0;
 
   void rebuild() {
-    std::vector<Tile> ct, et;
+    std::vector<Tile> ct, et, pt;
     blocks.clear();
     nactive = 0;
+    rotate = tuning("group_rotate", 1) != 0;
     size_t in_block = 0;
     for (int id = 0; id < (int)solves.size(); id++) {
       const Solve &s = solves[id];
       if (!s.joined || s.removed || s.done) continue;
       nactive++;
+      if (rotate && !s.primed)
+        for (int a = 0, l = 0; a < s.ncell; a += kCellTile, l++)
+          pt.push_back(Tile{id, a, std::min(kCellTile, s.ncell - a), l});
       const int nv = s.nedge + s.nbedge;
       const size_t vbytes = sizeof(T) * 4 * (size_t)nv;
       if (blocks.empty() || (in_block > 0 && in_block + vbytes > block_bytes)) {
@@ -661,8 +684,10 @@ struct Group : GroupBase {
     }
     upload_tiles(d_ct, ct_cap, ct);
     upload_tiles(d_et, et_cap, et);
+    upload_tiles(d_pt, pt_cap, pt);
     nct = (int)ct.size();
     net = (int)et.size();
+    npt = (int)pt.size();
     if (exec) {
       cudaGraphExecDestroy(exec);
       exec = nullptr;
@@ -681,16 +706,31 @@ struct Group : GroupBase {
 
   void iteration(const Block &b) {
     const Tile *ct = d_ct + b.ct0, *et = d_et + b.et0;
-    launch_pdl(k_grp_save_adt<T>, b.nct, kThreads, 0, cs, ct, (const SolveDev<T> *)d_sd,
-               (const SolveState *)d_st, K);
+    if (!rotate)
+      launch_pdl(k_grp_save_adt<T>, b.nct, kThreads, 0, cs, ct, (const SolveDev<T> *)d_sd,
+                 (const SolveState *)d_st, K);
     launch_pdl(k_grp_flux<T>, b.net, kThreads, 0, cs, et, (const SolveDev<T> *)d_sd,
                (const SolveState *)d_st, K);
-    launch_pdl(k_grp_fold<T, true>, b.nct, kThreads, 0, cs, ct, (const SolveDev<T> *)d_sd, d_st,
-               K);
+    launch_pdl(k_grp_fold<T, 0>, b.nct, kThreads, 0, cs, ct, (const SolveDev<T> *)d_sd, d_st, K);
     launch_pdl(k_grp_flux<T>, b.net, kThreads, 0, cs, et, (const SolveDev<T> *)d_sd,
                (const SolveState *)d_st, K);
-    launch_pdl(k_grp_fold<T, false>, b.nct, kThreads, 0, cs, ct, (const SolveDev<T> *)d_sd, d_st,
-               K);
+    if (rotate)
+      launch_pdl(k_grp_fold<T, 2>, b.nct, kThreads, 0, cs, ct, (const SolveDev<T> *)d_sd, d_st,
+                 K);
+    else
+      launch_pdl(k_grp_fold<T, 1>, b.nct, kThreads, 0, cs, ct, (const SolveDev<T> *)d_sd, d_st,
+                 K);
+  }
+
+  // save_soln + adt_calc of the solves that have not had them yet (rotated
+  // iteration only), before their first iteration
+  void prime() {
+    if (!rotate || npt == 0) return;
+    launch_pdl(k_grp_save_adt<T>, npt, kThreads, 0, cs, (const Tile *)d_pt,
+               (const SolveDev<T> *)d_sd, (const SolveState *)d_st, K);
+    for (auto &s : solves)
+      if (s.joined && !s.removed && !s.done) s.primed = true;
+    npt = 0;
   }
 
   int join_pending() {
@@ -722,6 +762,7 @@ struct Group : GroupBase {
     if (error_pending()) return -1;
     if (changed) rebuild();
     if (error_pending()) return -1;
+    if (exec && niter > 0) prime();
     if (exec)
       for (int i = 0; i < niter; i++) OP2B_CUDA(cudaGraphLaunch(exec, cs));
     if ((int)solves.size() > 0 && cap > 0) {
@@ -845,6 +886,7 @@ struct Group : GroupBase {
     join_pending();
     if (changed) rebuild();
     if (nactive == 0 || iters <= 0) return etile;
+    prime();  // before the snapshot: trials start from primed solves
     // snapshot of everything an iteration writes
     std::vector<std::pair<void *, size_t>> regions;
     for (auto &s : solves) {
