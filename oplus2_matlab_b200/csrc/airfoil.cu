@@ -503,14 +503,17 @@ struct CellNodes {  // adt_calc's four x arguments through pcell
 // once; MINB is the launch-bounds occupancy target (register cap).  SAVE:
 // save_soln follows update (the next outer iteration's first loop), so the
 // new q is also stored to qsave -- usually qold itself, which update read at
-// the same cell first, hence the plain (coherent) load of qold
+// the same cell first, hence the plain (coherent) load of qold.  adt_out,
+// when not null, receives adt_calc's values instead of adt (update still
+// reads adt): the loops run ahead of their calls into spare buffers
 template <class T, bool ADT, int U, int MINB, bool SAVE = false>
 __global__ void __launch_bounds__(256, MINB)
     k_fold_update(int n, const int *__restrict__ ell, int W, const T *__restrict__ vals,
                   const T *qold, T *__restrict__ q, T *__restrict__ res,
                   T *__restrict__ adt, CellNodes N, const T *__restrict__ x0,
                   const T *__restrict__ x1, const T *__restrict__ x2, const T *__restrict__ x3,
-                  AirConsts<T> K, T *seq, RedSlot<T> slot, unsigned *ticket, T *qsave) {
+                  AirConsts<T> K, T *seq, RedSlot<T> slot, unsigned *ticket, T *qsave,
+                  T *adt_out) {
   const bool quad = N.m0.map && N.m0.map == N.m1.map && N.m0.map == N.m2.map &&
                     N.m0.map == N.m3.map && N.m0.dim == 4 && N.m0.idx == 0 && N.m1.idx == 1 &&
                     N.m2.idx == 2 && N.m3.idx == 3;
@@ -587,7 +590,7 @@ __global__ void __launch_bounds__(256, MINB)
       const T z[4] = {T(0), T(0), T(0), T(0)};
       st4(res + 4 * (size_t)c, z);
       if (seq) st4(seq + 4 * (size_t)c, sq);
-      if (ADT) adt[c] = adt_calc(xs[u][0], xs[u][1], xs[u][2], xs[u][3], qn, K);
+      if (ADT) (adt_out ? adt_out : adt)[c] = adt_calc(xs[u][0], xs[u][1], xs[u][2], xs[u][3], qn, K);
     }
 #pragma unroll
     for (int u = 0; u < U; u++)
@@ -616,7 +619,7 @@ __global__ void __launch_bounds__(256, MINB)
                      const T *qold, T *__restrict__ q, T *__restrict__ res, T *__restrict__ adt,
                      CellNodes N, const T *__restrict__ x0, const T *__restrict__ x1,
                      const T *__restrict__ x2, const T *__restrict__ x3, AirConsts<T> K, T *seq,
-                     RedSlot<T> slot, unsigned *ticket, T *qsave) {
+                     RedSlot<T> slot, unsigned *ticket, T *qsave, T *adt_out) {
   const bool quad = N.m0.map && N.m0.map == N.m1.map && N.m0.map == N.m2.map &&
                     N.m0.map == N.m3.map && N.m0.dim == 4 && N.m0.idx == 0 && N.m1.idx == 1 &&
                     N.m2.idx == 2 && N.m3.idx == 3;
@@ -686,7 +689,7 @@ __global__ void __launch_bounds__(256, MINB)
     const T z[4] = {T(0), T(0), T(0), T(0)};
     st4(res + 4 * (size_t)c, z);
     if (seq) st4(seq + 4 * (size_t)c, sq);
-    if (ADT) adt[c] = adt_calc(xs[0], xs[1], xs[2], xs[3], qn, K);
+    if (ADT) (adt_out ? adt_out : adt)[c] = adt_calc(xs[0], xs[1], xs[2], xs[3], qn, K);
     if (cn < n) {
 #pragma unroll
       for (int j = 0; j < 4; j++) {
@@ -1459,7 +1462,8 @@ bool run_res_bres(op_set rset, const op_arg *ra, op_set bset, const op_arg *ba) 
 // update follows, applies it (and adt_calc) to the cell before storing
 template <class T>
 static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op_set bset,
-                        const op_arg *ba, const op_arg *ua, const op_arg *aa, const op_arg *sa) {
+                        const op_arg *ba, const op_arg *ua, const op_arg *aa, const op_arg *sa,
+                        void *adt_out, void *save_out) {
   // save_soln rides on the one-cell-per-thread fold + update + adt_calc forms
   const int fvar = tuning("fold_variant", 0);
   if (sa && (!ua || !aa || (fvar != 0 && fvar != 4 && fvar != 5))) return false;
@@ -1574,12 +1578,13 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
       // per thread; 3 two cells at >= 3 CTAs per SM; 4 one cell per thread
       // at >= 4 (3 with adt_calc; FP64 3); 5 one cell per thread, the
       // cell's own streams fetched a cell ahead
-      T *qsave = sa ? (T *)sa[1].dat->data_d : nullptr;
+      T *qsave = sa ? (T *)(save_out ? save_out : sa[1].dat->data_d) : nullptr;
+      T *adt_to = aa ? (T *)adt_out : nullptr;
       auto launch = [&](auto kernel) {
         launch_pdl(kernel, grid_of((const void *)kernel), 256, 0, s, ncell,
                    (const int *)sp->d_ell, W, (const T *)vals,
                    qold, q, res, adt, N, xs[0], xs[1], xs[2], xs[3], K, seqbuf, rslot,
-                   red_ticket(), qsave);
+                   red_ticket(), qsave, adt_to);
       };
       const int fv = fvar;
       if (sa) {
@@ -1613,9 +1618,11 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
 }
 
 bool run_res_chain(char const *name, op_set rset, const op_arg *ra, op_set bset,
-                   const op_arg *ba, const op_arg *ua, const op_arg *aa, const op_arg *sa) {
-  return is_double(ra[0]) ? res_chain_t<double>(name, rset, ra, bset, ba, ua, aa, sa)
-                          : res_chain_t<float>(name, rset, ra, bset, ba, ua, aa, sa);
+                   const op_arg *ba, const op_arg *ua, const op_arg *aa, const op_arg *sa,
+                   void *adt_out, void *save_out) {
+  return is_double(ra[0])
+             ? res_chain_t<double>(name, rset, ra, bset, ba, ua, aa, sa, adt_out, save_out)
+             : res_chain_t<float>(name, rset, ra, bset, ba, ua, aa, sa, adt_out, save_out);
 }
 
 }  // namespace op2b

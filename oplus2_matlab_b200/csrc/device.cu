@@ -268,6 +268,7 @@ op_dat op_decl_dat_char(op_set set, int dim, char const *type, int size, char *d
 // declaration of the same name replaces the earlier one (jac2/jac.cpp:137-140).
 void op_decl_const_char(int dim, char const *type, int size, char *dat, char const *name) {
   flush_pending();
+  ahead_drop();  // values run ahead used the old constants
   if (dim <= 0 || size <= 0 || dat == nullptr) {
     fail(-1, "op_decl_const error -- invalid constant %s\n", name ? name : "(null)");
     return;
@@ -324,6 +325,7 @@ void op_exit(void) {
   release_jac_pairs();
   renumber_reset();
   checkpoint_reset();
+  ahead_reset();
   for (auto &m : R.maps) dev_free(m.d);
   R.maps.clear();
   for (int i = 0; i < OP_dat_index; i++) dev_free(OP_dat_list[i]->data_d);

@@ -23,6 +23,9 @@ struct Graph {
 };
 
 static bool g_prev_deferred = false;
+static int g_live_graphs = 0;
+
+int live_graphs() { return g_live_graphs; }
 
 }  // namespace op2b
 
@@ -37,6 +40,7 @@ int op2b_capture_begin(int profile) {
   if (error_pending()) return 0;
   Runtime &R = rt();
   flush_pending();  // loops held back before the capture run outside the graph
+  ahead_drop();     // a graph bakes dataset pointers: nothing may be swapped in later
   deliver_deferred();
   g_pending_mark = red_pending_count();
   R.capture_events.clear();
@@ -84,6 +88,7 @@ void *op2b_capture_end(void) {
     fail(-1, "op2b error: graph instantiation failed: %s\n", cudaGetErrorString(e));
     return nullptr;
   }
+  g_live_graphs++;
   return g;
 }
 
@@ -130,6 +135,7 @@ void op2b_graph_destroy(void *h) {
   if (g->exec) cudaGraphExecDestroy(g->exec);
   if (g->graph) cudaGraphDestroy(g->graph);
   delete g;
+  if (g_live_graphs > 0) g_live_graphs--;
 }
 
 }  // extern "C"

@@ -160,6 +160,13 @@ struct PhaseScope {
 int const_get_f32(char const *name, float *out, int n);
 int const_get_f64(char const *name, double *out, int n);
 
+// loops run ahead of their calls (loops.cpp): after an update whose result
+// must reach the caller, the next adt_calc (and save_soln) run in the
+// update's kernel into spare buffers, swapped in when the calls come
+void ahead_drop();   // discard what was run ahead (constants, capture, restore)
+void ahead_reset();  // op_exit: also free the spare buffers
+int live_graphs();   // captured graphs not yet destroyed (graph.cu)
+
 // renumbering of the sets for locality (renumber.cu)
 bool renumber_enabled();
 void renumber_apply();                 // first loop call: order the sets, move the data

@@ -220,6 +220,77 @@ bool res_holdable() {
   return effective_strategy("res_calc") == OP2B_STRATEGY_GATHER && tuning("gather_flux", 1);
 }
 
+// ---- loops run ahead of their calls --------------------------------------
+// An update whose reduction must reach the caller before its call returns
+// (reductions not deferred) cannot wait for the adt_calc the app calls next,
+// nor, at the end of an outer iteration, for the next save_soln.  The update's
+// per-cell pass computes them anyway, from the q it has just produced, into
+// spare device buffers of adt (and of save_soln's output); the datasets
+// themselves are left as they were.  When the expected call comes with the
+// same arguments (and the constants unchanged), its result is already
+// there: the dataset's device buffer and its spare swap, and no kernel runs.
+// Any other call drops what was run ahead.  The observable state -- every
+// dataset's device buffer between calls -- is the state without run-ahead.
+// Whether save_soln follows is predicted from the updates before: airfoil's
+// two updates per iteration alternate (adt_calc next, then save_soln next).
+// Not while a captured graph exists (graphs hold dataset pointers).
+struct Ahead {
+  bool adt = false, save = false;
+  std::vector<op_arg> adt_args, save_args;
+  unsigned consts_version = 0;
+};
+Ahead g_ahead;
+std::vector<op_arg> g_seen_adt, g_seen_save;  // the last adt_calc / save_soln calls
+unsigned g_save_after = 0;  // bit i: a save_soln came after the i-th latest update
+std::vector<void *> g_spare;  // per dataset index
+
+bool same_args(const std::vector<op_arg> &a, const op_arg *b) {
+  for (size_t i = 0; i < a.size(); i++)
+    if (a[i].argtype != b[i].argtype || a[i].dat != b[i].dat || a[i].map != b[i].map ||
+        a[i].idx != b[i].idx || a[i].acc != b[i].acc || a[i].dim != b[i].dim)
+      return false;
+  return true;
+}
+
+void *spare_of(op_dat d) {
+  if (g_spare.size() <= (size_t)d->index) g_spare.resize(d->index + 1, nullptr);
+  if (!g_spare[d->index]) g_spare[d->index] = dev_alloc((size_t)d->size * d->set->size);
+  return g_spare[d->index];
+}
+
+void swap_in(op_dat d) { std::swap(d->data_d, *reinterpret_cast<char **>(&g_spare[d->index])); }
+
+// res_calc, bres_calc, update whose rms is returned now: run the next
+// adt_calc (and save_soln) ahead; false when that does not apply
+bool run_chain_ahead(const std::vector<Held> &ch) {
+  if (!tuning("run_ahead", 1) || rt().gbl_deferred || live_graphs() > 0 ||
+      !tuning("gather_slots", 1))
+    return false;
+  const Held &u = ch[2];
+  const op_arg *ua = u.args.data();
+  if (g_seen_adt.size() != 6 || !adt_follows_update(ua, u.set, g_seen_adt[4].dat->set,
+                                                    g_seen_adt.data()))
+    return false;
+  // save_soln predicted from the update two before this one (bit 0 is this
+  // update, bit 1 the previous one)
+  const bool save = ((g_save_after >> 2) & 1) && g_seen_save.size() == 2 &&
+                    save_follows_update(ua, u.set, g_seen_save[0].dat->set, g_seen_save.data()) &&
+                    !dat_in(g_seen_save[1].dat, {g_seen_adt[0].dat, g_seen_adt[1].dat,
+                                                 g_seen_adt[2].dat, g_seen_adt[3].dat});
+  void *adt_out = spare_of(g_seen_adt[5].dat);
+  void *save_out = save ? spare_of(g_seen_save[1].dat) : nullptr;
+  if (error_pending()) return false;
+  if (!run_res_chain(nullptr, ch[0].set, ch[0].args.data(), ch[1].set, ch[1].args.data(), ua,
+                     g_seen_adt.data(), save ? g_seen_save.data() : nullptr, adt_out, save_out))
+    return false;
+  g_ahead.adt = true;
+  g_ahead.save = save;
+  g_ahead.adt_args = g_seen_adt;
+  g_ahead.save_args = g_seen_save;
+  g_ahead.consts_version = rt().consts_version;
+  return true;
+}
+
 // run a chain, fused as far as the kernels allow
 void run_chain(const std::vector<Held> &ch, const Held *adt) {
   if (ch.size() == 4) {  // res_calc, bres_calc, update, save_soln
@@ -231,6 +302,10 @@ void run_chain(const std::vector<Held> &ch, const Held *adt) {
     run_chain(std::vector<Held>(ch.begin(), ch.begin() + 3), nullptr);
     run_chain(std::vector<Held>{sv}, adt);
     return;
+  }
+  if (ch.size() == 3 && !adt && ch[2].kind == K_AUPDATE) {
+    g_save_after <<= 1;  // a new update: what follows it is not known yet
+    if (run_chain_ahead(ch)) return;
   }
   const Held &h0 = ch[0];
   const op_arg *a0 = h0.args.data();
@@ -338,6 +413,17 @@ bool holdable(Kind k) {
 }  // namespace
 
 namespace op2b {
+void ahead_drop() { g_ahead = Ahead(); }
+
+void ahead_reset() {
+  g_ahead = Ahead();
+  g_seen_adt.clear();
+  g_seen_save.clear();
+  g_save_after = 0;
+  for (void *p : g_spare) dev_free(p);
+  g_spare.clear();
+}
+
 void flush_pending() {
   if (g_chain.empty()) return;
   std::vector<Held> ch;
@@ -395,6 +481,25 @@ void par_loop_run(char const *name, op_set set, int nargs, const op_arg *args) {
          "(%d args)\n",
          name, nargs);
     return;
+  }
+  if (k == K_ADT) g_seen_adt.assign(args, args + nargs);
+  if (k == K_SAVE) {
+    g_seen_save.assign(args, args + nargs);
+    g_save_after |= 1;
+  }
+  if (g_ahead.adt || g_ahead.save) {  // the call run ahead: swap its result in
+    if (k == K_SAVE && g_ahead.save && same_args(g_ahead.save_args, args)) {
+      swap_in(args[1].dat);
+      g_ahead.save = false;
+      return;
+    }
+    if (k == K_ADT && g_ahead.adt && same_args(g_ahead.adt_args, args) &&
+        rt().consts_version == g_ahead.consts_version) {
+      swap_in(args[5].dat);
+      g_ahead = Ahead();
+      return;
+    }
+    g_ahead = Ahead();
   }
   if (!g_chain.empty()) {
     if (extend_chain(k, name, set, nargs, args)) return;

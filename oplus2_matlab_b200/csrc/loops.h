@@ -76,10 +76,13 @@ bool run_res_bres(op_set res_set, const op_arg *res_args, op_set bres_set,
 // does not suit slots (nothing has run).  save_args: save_soln between
 // update and adt_calc (the next outer iteration's first loops), storing the
 // new q to its output as well; needs update and adt_calc, else false.
-// name: the timer name, or nullptr for the joined loop names.
+// adt_out / save_out (device buffers of adt's and save_soln's output size,
+// or nullptr): adt_calc's and save_soln's values go there instead of into
+// their datasets.  name: the timer name, or nullptr for the joined loop names.
 bool run_res_chain(char const *name, op_set res_set, const op_arg *res_args, op_set bres_set,
                    const op_arg *bres_args, const op_arg *update_args, const op_arg *adt_args,
-                   const op_arg *save_args = nullptr);
+                   const op_arg *save_args = nullptr, void *adt_out = nullptr,
+                   void *save_out = nullptr);
 void release_fused_plans();
 
 }  // namespace op2b

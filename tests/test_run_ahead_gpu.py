@@ -1,0 +1,93 @@
+"""Loops run ahead of their calls.  With reductions returned at every call
+(the reference's semantics), an update cannot wait for the adt_calc that
+follows it, so its per-cell pass computes that adt_calc (and, at the end of
+an outer iteration, the next save_soln) into spare buffers, swapped in when
+the matching call comes.  Whatever the app calls instead, every dataset must
+read exactly as it would without run-ahead: each sequence below runs twice,
+with the "run_ahead" knob on and off, and every field is compared bit for
+bit at each fetch and at the end."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oplus2_matlab_b200 import _lib, api, apps
+from oplus2_matlab_b200 import mesh as M
+
+pytestmark = pytest.mark.gpu
+
+IT = ["save_soln"] + ["adt_calc", "res_calc", "bres_calc", "update"] * 2
+
+SEQUENCES = {
+    # the app's own order: adt_calc and save_soln are committed from run-ahead
+    "airfoil": IT * 4,
+    # a fetch of adt between the update and its adt_calc sees the old adt
+    "fetch_between": IT * 2 + ["adt_calc", "res_calc", "bres_calc", "update", "fetch",
+                               "adt_calc", "fetch"] + IT,
+    # the adt_calc never comes: res_calc reads the old adt
+    "skip_adt": IT + ["adt_calc", "res_calc", "bres_calc", "update", "res_calc", "bres_calc",
+                      "update"] + IT,
+    # save_soln comes, then not adt_calc
+    "save_then_other": IT * 2 + ["save_soln", "res_calc", "bres_calc", "update"] + IT,
+    # the constants change between the update and its adt_calc
+    "const_change": IT * 2 + ["cfl"] + ["adt_calc", "res_calc", "bres_calc", "update"] + IT,
+    # adt_calc twice, save_soln twice
+    "repeats": IT * 2 + ["save_soln", "save_soln", "adt_calc", "adt_calc"] + IT,
+}
+
+
+def run(op2, seq, ahead, dt):
+    lib = _lib.load()
+    lib.op2b_set_tuning(b"run_ahead", 1 if ahead else 0)
+    op2.set_strategy(op2.STRATEGY_GATHER)
+    op2.set_reduction(op2.REDUCE_TREE)
+    A = apps.Airfoil(M.naca0012(30, 45, scramble=True), dt)
+    snaps, rms = [], []
+    try:
+        for step in seq:
+            if step == "fetch":
+                snaps.append({k: v.copy() for k, v in A.fetch().items()})
+            elif step == "cfl":
+                api.op_decl_const("cfl", 1, A.tn, A.dtype.type(0.8))
+            else:
+                if step == "update":
+                    A.rms[0] = 0
+                A.loop(step)
+                if step == "update":
+                    rms.append(A.rms[0])
+        snaps.append({k: v.copy() for k, v in A.fetch().items()})
+    finally:
+        lib.op2b_set_tuning(b"run_ahead", 1)
+    assert op2.last_error() == ""
+    return snaps, np.array(rms)
+
+
+def loop_count(name):
+    cnt = C.c_int(0)
+    _lib.load().op2b_loop_time(name.encode(), C.byref(cnt))
+    return cnt.value
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("seq", sorted(SEQUENCES))
+def test_same_fields_with_and_without_run_ahead(op2, seq, dt):
+    with_ahead, rms_a = run(op2, SEQUENCES[seq], True, dt)
+    api.op_exit()
+    api.op_init([], 0)
+    without, rms_b = run(op2, SEQUENCES[seq], False, dt)
+    assert np.array_equal(rms_a, rms_b)
+    assert len(with_ahead) == len(without)
+    for a, b in zip(with_ahead, without):
+        for k in ("q", "qold", "adt", "res"):
+            assert np.array_equal(a[k], b[k]), (seq, k)
+
+
+def test_run_ahead_replaces_the_calls(op2):
+    """In the app's order, after the first iteration every adt_calc and
+    save_soln comes from the update before it: the fused launches run and
+    the separate kernels do not."""
+    run(op2, IT * 6, True, np.float32)
+    assert loop_count("res_calc+bres_calc+update+adt_calc") >= 6
+    assert loop_count("res_calc+bres_calc+update+save_soln+adt_calc") >= 4
+    assert loop_count("save_soln+adt_calc") <= 2
+    assert loop_count("adt_calc") <= 2
