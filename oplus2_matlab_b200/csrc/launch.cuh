@@ -52,12 +52,13 @@ inline void launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, 
 // resident at once for `kernel`: the size of one wave of a grid-stride
 // grid is that times the SM count.  Cached per kernel (the host-side query
 // costs microseconds; a loop call should not pay it each time).
-inline int resident_ctas(const void *kernel, int threads) {
+inline int resident_ctas(const void *kernel, int threads, size_t smem = 0) {
   static std::unordered_map<const void *, int> cache;
   auto it = cache.find(kernel);
   if (it != cache.end()) return it->second;
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0) != cudaSuccess || n < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess ||
+      n < 1)
     n = 1;
   cache.emplace(kernel, n);
   return n;
