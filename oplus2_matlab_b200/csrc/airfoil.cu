@@ -1457,35 +1457,133 @@ bool run_res_bres(op_set rset, const op_arg *ra, op_set bset, const op_arg *ba) 
                           : res_bres_t<float>(rset, ra, bset, ba);
 }
 
-// res_calc [+ bres_calc [+ update [+ adt_calc]]] over contribution lists:
-// the flux pass, then one per-cell pass that folds the cell's list and, when
-// update follows, applies it (and adt_calc) to the cell before storing
+// the flux pass of res_calc (and bres_calc's values when B.n > 0) into vals
 template <class T>
-static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op_set bset,
-                        const op_arg *ba, const op_arg *ua, const op_arg *aa, const op_arg *sa,
-                        void *adt_out, void *save_out) {
-  // save_soln rides on the one-cell-per-thread fold + update + adt_calc forms
-  const int fvar = tuning("fold_variant", 0);
-  if (sa && (!ua || !aa || (fvar != 0 && fvar != 4 && fvar != 5))) return false;
-  AirConsts<T> K = air_consts<T>();
-  if (error_pending()) return true;
-  cudaStream_t s = rt().stream;
+static void launch_flux(const op_arg *ra, const ResEdges<T> &E, const BresEdges<T> &B, T *vals,
+                        size_t nval, const AirConsts<T> &K, cudaStream_t s) {
+  const long long nflux = (long long)E.n + B.n;
+  // flux_ctas_per_sm = 0: one edge per thread (many short CTAs balance the
+  // SMs); n > 0: at most n CTAs per SM, grid-stride
+  const int per_sm = tuning("flux_ctas_per_sm", 16);
+  long long fg = (nflux + 255) / 256;
+  if (per_sm > 0) fg = std::min(fg, (long long)rt().num_sms * per_sm);
+  const unsigned fgrid = (unsigned)std::max(1LL, fg);
+  auto pair = [](const op_arg &a, const op_arg &b) {
+    return a.map && a.map == b.map && a.map->dim == 2 && a.idx == 0 && b.idx == 1;
+  };
+  const bool shape = pair(ra[0], ra[1]) && pair(ra[2], ra[3]) && pair(ra[4], ra[5]) &&
+                     ra[2].map == ra[4].map && ra[0].dat == ra[1].dat && ra[2].dat == ra[3].dat &&
+                     ra[4].dat == ra[5].dat && (long long)nval < (1LL << 30) &&
+                     (long long)ra[2].dat->set->size < (1LL << 30) &&
+                     (long long)ra[0].dat->set->size < (1LL << 30);
+  if (shape && tuning("flux_pair", 1))
+    launch_pdl(k_res_flux_pair<T>, fgrid, 256, 0, s, E.n,
+               reinterpret_cast<const int2 *>(map_dev(ra[0].map)),
+               reinterpret_cast<const int2 *>(map_dev(ra[2].map)), E.xa, E.qa, E.adta, B, vals, K);
+  else if (tuning("flux_pipe", 0))
+    launch_pdl(k_res_flux_list<T, true, sizeof(T) == 4 ? 6 : 3>, fgrid, 256, 0, s, E, B, vals, K);
+  else
+    launch_pdl(k_res_flux_list<T, false, sizeof(T) == 4 ? 8 : 4>, fgrid, 256, 0, s, E, B, vals, K);
+}
+
+// the plans and value buffer of a res_calc (+ bres_calc) chain; nullptr
+// when the mesh does not suit slots; *err when a plan failed
+template <class T>
+static SlotPlan *chain_plans(op_set rset, const op_arg *ra, op_set bset, const op_arg *ba,
+                             bool *err) {
+  *err = false;
   GatherPlan *g = get_gather_plan(rset, ra, {6, 7});
   GatherPlan *gb = ba ? get_gather_plan(bset, ba, {4}) : nullptr;
-  if (!g || (ba && !gb)) return true;
+  if (!g || (ba && !gb)) {
+    *err = true;
+    return nullptr;
+  }
   SlotPlan *sp = get_slot_plan(g, gb);
-  if (!sp) return false;
-  const int W = sp->width, ncell = sp->ntarget;
+  if (!sp) return nullptr;
   const size_t nval = (size_t)sp->na + sp->nb + 1;
   const size_t need = sizeof(T) * 4 * nval;
   if (sp->buf_bytes < need) {
     dev_free(sp->d_buf);
     sp->d_buf = dev_alloc(need);
     sp->buf_bytes = sp->d_buf ? need : 0;
-    if (!sp->d_buf) return true;
+    if (!sp->d_buf) {
+      *err = true;
+      return nullptr;
+    }
     // the padding entry, never written by the flux pass: -0.0
-    k_fill<T><<<1, 32, 0, s>>>((T *)sp->d_buf + 4 * (nval - 1), 4, T(-0.0));
+    k_fill<T><<<1, 32, 0, rt().stream>>>((T *)sp->d_buf + 4 * (nval - 1), 4, T(-0.0));
   }
+  return sp;
+}
+
+template <class T>
+static ResEdges<T> res_edges(op_set rset, const op_arg *ra) {
+  return ResEdges<T>{rset->size, idx_map(ra[0]), idx_map(ra[1]), idx_map(ra[2]), idx_map(ra[3]),
+                     idx_map(ra[4]), idx_map(ra[5]), (const T *)ra[0].dat->data_d,
+                     (const T *)ra[1].dat->data_d, (const T *)ra[2].dat->data_d,
+                     (const T *)ra[3].dat->data_d, (const T *)ra[4].dat->data_d,
+                     (const T *)ra[5].dat->data_d};
+}
+
+template <class T>
+static BresEdges<T> bres_edges(op_set bset, const op_arg *ba) {
+  BresEdges<T> B;
+  memset(&B, 0, sizeof B);
+  if (ba)
+    B = BresEdges<T>{bset->size, idx_map(ba[0]), idx_map(ba[1]), idx_map(ba[2]),
+                     idx_map(ba[3]), idx_map(ba[5]), (const T *)ba[0].dat->data_d,
+                     (const T *)ba[1].dat->data_d, (const T *)ba[2].dat->data_d,
+                     (const T *)ba[3].dat->data_d, (const int *)ba[5].dat->data_d};
+  return B;
+}
+
+// The flux pass of a res_calc + bres_calc chain that has not been called
+// yet, with adt read from adt_now (a spare buffer about to become adt's):
+// the values the chain's per-cell pass will fold, if the calls come as
+// expected (the caller checks that before skipping its own flux pass)
+template <class T>
+static bool res_flux_ahead_t(op_set rset, const op_arg *ra, op_set bset, const op_arg *ba,
+                             op_dat adt, const void *adt_now) {
+  AirConsts<T> K = air_consts<T>();
+  if (error_pending()) return false;
+  bool err = false;
+  SlotPlan *sp = chain_plans<T>(rset, ra, bset, ba, &err);
+  if (!sp || err) return false;
+  ResEdges<T> E = res_edges<T>(rset, ra);
+  BresEdges<T> B = bres_edges<T>(bset, ba);
+  if (ra[4].dat == adt) E.adta = (const T *)adt_now;
+  if (ra[5].dat == adt) E.adtb = (const T *)adt_now;
+  if (ba && ba[3].dat == adt) B.adt = (const T *)adt_now;
+  launch_flux<T>(ra, E, B, (T *)sp->d_buf, (size_t)sp->na + sp->nb + 1, K, rt().stream);
+  return true;
+}
+
+bool run_res_flux_ahead(op_set rset, const op_arg *ra, op_set bset, const op_arg *ba, op_dat adt,
+                        const void *adt_now) {
+  return is_double(ra[0]) ? res_flux_ahead_t<double>(rset, ra, bset, ba, adt, adt_now)
+                          : res_flux_ahead_t<float>(rset, ra, bset, ba, adt, adt_now);
+}
+
+// res_calc [+ bres_calc [+ update [+ adt_calc]]] over contribution lists:
+// the flux pass, then one per-cell pass that folds the cell's list and, when
+// update follows, applies it (and adt_calc) to the cell before storing
+template <class T>
+static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op_set bset,
+                        const op_arg *ba, const op_arg *ua, const op_arg *aa, const op_arg *sa,
+                        void *adt_out, void *save_out, bool flux_done,
+                        std::vector<GblRequest> *held) {
+  // save_soln rides on the one-cell-per-thread fold + update + adt_calc forms
+  const int fvar = tuning("fold_variant", 0);
+  if (sa && (!ua || !aa || (fvar != 0 && fvar != 4 && fvar != 5))) return false;
+  AirConsts<T> K = air_consts<T>();
+  if (error_pending()) return true;
+  cudaStream_t s = rt().stream;
+  bool err = false;
+  SlotPlan *sp = chain_plans<T>(rset, ra, bset, ba, &err);
+  if (err) return true;
+  if (!sp) return false;
+  const int W = sp->width, ncell = sp->ntarget;
+  const size_t nval = (size_t)sp->na + sp->nb + 1;
   T *vals = (T *)sp->d_buf;
 
   std::string name = loop_name ? loop_name : "res_calc";
@@ -1498,47 +1596,11 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
   int rslot_id = ua ? red_new_slot() : -1;
   {
     LoopScope ls(name.c_str(), bytes, 0);
-    ResEdges<T> E{rset->size, idx_map(ra[0]), idx_map(ra[1]), idx_map(ra[2]), idx_map(ra[3]),
-                  idx_map(ra[4]), idx_map(ra[5]), (const T *)ra[0].dat->data_d,
-                  (const T *)ra[1].dat->data_d, (const T *)ra[2].dat->data_d,
-                  (const T *)ra[3].dat->data_d, (const T *)ra[4].dat->data_d,
-                  (const T *)ra[5].dat->data_d};
-    BresEdges<T> B;
-    memset(&B, 0, sizeof B);
-    if (ba)
-      B = BresEdges<T>{bset->size, idx_map(ba[0]), idx_map(ba[1]), idx_map(ba[2]),
-                       idx_map(ba[3]), idx_map(ba[5]), (const T *)ba[0].dat->data_d,
-                       (const T *)ba[1].dat->data_d, (const T *)ba[2].dat->data_d,
-                       (const T *)ba[3].dat->data_d, (const int *)ba[5].dat->data_d};
-    const long long nflux = (long long)E.n + B.n;
-    {
+    ResEdges<T> E = res_edges<T>(rset, ra);
+    BresEdges<T> B = bres_edges<T>(bset, ba);
+    if (!flux_done) {
       PhaseScope ph(name + ":flux");
-      // flux_ctas_per_sm = 0: one edge per thread (many short CTAs balance
-      // the SMs); n > 0: at most n CTAs per SM, grid-stride
-      const int per_sm = tuning("flux_ctas_per_sm", 16);
-      long long fg = (nflux + 255) / 256;
-      if (per_sm > 0) fg = std::min(fg, (long long)rt().num_sms * per_sm);
-      const unsigned fgrid = (unsigned)std::max(1LL, fg);
-      auto pair = [](const op_arg &a, const op_arg &b) {
-        return a.map && a.map == b.map && a.map->dim == 2 && a.idx == 0 && b.idx == 1;
-      };
-      const bool shape = pair(ra[0], ra[1]) && pair(ra[2], ra[3]) && pair(ra[4], ra[5]) &&
-                         ra[2].map == ra[4].map && ra[0].dat == ra[1].dat &&
-                         ra[2].dat == ra[3].dat && ra[4].dat == ra[5].dat &&
-                         (long long)nval < (1LL << 30) &&
-                         (long long)ra[2].dat->set->size < (1LL << 30) &&
-                         (long long)ra[0].dat->set->size < (1LL << 30);
-      if (shape && tuning("flux_pair", 1))
-        launch_pdl(k_res_flux_pair<T>, fgrid, 256, 0, s, E.n,
-                   reinterpret_cast<const int2 *>(map_dev(ra[0].map)),
-                   reinterpret_cast<const int2 *>(map_dev(ra[2].map)), E.xa, E.qa, E.adta, B,
-                   vals, K);
-      else if (tuning("flux_pipe", 0))
-        launch_pdl(k_res_flux_list<T, true, sizeof(T) == 4 ? 6 : 3>, fgrid, 256, 0, s, E, B, vals,
-                   K);
-      else
-        launch_pdl(k_res_flux_list<T, false, sizeof(T) == 4 ? 8 : 4>, fgrid, 256, 0, s, E, B,
-                   vals, K);
+      launch_flux<T>(ra, E, B, vals, nval, K, s);
     }
     PhaseScope ph(name + ":fold");
     T *res = (T *)ra[6].dat->data_d;
@@ -1612,17 +1674,22 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
       }
     }
   }
-  if (ua)
-    red_finish({GblRequest{ua[4].data, rslot_id, OP_INC, sizeof(T) == 8 ? GBL_F64 : GBL_F32, seq}});
+  if (ua) {
+    GblRequest rq{ua[4].data, rslot_id, OP_INC, sizeof(T) == 8 ? GBL_F64 : GBL_F32, seq};
+    if (held) held->push_back(rq);  // the caller delivers it
+    else red_finish({rq});
+  }
   return true;
 }
 
 bool run_res_chain(char const *name, op_set rset, const op_arg *ra, op_set bset,
                    const op_arg *ba, const op_arg *ua, const op_arg *aa, const op_arg *sa,
-                   void *adt_out, void *save_out) {
-  return is_double(ra[0])
-             ? res_chain_t<double>(name, rset, ra, bset, ba, ua, aa, sa, adt_out, save_out)
-             : res_chain_t<float>(name, rset, ra, bset, ba, ua, aa, sa, adt_out, save_out);
+                   void *adt_out, void *save_out, bool flux_done,
+                   std::vector<GblRequest> *held) {
+  return is_double(ra[0]) ? res_chain_t<double>(name, rset, ra, bset, ba, ua, aa, sa, adt_out,
+                                                save_out, flux_done, held)
+                          : res_chain_t<float>(name, rset, ra, bset, ba, ua, aa, sa, adt_out,
+                                               save_out, flux_done, held);
 }
 
 }  // namespace op2b

@@ -137,6 +137,18 @@ void red_finish(const std::vector<GblRequest> &reqs) {
   if (pending().empty() && rs().graph_slots == 0) rs().next_slot = 0;
 }
 
+void red_finish_after(cudaEvent_t done, const std::vector<GblRequest> &reqs) {
+  if (reqs.empty()) return;
+  RedState &S = rs();
+  OP2B_CUDA(cudaEventSynchronize(done));  // the slots are host memory
+  for (auto &r : reqs) {
+    const char *p = S.host + (size_t)r.slot * 8;
+    if (r.type == GBL_F64) combine<double>(r.host, *(const double *)p, r.acc, r.assign);
+    else combine<float>(r.host, *(const float *)p, r.acc, r.assign);
+  }
+  if (pending().empty() && S.graph_slots == 0) S.next_slot = 0;
+}
+
 size_t red_pending_count() { return pending().size(); }
 
 std::vector<GblRequest> red_take_pending_since(size_t mark) {

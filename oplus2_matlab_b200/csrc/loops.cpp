@@ -168,6 +168,7 @@ struct Held {
   std::string name;
   op_set set = nullptr;
   std::vector<op_arg> args;
+  bool flux_done = false;  // res_calc: its flux pass already ran (run ahead)
 };
 std::vector<Held> g_chain;
 
@@ -241,6 +242,24 @@ struct Ahead {
 };
 Ahead g_ahead;
 std::vector<op_arg> g_seen_adt, g_seen_save;  // the last adt_calc / save_soln calls
+// The next res_calc + bres_calc's flux pass runs ahead too, queued behind
+// the update's per-cell pass: it reads q as the update leaves it and adt from
+// the spare buffer the update has just filled, so it is valid once that
+// adt_calc is committed and the res_calc and bres_calc calls repeat the last
+// ones.  The update's reduction is waited for on an event before it, so the
+// flux pass runs while the host returns the rms and takes the next calls.
+std::vector<op_arg> g_seen_res, g_seen_bres;  // the last res_calc / bres_calc calls
+op_set g_seen_res_set = nullptr, g_seen_bres_set = nullptr;
+struct NextFlux {
+  bool valid = false, adt_committed = false;
+  std::vector<op_arg> res_args, bres_args;
+  op_set res_set = nullptr, bres_set = nullptr;
+  unsigned consts_version = 0;
+};
+NextFlux g_next;
+std::vector<op_arg> g_expect_bres;  // after a res_calc whose flux ran ahead
+op_set g_expect_bres_set = nullptr;
+cudaEvent_t g_fold_done = nullptr;
 unsigned g_save_after = 0;  // bit i: a save_soln came after the i-th latest update
 std::vector<void *> g_spare;  // per dataset index
 
@@ -280,14 +299,38 @@ bool run_chain_ahead(const std::vector<Held> &ch) {
   void *adt_out = spare_of(g_seen_adt[5].dat);
   void *save_out = save ? spare_of(g_seen_save[1].dat) : nullptr;
   if (error_pending()) return false;
+  std::vector<GblRequest> held;
   if (!run_res_chain(nullptr, ch[0].set, ch[0].args.data(), ch[1].set, ch[1].args.data(), ua,
-                     g_seen_adt.data(), save ? g_seen_save.data() : nullptr, adt_out, save_out))
+                     g_seen_adt.data(), save ? g_seen_save.data() : nullptr, adt_out, save_out,
+                     ch[0].flux_done, &held))
     return false;
   g_ahead.adt = true;
   g_ahead.save = save;
   g_ahead.adt_args = g_seen_adt;
   g_ahead.save_args = g_seen_save;
   g_ahead.consts_version = rt().consts_version;
+  // the next chain's flux pass, behind an event that marks this update done
+  const bool next = tuning("flux_ahead", 1) && g_seen_res.size() == 8 &&
+                    g_seen_bres.size() == 6 && g_seen_res[2].dat == ua[1].dat &&
+                    g_seen_res[3].dat == ua[1].dat && g_seen_res[4].dat == ua[3].dat &&
+                    g_seen_res[5].dat == ua[3].dat && g_seen_res[6].dat == ua[2].dat &&
+                    bres_follows_res(g_seen_res.data(), g_seen_bres.data()) &&
+                    g_seen_adt[5].dat == ua[3].dat;
+  if (!next) {
+    red_finish(held);
+    return true;
+  }
+  if (!g_fold_done) OP2B_CUDA(cudaEventCreateWithFlags(&g_fold_done, cudaEventDisableTiming));
+  OP2B_CUDA(cudaEventRecord(g_fold_done, rt().stream));
+  g_next = NextFlux();
+  g_next.valid = run_res_flux_ahead(g_seen_res_set, g_seen_res.data(), g_seen_bres_set,
+                                    g_seen_bres.data(), ua[3].dat, adt_out);
+  g_next.res_args = g_seen_res;
+  g_next.bres_args = g_seen_bres;
+  g_next.res_set = g_seen_res_set;
+  g_next.bres_set = g_seen_bres_set;
+  g_next.consts_version = rt().consts_version;
+  red_finish_after(g_fold_done, held);
   return true;
 }
 
@@ -318,7 +361,8 @@ void run_chain(const std::vector<Held> &ch, const Held *adt) {
     const Held *u = ch.size() > 2 ? &ch[2] : nullptr;
     if (u && tuning("gather_slots", 1) &&
         run_res_chain(nullptr, h0.set, a0, h1.set, h1.args.data(), u->args.data(),
-                      adt ? adt->args.data() : nullptr))
+                      adt ? adt->args.data() : nullptr, nullptr, nullptr, nullptr,
+                      h0.flux_done && h1.kind == K_BRES))
       return;
     if (!run_res_bres(h0.set, a0, h1.set, h1.args.data())) {
       run_kind(h0.kind, 0, h0.name.c_str(), h0.set, a0);
@@ -413,12 +457,20 @@ bool holdable(Kind k) {
 }  // namespace
 
 namespace op2b {
-void ahead_drop() { g_ahead = Ahead(); }
+void ahead_drop() {
+  g_ahead = Ahead();
+  g_next = NextFlux();
+  for (Held &h : g_chain) h.flux_done = false;
+}
 
 void ahead_reset() {
-  g_ahead = Ahead();
+  ahead_drop();
   g_seen_adt.clear();
   g_seen_save.clear();
+  g_seen_res.clear();
+  g_seen_bres.clear();
+  g_expect_bres.clear();
+  g_seen_res_set = g_seen_bres_set = g_expect_bres_set = nullptr;
   g_save_after = 0;
   for (void *p : g_spare) dev_free(p);
   g_spare.clear();
@@ -487,6 +539,14 @@ void par_loop_run(char const *name, op_set set, int nargs, const op_arg *args) {
     g_seen_save.assign(args, args + nargs);
     g_save_after |= 1;
   }
+  if (k == K_RES) {
+    g_seen_res.assign(args, args + nargs);
+    g_seen_res_set = set;
+  }
+  if (k == K_BRES) {
+    g_seen_bres.assign(args, args + nargs);
+    g_seen_bres_set = set;
+  }
   if (g_ahead.adt || g_ahead.save) {  // the call run ahead: swap its result in
     if (k == K_SAVE && g_ahead.save && same_args(g_ahead.save_args, args)) {
       swap_in(args[1].dat);
@@ -497,16 +557,34 @@ void par_loop_run(char const *name, op_set set, int nargs, const op_arg *args) {
         rt().consts_version == g_ahead.consts_version) {
       swap_in(args[5].dat);
       g_ahead = Ahead();
+      g_next.adt_committed = true;
       return;
     }
     g_ahead = Ahead();
+    g_next = NextFlux();
   }
+  // the flux pass run ahead counts for this res_calc only if everything
+  // since matched; a bres_calc other than the expected one undoes it
+  bool res_flux_done = false;
+  if (k == K_RES) {
+    res_flux_done = g_next.valid && g_next.adt_committed && g_chain.empty() &&
+                    set == g_next.res_set && same_args(g_next.res_args, args) &&
+                    rt().consts_version == g_next.consts_version;
+    g_expect_bres = g_next.bres_args;
+    g_expect_bres_set = g_next.bres_set;
+  }
+  g_next = NextFlux();
+  if (k == K_BRES && !g_chain.empty() && g_chain[0].kind == K_RES && g_chain[0].flux_done &&
+      !(g_chain.size() == 1 && set == g_expect_bres_set && g_expect_bres.size() == 6 &&
+        same_args(g_expect_bres, args)))
+    g_chain[0].flux_done = false;
   if (!g_chain.empty()) {
     if (extend_chain(k, name, set, nargs, args)) return;
     flush_pending();
   }
   if (holdable(k)) {
     g_chain.push_back(make_held(k, name, set, nargs, args));
+    if (k == K_RES) g_chain.back().flux_done = res_flux_done;
     return;
   }
   run_kind(k, v, name, set, args);

@@ -48,6 +48,8 @@ void *red_slot_ptr(int slot);    // 8-byte device slot
 int red_new_slot();
 void *red_seq_buffer(size_t bytes);  // scratch for SEQ-mode contributions
 void red_finish(const std::vector<GblRequest> &reqs);
+// the same, waiting only for the work up to the event (not deferred mode)
+void red_finish_after(cudaEvent_t done, const std::vector<GblRequest> &reqs);
 // deferred requests (graph capture): count, take those added since a mark,
 // and re-arm a set (replacing any pending request on the same slots)
 size_t red_pending_count();
@@ -79,10 +81,18 @@ bool run_res_bres(op_set res_set, const op_arg *res_args, op_set bres_set,
 // adt_out / save_out (device buffers of adt's and save_soln's output size,
 // or nullptr): adt_calc's and save_soln's values go there instead of into
 // their datasets.  name: the timer name, or nullptr for the joined loop names.
+// flux_done: the flux pass already ran for exactly these arguments (run
+// ahead, run_res_flux_ahead).  held: the update's reduction is appended
+// there for the caller to deliver, instead of being delivered here.
 bool run_res_chain(char const *name, op_set res_set, const op_arg *res_args, op_set bres_set,
                    const op_arg *bres_args, const op_arg *update_args, const op_arg *adt_args,
                    const op_arg *save_args = nullptr, void *adt_out = nullptr,
-                   void *save_out = nullptr);
+                   void *save_out = nullptr, bool flux_done = false,
+                   std::vector<GblRequest> *held = nullptr);
+// the flux pass of a res_calc + bres_calc chain before its calls, adt read
+// from adt_now instead of adt's buffer; false when not applicable
+bool run_res_flux_ahead(op_set res_set, const op_arg *res_args, op_set bres_set,
+                        const op_arg *bres_args, op_dat adt, const void *adt_now);
 void release_fused_plans();
 
 }  // namespace op2b

@@ -2,7 +2,8 @@
 (the reference's semantics), an update cannot wait for the adt_calc that
 follows it, so its per-cell pass computes that adt_calc (and, at the end of
 an outer iteration, the next save_soln) into spare buffers, swapped in when
-the matching call comes.  Whatever the app calls instead, every dataset must
+the matching call comes; the next res_calc + bres_calc's flux pass is
+queued behind it.  Whatever the app calls instead, every dataset must
 read exactly as it would without run-ahead: each sequence below runs twice,
 with the "run_ahead" knob on and off, and every field is compared bit for
 bit at each fetch and at the end."""
@@ -33,6 +34,11 @@ SEQUENCES = {
     "const_change": IT * 2 + ["cfl"] + ["adt_calc", "res_calc", "bres_calc", "update"] + IT,
     # adt_calc twice, save_soln twice
     "repeats": IT * 2 + ["save_soln", "save_soln", "adt_calc", "adt_calc"] + IT,
+    # the next res_calc's flux pass also runs ahead: res_calc called twice,
+    # bres_calc skipped, a fetch between res_calc and bres_calc
+    "res_twice": IT * 2 + ["adt_calc", "res_calc", "res_calc", "bres_calc", "update"] + IT,
+    "bres_skipped": IT * 2 + ["adt_calc", "res_calc", "update"] + IT,
+    "fetch_in_chain": IT * 2 + ["adt_calc", "res_calc", "fetch", "bres_calc", "update"] + IT,
 }
 
 
