@@ -102,19 +102,22 @@ def parse():
 
 class Dist:
     """One process per GPU under torchrun; torch.distributed only for the
-    barrier and the max over ranks."""
+    barrier and the max over ranks.  OP2B_DIST_BACKEND=gloo runs the same
+    plumbing on host tensors (the CPU tests use it)."""
 
     def __init__(self):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = os.environ.get("OP2B_DIST_BACKEND", "nccl")
         self.dist = None
         if self.world > 1:
             import datetime
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            if self.backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(self.backend, timeout=datetime.timedelta(seconds=120))
             self.torch, self.dist = torch, dist
 
     def barrier(self):
@@ -124,7 +127,7 @@ class Dist:
     def max(self, v):
         if not self.dist:
             return v
-        t = self.torch.tensor([float(v)], device="cuda")
+        t = self.torch.tensor([float(v)], device="cuda" if self.backend == "nccl" else "cpu")
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 

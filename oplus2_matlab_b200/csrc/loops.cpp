@@ -277,7 +277,12 @@ void *spare_of(op_dat d) {
   return g_spare[d->index];
 }
 
-void swap_in(op_dat d) { std::swap(d->data_d, *reinterpret_cast<char **>(&g_spare[d->index])); }
+// the spare buffer becomes the dataset's, the dataset's old buffer the spare
+void swap_in(op_dat d) {
+  void *old = d->data_d;
+  d->data_d = static_cast<char *>(g_spare[d->index]);
+  g_spare[d->index] = old;
+}
 
 // res_calc, bres_calc, update whose rms is returned now: run the next
 // adt_calc (and save_soln) ahead; false when that does not apply
