@@ -45,13 +45,15 @@ __device__ __forceinline__ float jac_inc(float du, float beta, typename JacLayou
   return (float)((double)du + (double)beta * (double)a * (double)u);
 }
 
-// res, GATHER: one thread per node with incoming contributions
+// res, GATHER: one thread per node with incoming contributions; du_out is du
+// itself, or a spare buffer when the loop runs ahead of its call
 template <int V>
 __global__ void k_jac_res_gather(int nrows, const int *__restrict__ active,
                                  const int *__restrict__ row, const int *__restrict__ keys,
                                  IdxMap mA, IdxMap mu,
                                  const typename JacLayout<V>::AT *__restrict__ A,
-                                 const float *__restrict__ u, float *__restrict__ du, float beta) {
+                                 const float *__restrict__ u, const float *du, float beta,
+                                 float *du_out) {
   typedef JacLayout<V> L;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   int n = 0, k0 = 0, k1 = 0;
@@ -70,7 +72,7 @@ __global__ void k_jac_res_gather(int nrows, const int *__restrict__ active,
     float uu = __ldg(u + (size_t)jat(mu, e) * L::U);
     d = jac_inc<V>(d, beta, a, uu);
   }
-  du[(size_t)n * L::DU] = d;
+  du_out[(size_t)n * L::DU] = d;
 }
 
 // res, GATHER over precomputed (edge, u element) pairs per contribution:
@@ -79,7 +81,8 @@ template <int V>
 __global__ void k_jac_res_pairs(int nrows, const int *__restrict__ active,
                                 const int *__restrict__ row, const int2 *__restrict__ pairs,
                                 const typename JacLayout<V>::AT *__restrict__ A,
-                                const float *__restrict__ u, float *__restrict__ du, float beta) {
+                                const float *__restrict__ u, const float *du, float beta,
+                                float *du_out) {
   typedef JacLayout<V> L;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   int n = 0, k0 = 0, k1 = 0;
@@ -98,7 +101,7 @@ __global__ void k_jac_res_pairs(int nrows, const int *__restrict__ active,
     float uu = __ldg(u + (size_t)p.y * L::U);
     d = jac_inc<V>(d, beta, a, uu);
   }
-  du[(size_t)n * L::DU] = d;
+  du_out[(size_t)n * L::DU] = d;
 }
 
 // pairs[k] = (A element, u element) of gather key k (slot 0 of the group)
@@ -215,14 +218,17 @@ void release_jac_pairs() {
   g_jac_pairs.clear();
 }
 
+// du_out: nullptr (in place) or a spare buffer of du's size, written for
+// every node (the loop run ahead: GATHER only, every node a target)
 template <int V>
-static void jac_res_t(char const *name, op_set set, const op_arg *args) {
+static bool jac_res_t(char const *name, op_set set, const op_arg *args, float *du_out) {
   typedef JacLayout<V> L;
   cudaStream_t s = rt().stream;
   const float beta = *(const float *)args[3].data;  // gbl OP_READ, passed by value
+  if (du_out && (V != 1 || effective_strategy(name) == OP2B_STRATEGY_COLOURED)) return false;
   if (effective_strategy(name) == OP2B_STRATEGY_COLOURED) {
     DevPlan *p = get_plan(name, set, OP_part_size, 4, args, 2, kJacResInds);
-    if (!p) return;
+    if (!p) return false;
     LoopScope ls(name, p->transfer, p->transfer2);
     JacPlanView v;
     v.blkmap = p->d_blkmap; v.offset = p->d_offset; v.nelems = p->d_nelems;
@@ -238,33 +244,43 @@ static void jac_res_t(char const *name, op_set set, const op_arg *args) {
         k_jac_res_coloured<V><<<p->ncolblk[c], nthread, p->nshared, s>>>(
             v, off, idx_map(args[0]), (const typename L::AT *)args[0].dat->data_d,
             (const float *)args[1].dat->data_d, (float *)args[2].dat->data_d, beta);
-    return;
+    return true;
   }
   GatherPlan *g = get_gather_plan(set, args, {2});
-  if (!g) return;
+  if (!g) return false;
+  if (du_out && g->nactive != args[2].dat->set->size) return false;
   LoopScope ls(name, compulsory_bytes(set, 4, args), 0);
-  if (g->nactive == 0) return;
+  if (g->nactive == 0) return true;
+  float *du = (float *)args[2].dat->data_d;
+  float *dst = du_out ? du_out : du;
   // (edge, u element) per contribution, built once per plan and map pair
   int2 *pairs = jac_pairs(g, args, s);
   if (pairs)
     launch_pdl(k_jac_res_pairs<V>, (unsigned)((g->nactive + 255) / 256), 256, 0, s, g->nactive,
                (const int *)g->d_active, (const int *)g->d_row, (const int2 *)pairs,
                (const typename L::AT *)args[0].dat->data_d, (const float *)args[1].dat->data_d,
-               (float *)args[2].dat->data_d, beta);
+               (const float *)du, beta, dst);
   else
     launch_pdl(k_jac_res_gather<V>, (unsigned)((g->nactive + 255) / 256), 256, 0, s, g->nactive,
                (const int *)g->d_active, (const int *)g->d_row, (const int *)g->d_keys,
                idx_map(args[0]), idx_map(args[1]), (const typename L::AT *)args[0].dat->data_d,
-               (const float *)args[1].dat->data_d, (float *)args[2].dat->data_d, beta);
+               (const float *)args[1].dat->data_d, (const float *)du, beta, dst);
+  return true;
 }
 
 void run_jac_res(char const *name, op_set set, const op_arg *args, int variant) {
-  if (variant == 2) jac_res_t<2>(name, set, args);
-  else jac_res_t<1>(name, set, args);
+  if (variant == 2) jac_res_t<2>(name, set, args, nullptr);
+  else jac_res_t<1>(name, set, args, nullptr);
+}
+
+bool run_jac_res_ahead(char const *name, op_set set, const op_arg *args, int variant,
+                       void *du_out) {
+  return variant == 1 && jac_res_t<1>(name, set, args, (float *)du_out);
 }
 
 template <int V>
-static void jac_update_t(char const *name, op_set set, const op_arg *args) {
+static void jac_update_t(char const *name, op_set set, const op_arg *args,
+                         std::vector<GblRequest> *held) {
   cudaStream_t s = rt().stream;
   float alpha = 0.f;
   if (const_get_f32("alpha", &alpha, 1) < 1) {
@@ -285,13 +301,16 @@ static void jac_update_t(char const *name, op_set set, const op_arg *args) {
                red_ticket());
     if (seq) k_seq_sum<float><<<1, 32, 0, s>>>(seqbuf, n, *(const float *)args[3].data, r_sum);
   }
-  red_finish({GblRequest{args[3].data, slot_sum, OP_INC, GBL_F32, seq},
-              GblRequest{args[4].data, slot_max, OP_MAX, GBL_F32, false}});
+  std::vector<GblRequest> rq{GblRequest{args[3].data, slot_sum, OP_INC, GBL_F32, seq},
+                             GblRequest{args[4].data, slot_max, OP_MAX, GBL_F32, false}};
+  if (held) held->insert(held->end(), rq.begin(), rq.end());  // the caller delivers them
+  else red_finish(rq);
 }
 
-void run_jac_update(char const *name, op_set set, const op_arg *args, int variant) {
-  if (variant == 2) jac_update_t<2>(name, set, args);
-  else jac_update_t<1>(name, set, args);
+void run_jac_update(char const *name, op_set set, const op_arg *args, int variant,
+                    std::vector<GblRequest> *held) {
+  if (variant == 2) jac_update_t<2>(name, set, args, held);
+  else jac_update_t<1>(name, set, args, held);
 }
 
 }  // namespace op2b

@@ -66,7 +66,13 @@ void run_res_calc(char const *name, op_set set, const op_arg *args);
 void run_bres_calc(char const *name, op_set set, const op_arg *args);
 void run_airfoil_update(char const *name, op_set set, const op_arg *args);
 void run_jac_res(char const *name, op_set set, const op_arg *args, int variant);
-void run_jac_update(char const *name, op_set set, const op_arg *args, int variant);
+// held: the reductions are appended there for the caller to deliver
+void run_jac_update(char const *name, op_set set, const op_arg *args, int variant,
+                    std::vector<GblRequest> *held = nullptr);
+// jac1's res into du_out (a spare buffer of du's size) instead of du, ahead
+// of its call; false when not applicable (nothing launched)
+bool run_jac_res_ahead(char const *name, op_set set, const op_arg *args, int variant,
+                       void *du_out);
 
 // fused loop pairs (airfoil.cu); false = not applicable, run them separately
 bool run_save_adt(op_set set, const op_arg *save_args, const op_arg *adt_args);

@@ -97,3 +97,60 @@ def test_run_ahead_replaces_the_calls(op2):
     assert loop_count("res_calc+bres_calc+update+save_soln+adt_calc") >= 4
     assert loop_count("save_soln+adt_calc") <= 2
     assert loop_count("adt_calc") <= 2
+
+
+JAC_SEQUENCES = {
+    "plain": ["iter"] * 12,
+    # a fetch between update and res, then beta changed before a res
+    "fetch_and_beta": ["iter"] * 4 + ["update", "fetch", "res", "update", "beta", "res",
+                                      "update"] + ["iter"] * 3,
+    # update twice, res twice
+    "repeats": ["iter"] * 3 + ["update", "update", "res", "res", "update"] + ["iter"] * 2,
+}
+
+
+def run_jac(op2, seq, ahead, variant):
+    lib = _lib.load()
+    lib.op2b_set_tuning(b"run_ahead", 1 if ahead else 0)
+    op2.set_strategy(op2.STRATEGY_GATHER)
+    op2.set_reduction(op2.REDUCE_TREE)
+    J = apps.Jac(M.jac(40, variant), variant)
+    out, snaps = [], []
+
+    def update():
+        J.u_sum[0] = 0
+        J.u_max[0] = 0
+        api.op_par_loop("update", J.nodes, *J.upd_args)
+        out.append((float(J.u_sum[0]), float(J.u_max[0])))
+    try:
+        for step in seq:
+            if step == "iter":
+                api.op_par_loop("res", J.edges, *J.res_args)
+                update()
+            elif step == "res":
+                api.op_par_loop("res", J.edges, *J.res_args)
+            elif step == "update":
+                update()
+            elif step == "beta":
+                J.beta[0] = np.float32(0.75)
+            elif step == "fetch":
+                api.op_fetch_data(J.p_du)
+                snaps.append((J.fetch().copy(), J.du.copy()))
+        api.op_fetch_data(J.p_du)
+        snaps.append((J.fetch().copy(), J.du.copy()))
+    finally:
+        lib.op2b_set_tuning(b"run_ahead", 1)
+    assert op2.last_error() == ""
+    return out, snaps
+
+
+@pytest.mark.parametrize("variant", [1, 2])
+@pytest.mark.parametrize("seq", sorted(JAC_SEQUENCES))
+def test_jac_same_results_with_and_without_run_ahead(op2, seq, variant):
+    a_out, a_snaps = run_jac(op2, JAC_SEQUENCES[seq], True, variant)
+    api.op_exit()
+    api.op_init([], 0)
+    b_out, b_snaps = run_jac(op2, JAC_SEQUENCES[seq], False, variant)
+    assert a_out == b_out
+    for (ua, dua), (ub, dub) in zip(a_snaps, b_snaps):
+        assert np.array_equal(ua, ub) and np.array_equal(dua, dub)
