@@ -56,13 +56,16 @@ class Server:
     """Admit, iterate and retire solves on one GPU."""
 
     def __init__(self, dtype=np.float32, budget_bytes=150 * 10**9, iters_per_step=10,
-                 keep_q=False, clock=time.perf_counter, max_active=0, policy="fifo"):
+                 keep_q=False, clock=time.perf_counter, max_active=0, policy="fifo",
+                 group=None):
         """max_active > 0 caps the solves iterated together (0: memory budget
         only); policy "fifo" admits in arrival order, "shortest" admits the
-        queued request with the least work (cells x iteration cap) first."""
+        queued request with the least work (cells x iteration cap) first.
+        group: the solve group to drive (default: a new G.Group of dtype)."""
         if policy not in ("fifo", "shortest"):
             raise ValueError("policy must be 'fifo' or 'shortest'")
-        self.group = G.Group(dtype)
+        self.group = group if group is not None else G.Group(dtype)
+        self._unsorted = False
         self.budget = int(budget_bytes)
         self.k = int(iters_per_step)
         self.keep_q = keep_q
@@ -77,12 +80,14 @@ class Server:
 
     def submit(self, req):
         self.queue.append(req)
+        self._unsorted = True
 
     def _admit(self, now):
         g = self.group
-        if self.policy == "shortest" and len(self.queue) > 1:
+        if self.policy == "shortest" and self._unsorted and len(self.queue) > 1:
             self.queue = deque(sorted(self.queue, key=lambda q: (q.mesh.ncell * q.max_iter,
                                                                  q.arrival)))
+        self._unsorted = False
         while self.queue:
             if self.max_active and len(self.active) >= self.max_active:
                 break
