@@ -91,17 +91,6 @@ def write_grid(mesh, path):
         raise IOError("cannot write %s" % path)
 
 
-def read_grid(path, I=0, J=0):
-    lib = _lib.load()
-    m = _lib.op2b_mesh()
-    if lib.op2b_mesh_read(str(path).encode(), C.byref(m)) != 0:
-        raise IOError("cannot read %s" % path)
-    try:
-        return AirfoilMesh(I=I, J=J, **_take(m))
-    finally:
-        lib.op2b_mesh_free(C.byref(m))
-
-
 def cells_to_IJ(cells):
     """I, J of a 2:1 (3I : J = 2 : 1) C-mesh with about `cells` cells."""
     J = max(4, int(round((cells / 2.0) ** 0.5)))
