@@ -7,7 +7,6 @@ still bit-identical to the reference's sequential build (contributions keep
 the app's element order) and come back from op_fetch_data in the app's
 order; the TREE rms stays within its summation tolerance; jac is unchanged.
 """
-import ctypes as C
 import hashlib
 import os
 import subprocess

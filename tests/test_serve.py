@@ -10,7 +10,6 @@ solved alone.
 import os
 import socket
 
-import numpy as np
 import pytest
 import torch.distributed as dist
 import torch.multiprocessing as mp
