@@ -242,7 +242,7 @@ int op2o_plan_check(const op2o_plan *P, const int *const *maps, const int *map_d
   for (int n = 0; n < nblock; n++) { err += (P->offset[n] != tot); tot += P->nelems[n]; }
   fails += (err != 0);
 
-  int *seen = calloc(nblock ? nblock : 1, sizeof(int));
+  int *seen = calloc(nblock > 0 ? (size_t)nblock : 1, sizeof(int));
   err = 0;
   for (int n = 0; n < nblock; n++) {
     int b = P->blkmap[n];
