@@ -56,6 +56,8 @@ sys.path.insert(0, ROOT)
 METRIC = "720k-cell airfoil iters/s"
 UNIT = "iters/s"
 I_MESH, J_MESH = 400, 600
+MESH_SEED = 20261203  # the seed of the scrambled and randomised configurations
+REF_MIN_ITERS = 400   # the reference arm times at least this many iterations
 
 
 def parse():
@@ -259,16 +261,35 @@ def iteration_bytes(m, s=4):
 
 # ------------------------------------------------------------ reference ----
 
-def run_reference_openmp(mesh, niter, fp64=False, threads=None):
+def make_grid(I, J, path, scramble=False):
+    """Write the reference apps' input (new_grid.dat) with the host-only
+    generator program oracle/_build/gen_grid (the restated naca0012.m), in a
+    child process, so the process timing the reference never loads this
+    repository's CUDA library.  Returns the set sizes (nnode, ncell, nedge,
+    nbedge) or None."""
+    gen = os.path.join(ROOT, "oracle", "_build", "gen_grid")
+    if not os.path.exists(gen):
+        return None
+    cmd = [gen, str(I), str(J)] + (["1", str(MESH_SEED)] if scramble else []) + [path]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    if r.returncode != 0:
+        return None
+    nnode, ncell, nedge, nbedge = (int(v) for v in r.stdout.split())
+    return {"nnode": nnode, "ncell": ncell, "nedge": nedge, "nbedge": nbedge}
+
+
+def run_reference_openmp(I, J, niter, fp64=False, threads=None):
     """The reference's OpenMP airfoil (oracle/_ref/airfoil_op_f32) on this
-    host; returns (iters/s from its own op_timing_output, seconds, cores)."""
+    host, on the I x J mesh; returns (iters/s from its own op_timing_output,
+    seconds, cores, set sizes) or None."""
     binary = os.path.join(ROOT, "oracle", "_ref", "airfoil_op_f64" if fp64 else "airfoil_op_f32")
     if not os.path.exists(binary):
         return None
-    from oplus2_matlab_b200 import mesh as M
-    d = tempfile.mkdtemp(dir=os.path.join(ROOT, "oracle", "_ref"))
+    d = tempfile.mkdtemp(prefix="op2b_reference_")
     try:
-        M.write_grid(mesh, os.path.join(d, "new_grid.dat"))
+        sizes = make_grid(I, J, os.path.join(d, "new_grid.dat"))
+        if sizes is None:
+            return None
         cores = threads or os.cpu_count()
         env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_PROC_BIND="close",
                    OP2REF_NITER=str(niter), OP2REF_PRINT=str(max(niter, 1)))
@@ -281,31 +302,32 @@ def run_reference_openmp(mesh, niter, fp64=False, threads=None):
             if len(f) >= 4 and f[0].isdigit() and f[-1] in ("save_soln", "adt_calc", "res_calc",
                                                           "bres_calc", "update"):
                 tot += float(f[1])
-        return (niter / tot if tot > 0 else None), tot, cores
+        return (niter / tot if tot > 0 else None), tot, cores, sizes
     finally:
         shutil.rmtree(d, ignore_errors=True)
 
 
 def impl_reference(args, dist):
-    """--impl reference: rank 0 times the reference's OpenMP airfoil; other
-    ranks exit without work."""
+    """--impl reference: rank 0 times the reference's OpenMP airfoil on the
+    same 720k mesh (written by the host-only generator; nothing of this
+    repository's GPU library is loaded); other ranks exit without work."""
     if dist.rank != 0:
         return
-    from oplus2_matlab_b200 import mesh as M
-    mesh = M.naca0012(I_MESH, J_MESH)
-    niter = max(1, args.steps + args.warmup)
-    res = run_reference_openmp(mesh, niter, fp64=args.fp64)
+    niter = max(REF_MIN_ITERS, args.steps + args.warmup)
+    res = run_reference_openmp(I_MESH, J_MESH, niter, fp64=args.fp64)
     base = {"impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup}
     if res is None or res[0] is None:
-        print(json.dumps(dict(base, unavailable="reference OpenMP build oracle/_ref/airfoil_op_f32 missing or failed")))
+        print(json.dumps(dict(base, unavailable="reference OpenMP build oracle/_ref/airfoil_op_f32 "
+                                                "or the grid writer oracle/_build/gen_grid missing or failed")))
         return
-    v, secs, cores = res
+    v, secs, cores, sizes = res
     line = dict(base, value=v, ms_per_step=1e3 / v, scaling="weak", vs_baseline=None,
                 dtype="f64" if args.fp64 else "f32", data="synthetic",
-                config={"workload": "airfoil NACA0012 C-mesh 1200x600 cells (720,000), %s, "
-                                    "reference OpenMP airfoil_op on host cores" % ("FP64" if args.fp64 else "FP32"),
-                        "cells": mesh.ncell, "edges": mesh.nedge, "iterations": niter},
+                config=plain_config(I_MESH, J_MESH, sizes, False),
+                reference={"build": "reference airfoil_op (OpenMP), compiled from its sources by "
+                                    "oracle/Makefile", "iterations": niter, "seconds": secs,
+                           "timing": "sum of the per-loop times of its own op_timing_output"},
                 cpu_baseline={"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
                               "sample": "%d iterations of the 720k mesh, sum of op_timing_output" % niter},
                 e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
@@ -322,13 +344,19 @@ def plain_mesh(args):
     return M.naca0012(I, J, scramble=scramble)
 
 
-def workload_name(mesh, args):
-    if args.mesh == "400x600":
-        return ("airfoil 720k cells (I=400, J=600: 720,000 cells, 1,438,600 edges, "
-                "721,801 nodes, 2,800 bedges), one outer iteration per step")
-    return ("airfoil %s (%s%d cells, %d edges, %d nodes, %d bedges), one outer iteration per step"
-            % (args.mesh, "scrambled numbering, " if args.mesh.endswith("s") else "",
-               mesh.ncell, mesh.nedge, mesh.nnode, mesh.nbedge))
+def plain_config(I, J, sizes, scrambled):
+    """The workload keys both arms report for the plain single-mesh solve
+    (the reference arm's config holds exactly these)."""
+    return {"workload": "airfoil NACA0012 C-mesh I=%d, J=%d%s: %d cells, %d edges, %d nodes, "
+                        "%d bedges; one outer iteration (save_soln + 2 x (adt_calc, res_calc, "
+                        "bres_calc, update)) per step"
+                        % (I, J, ", scrambled numbering" if scrambled else "", sizes["ncell"],
+                           sizes["nedge"], sizes["nnode"], sizes["nbedge"]),
+            "cells": sizes["ncell"], "edges": sizes["nedge"]}
+
+
+def mesh_sizes(mesh):
+    return {"nnode": mesh.nnode, "ncell": mesh.ncell, "nedge": mesh.nedge, "nbedge": mesh.nbedge}
 
 
 def impl_ours(args, dist):
@@ -486,12 +514,11 @@ def impl_ours(args, dist):
         "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.fp64 else "f32",
         "data": "synthetic: NACA0012 C-mesh from the reference's generator, free-stream start",
-        "config": {"workload": workload_name(mesh, args),
-                   "cells": mesh.ncell, "edges": mesh.nedge, "strategy": args.strategy,
-                   "renumbered": bool(args.renumber),
-                   "reduction": "tree", "l2": "flushed before every step (untimed read-only sweep of 3x the 126 MB L2)",
-                   "timing": "CUDA events around each graph launch on the library stream",
-                   "parallelism": "replicas" if dist.world > 1 else "single GPU"},
+        "config": dict(plain_config(mesh.I, mesh.J, mesh_sizes(mesh), args.mesh.endswith("s")),
+                       strategy=args.strategy, renumbered=bool(args.renumber), reduction="tree",
+                       l2="flushed before every step (untimed read-only sweep of 3x the 126 MB L2)",
+                       timing="CUDA events around each graph launch on the library stream",
+                       parallelism="replicas" if dist.world > 1 else "single GPU"),
         "roofline": {"bound": "hbm", "kernel": res_key, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": ncu_traffic(),
                      "peak_source": peak_kind,
@@ -578,12 +605,12 @@ def run_e2e(mesh, fp64, niter, strategy, dist):
 
 def cpu_baseline(mesh, fp64):
     """The reference OpenMP build on a bounded sample (about 10-30 s)."""
-    probe = run_reference_openmp(mesh, 3, fp64=fp64)
+    probe = run_reference_openmp(mesh.I, mesh.J, 3, fp64=fp64)
     if probe is None or probe[0] is None:
         return None
     rate = probe[0]
     niter = int(min(400, max(5, 15.0 * rate)))
-    res = run_reference_openmp(mesh, niter, fp64=fp64)
+    res = run_reference_openmp(mesh.I, mesh.J, niter, fp64=fp64)
     if res is None or res[0] is None:
         return None
     return {"value": res[0], "unit": UNIT, "cores": res[2], "kind": "reference",

@@ -157,9 +157,14 @@ int op2b_l2_flush(void);
  * library, so ncell must be at most 4,194,304 (larger sizes return -1 and run
  * nothing).  The first call on a device looks up that array's address: make
  * it before any stream capture.  All calls share the array, so calls that
- * overlap on the GPU race; calls in one stream are safe.  Returns 0, a
- * negative code for bad arguments, or a CUDA error code; asynchronous on
- * `stream` (a cudaStream_t, NULL for the default stream). */
+ * overlap on the GPU race; calls in one stream are safe.  Misaligned or
+ * null pointers return -3 before anything is launched.  The scratch address
+ * is cached per device until op_exit: call op_exit before resetting a
+ * device.  The call runs on the caller's `stream` (a cudaStream_t, NULL for
+ * the default stream) with no ordering against the library's own stream:
+ * synchronise, or pass op2b_get_stream(), when mixing it with op_par_loop
+ * calls on the same data.  Returns 0, a negative code for bad arguments, or
+ * a CUDA error code; asynchronous. */
 int op2b_update_noalloc(int ncell, const float *qold, float *q, float *res, const float *adt,
                         float *rms, void *stream);
 

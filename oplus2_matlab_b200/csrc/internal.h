@@ -165,6 +165,7 @@ int const_get_f64(char const *name, double *out, int n);
 // update's kernel into spare buffers, swapped in when the calls come
 void ahead_drop();   // discard what was run ahead (constants, capture, restore)
 void ahead_reset();  // op_exit: also free the spare buffers
+void noalloc_reset();  // op_exit: forget op2b_update_noalloc's cached scratch addresses
 int live_graphs();   // captured graphs not yet destroyed (graph.cu)
 
 // renumbering of the sets for locality (renumber.cu)

@@ -278,6 +278,12 @@ bool run_jac_res_ahead(char const *name, op_set set, const op_arg *args, int var
   return variant == 1 && jac_res_t<1>(name, set, args, (float *)du_out);
 }
 
+bool can_run_jac_res_ahead(char const *name, op_set set, const op_arg *args, int variant) {
+  if (variant != 1 || effective_strategy(name) == OP2B_STRATEGY_COLOURED) return false;
+  GatherPlan *g = get_gather_plan(set, args, {2});
+  return g && g->nactive == args[2].dat->set->size;
+}
+
 template <int V>
 static void jac_update_t(char const *name, op_set set, const op_arg *args,
                          std::vector<GblRequest> *held) {

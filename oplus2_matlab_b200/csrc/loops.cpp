@@ -264,6 +264,10 @@ cudaEvent_t g_fold_done = nullptr;
 // spare buffer of du, and is swapped in when the res call repeats the last
 // one with the same beta
 std::vector<op_arg> g_seen_jres;
+// the res call's beta (gbl OP_READ), copied when the call is recorded: the
+// caller's variable may be gone by the next update, so g_seen_jres[3].data
+// points here, never at the caller's memory
+alignas(16) char g_seen_jres_beta[16];
 op_set g_seen_jres_set = nullptr;
 int g_seen_jres_variant = 0;
 std::string g_seen_jres_name;
@@ -358,6 +362,8 @@ bool jac_update_ahead(char const *name, op_set set, const op_arg *a, int variant
   if (!tuning("run_ahead", 1) || rt().gbl_deferred || live_graphs() > 0 || variant != 1 ||
       g_seen_jres.size() != 4 || g_seen_jres_variant != 1 ||
       g_seen_jres[1].dat != a[2].dat || g_seen_jres[2].dat != a[1].dat)
+    return false;
+  if (!can_run_jac_res_ahead(g_seen_jres_name.c_str(), g_seen_jres_set, g_seen_jres.data(), 1))
     return false;
   void *du_out = spare_of(a[1].dat);
   if (error_pending()) return false;
@@ -604,6 +610,14 @@ void par_loop_run(char const *name, op_set set, int nargs, const op_arg *args) {
       return;
     }
     g_seen_jres.assign(args, args + nargs);
+    const size_t beta_bytes =
+        (size_t)args[3].dim * (args[3].type && strcmp(args[3].type, "double") == 0 ? 8 : 4);
+    if (nargs == 4 && args[3].data && beta_bytes <= sizeof(g_seen_jres_beta)) {
+      memcpy(g_seen_jres_beta, args[3].data, beta_bytes);
+      g_seen_jres[3].data = g_seen_jres_beta;
+    } else {
+      g_seen_jres.clear();  // nothing recorded: no run-ahead for this res
+    }
     g_seen_jres_set = set;
     g_seen_jres_variant = v;
     g_seen_jres_name = name;

@@ -73,6 +73,9 @@ void run_jac_update(char const *name, op_set set, const op_arg *args, int varian
 // of its call; false when not applicable (nothing launched)
 bool run_jac_res_ahead(char const *name, op_set set, const op_arg *args, int variant,
                        void *du_out);
+// whether run_jac_res_ahead would launch for these arguments (GATHER, jac1,
+// every node a target); allocates nothing beyond the res loop's own plan
+bool can_run_jac_res_ahead(char const *name, op_set set, const op_arg *args, int variant);
 
 // fused loop pairs (airfoil.cu); false = not applicable, run them separately
 bool run_save_adt(op_set set, const op_arg *save_args, const op_arg *adt_args);

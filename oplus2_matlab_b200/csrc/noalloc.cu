@@ -18,12 +18,18 @@
 //    larger sets are rejected with an error and nothing runs;
 //  - the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture;
+//    before any stream capture.  The address is cached per device until
+//    op_exit; a caller that resets a device (cudaDeviceReset) must call
+//    op_exit first, so that the next call looks the address up again;
+//  - qold, q and res are read and written as 16-byte vectors, so they must
+//    be 16-byte aligned (adt and rms 4-byte); misaligned pointers are
+//    rejected before anything is launched;
 //  - all calls share the one array: calls that overlap on the GPU (on
 //    different streams, or from different threads) race and give wrong
 //    sums.  Calls in one stream are ordered and safe.
 // No cudaMalloc, cudaFree or other allocating routine is called here.
 
+#include <stdint.h>
 #include <stdio.h>
 
 #include <mutex>
@@ -98,10 +104,20 @@ __global__ void __launch_bounds__(256) k_update_noalloc(int n, const float *__re
 }
 
 // device address of g_noalloc_scratch, looked up once per device
+constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_mu;
-void *g_addr[64];
+void *g_addr[kNoAllocMaxDevices];
 
 }  // namespace
+
+namespace op2b {
+// op_exit: forget the cached addresses (a device reset after op_exit
+// invalidates them; the next call looks them up again)
+void noalloc_reset() {
+  std::lock_guard<std::mutex> lock(g_mu);
+  for (auto &a : g_addr) a = nullptr;
+}
+}  // namespace op2b
 
 extern "C" int op2b_update_noalloc(int ncell, const float *qold, float *q, float *res,
                                    const float *adt, float *rms, void *stream) {
@@ -116,11 +132,24 @@ extern "C" int op2b_update_noalloc(int ncell, const float *qold, float *q, float
     fprintf(stderr, "op2b_update_noalloc error: null device pointer argument\n");
     return -3;
   }
+  if (ncell > 0 && ((((uintptr_t)qold | (uintptr_t)q | (uintptr_t)res) & 15) ||
+                    (((uintptr_t)adt | (uintptr_t)rms) & 3))) {
+    fprintf(stderr,
+            "op2b_update_noalloc error: qold, q and res must be 16-byte aligned and adt, rms "
+            "4-byte aligned; nothing was run\n");
+    return -3;
+  }
   if (ncell == 0) return 0;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return (int)e;
-  if (dev < 0 || dev >= 64) return -2;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) {
+    fprintf(stderr,
+            "op2b_update_noalloc error: device %d is beyond the %d devices whose scratch "
+            "address it caches; nothing was run\n",
+            dev, kNoAllocMaxDevices);
+    return -2;
+  }
   void *base = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_mu);

@@ -161,8 +161,11 @@ def main():
     ap.add_argument("--large", action="store_true")
     ap.add_argument("--only", default="")
     ap.add_argument("--skip-plans", action="store_true")
+    ap.add_argument("--ref", default=os.environ.get("OP2B_REFERENCE", "/root/reference"),
+                    help="the reference tree, from whose sources oracle/_ref is built")
     a = ap.parse_args()
-    subprocess.run(["make", "-s", "-f", os.path.join(ROOT, "oracle", "Makefile"), "ref"], check=True)
+    subprocess.run(["make", "-s", "-f", os.path.join(ROOT, "oracle", "Makefile"), "REF=" + a.ref,
+                    "ref"], check=True)
     os.makedirs(SCRATCH, exist_ok=True)
     out = {}
     small = {

@@ -5,6 +5,8 @@ library's normal update entry point (op_par_loop_update) -- q and res bit
 for bit, the rms within the FP32 tolerance the other tests use -- on two
 calls in a row, since both calls share the library's fixed scratch array.
 This file sorts last so a stop-at-first-failure run has done everything else.
+The argument checks run on the host before anything touches the GPU, so
+they are tested without one.
 """
 import ctypes as C
 
@@ -13,8 +15,6 @@ import pytest
 
 from oplus2_matlab_b200 import _lib, apps
 from oplus2_matlab_b200 import mesh as M
-
-pytestmark = pytest.mark.gpu
 
 
 def _cudart():
@@ -33,6 +33,25 @@ def _cudart():
 H2D, D2H = 1, 2
 
 
+def test_update_noalloc_rejects_misaligned_pointers_before_launch():
+    """qold, q and res are 16-byte vectors in the kernel; a misaligned
+    pointer would fault on the device, so it is refused on the host (-3),
+    as are null pointers and sizes beyond the fixed scratch (-1).  The
+    pointers below are never dereferenced: every case returns first."""
+    lib = _lib.load()
+    ok16, ok4 = 0x10000, 0x20000
+    assert lib.op2b_update_noalloc(64, ok16 + 4, ok16, ok16, ok4, ok4, None) == -3  # qold
+    assert lib.op2b_update_noalloc(64, ok16, ok16 + 8, ok16, ok4, ok4, None) == -3  # q
+    assert lib.op2b_update_noalloc(64, ok16, ok16, ok16 + 12, ok4, ok4, None) == -3  # res
+    assert lib.op2b_update_noalloc(64, ok16, ok16, ok16, ok4 + 2, ok4, None) == -3  # adt
+    assert lib.op2b_update_noalloc(64, ok16, ok16, ok16, ok4, ok4 + 1, None) == -3  # rms
+    assert lib.op2b_update_noalloc(64, None, ok16, ok16, ok4, ok4, None) == -3
+    assert lib.op2b_update_noalloc(4096 * 1024 + 1, ok16, ok16, ok16, ok4, ok4, None) == -1
+    assert lib.op2b_update_noalloc(-1, ok16, ok16, ok16, ok4, ok4, None) == -1
+    assert lib.op2b_update_noalloc(0, None, None, None, None, None, None) == 0
+
+
+@pytest.mark.gpu
 def test_update_noalloc_matches_op_par_loop_update(op2):
     m = M.naca0012(100, 150)  # 45,000 cells
     n = m.ncell
