@@ -146,6 +146,14 @@ long op2b_plan_validate(char const *name, op_set set, int part_size, int nargs, 
  * times its size; benchmark drivers call it between timed steps. */
 int op2b_l2_flush(void);
 
+/* Bounded waits that ran out in the library's kernels (mbarrier waits of
+ * the TMA-staged per-cell pass) since the last reset; reset != 0 clears the
+ * count.  Every wait gives up after one second, counts here and lets its
+ * kernel return, so a lost completion shows up as a nonzero count (and
+ * wrong results) instead of a hung GPU; 0 in every correct run.
+ * Synchronises the library stream.  No counterpart in the reference. */
+unsigned op2b_wait_timeouts(int reset);
+
 /* The airfoil update loop (q = qold - res/adt, res = 0, *rms += sum of
  * del^2) for callers that must not allocate device memory: code that cannot
  * afford cudaMalloc's device synchronisation, hosts that reserve all device

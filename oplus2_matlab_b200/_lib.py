@@ -126,6 +126,7 @@ PROTOTYPES = [
      [C.c_char_p, op_set, C.c_int, C.c_int, C.POINTER(op_arg), C.c_int, C.POINTER(C.c_int)]),
     ("op2b_version", C.c_char_p, []),
     ("op2b_l2_flush", C.c_int, []),
+    ("op2b_wait_timeouts", C.c_uint, [C.c_int]),
     ("op2b_set_tuning", C.c_int, [C.c_char_p, C.c_int]),
     ("op2b_update_noalloc", C.c_int, [C.c_int, _P, _P, _P, _P, _P, _P]),
     ("op2b_set_renumber", C.c_int, [C.c_int]),

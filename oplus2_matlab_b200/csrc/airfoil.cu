@@ -25,6 +25,7 @@
 #include "launch.cuh"
 #include "loops.h"
 #include "reduce.cuh"
+#include "tma.cuh"
 
 namespace op2b {
 
@@ -705,6 +706,215 @@ __global__ void __launch_bounds__(256, MINB)
   const T v[1] = {rms}, id[1] = {T(0)};
   RedSlot<T> sl[1] = {slot};
   grid_finish<T, OpSum, OpSum, 1>(v, id, OpSum(), OpSum(), sl, ticket);
+}
+
+// The per-cell pass (ordered fold + update [+ adt_calc] [+ save_soln]) with
+// its contiguous streams staged by the TMA engine.  One warp produces, NC
+// warps consume; a tile is TC = 32 NC consecutive cells, one per consumer
+// thread.  For every tile the producer's elected lane issues one
+// cp.async.bulk per array -- the cells' list entries, pcell rows (the
+// first hop of the gathers: plan and map data, issued before the PDL wait
+// for the first S tiles), res, qold, adt -- into one of S shared-memory
+// stages, completing on the stage's "full" mbarrier.  The consumers take
+// each cell's list and node indices and its res, qold, adt from the stage,
+// hand the stage back ("empty" barrier) as soon as they hold it in
+// registers, gather the listed flux values and the nodes' x (L2), and do
+// the arithmetic of k_fold_update in the same order, so q, res, adt, qold
+// are bit-identical to it.  So the streams of S tiles are in flight per
+// CTA without costing the consumers registers or issue slots.
+//
+// Cells are split into one balanced contiguous range per CTA (a multiple of
+// 4 cells, so every tile's copies start 16-byte aligned); a tile's copy
+// sizes are rounded down to 16 bytes and the consumers load the few
+// trailing elements past them from global memory.  Each thread folds its
+// del^2 over its cells in tile order, so the TREE sum depends only on the
+// cell count and the grid.  Waits are bounded (tma.cuh): a wait that runs
+// out is counted, its warp skips the remaining tiles, and before the CTA
+// returns its producer waits, bounded again, for copies still in flight.
+template <class T, bool ADT, bool SAVE, int NC, int S, int MINB>
+__global__ void __launch_bounds__((NC + 1) * 32, MINB)
+    k_fold_tma(int n, int chunk, int W, const int *__restrict__ ell, const T *__restrict__ vals,
+               const T *qold, T *q, T *res, const T *adt, const int4 *__restrict__ pcell,
+               const T *__restrict__ x0, const T *__restrict__ x1, const T *__restrict__ x2,
+               const T *__restrict__ x3, AirConsts<T> K, T *seq, RedSlot<T> slot,
+               unsigned *ticket, T *qsave, T *adt_out) {
+  constexpr int TC = NC * 32;
+  extern __shared__ __align__(128) unsigned char stage_mem[];
+  __shared__ __align__(8) unsigned long long full[S], empty[S];
+  __shared__ int timed_out;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int cb = (int)min((long long)n, (long long)blockIdx.x * chunk);
+  const int ce = (int)min((long long)n, (long long)cb + chunk);
+  const int ntile = (ce - cb + TC - 1) / TC;
+  // stage layout: list entries | pcell rows | res | qold | adt
+  const unsigned ell_b = ((unsigned)(TC * W * 4) + 15u) & ~15u;
+  const unsigned nd_b = ADT ? TC * 16u : 0u;
+  const unsigned v4_b = TC * 4u * sizeof(T);
+  const unsigned adt_b = ((unsigned)(TC * sizeof(T)) + 15u) & ~15u;
+  const unsigned stage_b = ell_b + nd_b + 2u * v4_b + adt_b;
+  if (threadIdx.x == 0) {
+    timed_out = 0;
+    for (int i = 0; i < S; i++) {
+      mbar_init(smem_addr(&full[i]), 1);
+      mbar_init(smem_addr(&empty[i]), NC);
+    }
+    mbar_init_fence();
+  }
+  __syncthreads();
+  T rms = T(0);
+  if (warp == NC) {  // ------------------------------------------ producer
+    if (lane == 0) {
+      // bytes of tile t's copies: each array's size rounded down to 16
+      auto sizes = [&](int t, unsigned (&b)[5]) {
+        const int nct = min(TC, ce - (cb + t * TC));
+        b[0] = (unsigned)(nct * W * 4) & ~15u;
+        b[1] = ADT ? nct * 16u : 0u;
+        b[2] = b[3] = nct * 4u * sizeof(T);
+        b[4] = (unsigned)(nct * sizeof(T)) & ~15u;
+      };
+      auto issue = [&](int t, bool plan_part, bool data_part) {
+        unsigned b[5];
+        sizes(t, b);
+        const int c0 = cb + t * TC;
+        const uint32_t st = smem_addr(stage_mem + (size_t)(t % S) * stage_b);
+        const uint32_t bar = smem_addr(&full[t % S]);
+        if (plan_part) {
+          if (b[0]) bulk_load(st, ell + (size_t)c0 * W, b[0], bar);
+          if (ADT) bulk_load(st + ell_b, pcell + c0, b[1], bar);
+        }
+        if (data_part) {
+          bulk_load(st + ell_b + nd_b, res + 4 * (size_t)c0, b[2], bar);
+          bulk_load(st + ell_b + nd_b + v4_b, qold + 4 * (size_t)c0, b[3], bar);
+          if (b[4]) bulk_load(st + ell_b + nd_b + 2 * v4_b, adt + c0, b[4], bar);
+        }
+      };
+      auto arm = [&](int t) {
+        unsigned b[5];
+        sizes(t, b);
+        mbar_arrive_expect_tx(smem_addr(&full[t % S]), b[0] + b[1] + b[2] + b[3] + b[4]);
+      };
+      const int pre = min(ntile, S);
+      for (int t = 0; t < pre; t++) {  // plan and map data: no kernel writes them
+        arm(t);
+        issue(t, true, false);
+      }
+      pdl_wait();
+      for (int t = 0; t < pre; t++) issue(t, false, true);
+      for (int t = S; t < ntile; t++) {
+        if (!mbar_wait(smem_addr(&empty[t % S]), (unsigned)((t / S - 1) & 1))) {
+          timed_out = 1;
+          break;
+        }
+        arm(t);
+        issue(t, true, true);
+      }
+    } else {
+      pdl_wait();
+    }
+    __syncwarp();
+    pdl_trigger();
+  } else {  // ----------------------------------------------------- consumers
+    pdl_wait();
+    pdl_trigger();
+    const int i = warp * 32 + lane;  // this thread's cell within a tile
+    for (int t = 0; t < ntile; t++) {
+      const int sidx = t % S;
+      if (!mbar_wait(smem_addr(&full[sidx]), (unsigned)((t / S) & 1))) {
+        timed_out = 1;
+        break;
+      }
+      const unsigned char *st = stage_mem + (size_t)sidx * stage_b;
+      const int c0 = cb + t * TC, c = c0 + i;
+      const int nct = min(TC, ce - c0);
+      int k[4] = {-1, -1, -1, -1}, nd[4] = {0, 0, 0, 0};
+      T r[4], qo[4], ad = T(1);
+      if (i < nct) {
+        const unsigned ell_copied = (unsigned)(nct * W * 4) & ~15u;
+        if ((unsigned)((i + 1) * W * 4) <= ell_copied) {
+          const int *e = reinterpret_cast<const int *>(st) + i * W;
+          if ((W & 3) == 0) {
+            const int4 kk = *reinterpret_cast<const int4 *>(e);
+            k[0] = kk.x; k[1] = kk.y; k[2] = kk.z; k[3] = kk.w;
+          } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++) k[j] = j < W ? e[j] : -1;
+          }
+        } else {
+          list_head(ell, W, c, k);
+        }
+        if (ADT) {
+          const int4 v = reinterpret_cast<const int4 *>(st + ell_b)[i];
+          nd[0] = v.x; nd[1] = v.y; nd[2] = v.z; nd[3] = v.w;
+        }
+        ldw4(reinterpret_cast<const T *>(st + ell_b + nd_b) + 4 * i, r);
+        ldw4(reinterpret_cast<const T *>(st + ell_b + nd_b + v4_b) + 4 * i, qo);
+        const unsigned adt_copied = (unsigned)(nct * sizeof(T)) & ~15u;
+        ad = (unsigned)((i + 1) * sizeof(T)) <= adt_copied
+                 ? reinterpret_cast<const T *>(st + ell_b + nd_b + 2 * v4_b)[i]
+                 : adt[c];
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_addr(&empty[sidx]));  // the stage is free again
+      if (i >= nct) continue;
+      T f[4][4], xs[4][2];
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (k[j] >= 0) ld4(vals + 4 * (size_t)(k[j] >> 1), f[j]);
+      if (ADT) {
+        ld2(x0 + 2 * (size_t)nd[0], xs[0]);
+        ld2(x1 + 2 * (size_t)nd[1], xs[1]);
+        ld2(x2 + 2 * (size_t)nd[2], xs[2]);
+        ld2(x3 + 2 * (size_t)nd[3], xs[3]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j++) add_listed(r, k[j], f[j]);
+      for (int j = 4; j < W; j++) {  // lists longer than 4
+        const int kk = __ldg(ell + (size_t)c * W + j);
+        T g[4];
+        ld4(vals + 4 * (size_t)(kk >> 1), g);
+        add_listed(r, kk, g);
+      }
+      // airfoil/update.h:1-12
+      T adti = rcp(ad);
+      T qn[4], sq[4];
+      for (int d = 0; d < 4; d++) {
+        T del = adti * r[d];
+        qn[d] = qo[d] - del;
+        sq[d] = del * del;
+        rms += sq[d];
+      }
+      st4(q + 4 * (size_t)c, qn);
+      if (SAVE) st4(qsave + 4 * (size_t)c, qn);  // airfoil/save_soln.h:1-3
+      const T z[4] = {T(0), T(0), T(0), T(0)};
+      st4(res + 4 * (size_t)c, z);
+      if (seq) st4(seq + 4 * (size_t)c, sq);
+      if (ADT) adt_out[c] = adt_calc(xs[0], xs[1], xs[2], xs[3], qn, K);
+    }
+  }
+  __syncthreads();
+  if (timed_out && threadIdx.x == NC * 32) {
+    // copies may still be in flight into this CTA's stages: wait for the
+    // last phase of every stage (bounded) before the CTA's memory goes
+    for (int sidx = 0; sidx < S && sidx < ntile; sidx++) {
+      const int last = sidx + ((ntile - 1 - sidx) / S) * S;
+      mbar_wait(smem_addr(&full[sidx]), (unsigned)((last / S) & 1));
+    }
+  }
+  if (seq) return;
+  const T v[1] = {rms}, id[1] = {T(0)};
+  RedSlot<T> sl[1] = {slot};
+  grid_finish<T, OpSum, OpSum, 1>(v, id, OpSum(), OpSum(), sl, ticket);
+}
+
+// shared memory of one k_fold_tma CTA: S stages for list width W
+template <class T, bool ADT, int NC, int S>
+inline size_t fold_tma_smem(int W) {
+  const size_t TC = NC * 32;
+  const size_t ell_b = (TC * W * 4 + 15) & ~(size_t)15;
+  const size_t nd_b = ADT ? TC * 16 : 0;
+  const size_t v4_b = TC * 4 * sizeof(T);
+  const size_t adt_b = (TC * sizeof(T) + 15) & ~(size_t)15;
+  return S * (ell_b + nd_b + 2 * v4_b + adt_b);
 }
 
 template <class T>
@@ -1574,7 +1784,7 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
                         std::vector<GblRequest> *held) {
   // save_soln rides on the one-cell-per-thread fold + update + adt_calc forms
   const int fvar = tuning("fold_variant", 0);
-  if (sa && (!ua || !aa || (fvar != 0 && fvar != 4 && fvar != 5))) return false;
+  if (sa && (!ua || !aa || (fvar != 0 && fvar != 4 && fvar != 5 && fvar != 6))) return false;
   AirConsts<T> K = air_consts<T>();
   if (error_pending()) return true;
   cudaStream_t s = rt().stream;
@@ -1649,6 +1859,64 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
                    red_ticket(), qsave, adt_to);
       };
       const int fv = fvar;
+      // fold_variant 6: the TMA-staged pass; fold_tma_cfg picks consumer
+      // warps x stages (1: 4 x 4, 2: 8 x 3, 3: 4 x 6, 4: 2 x 8)
+      auto launch_tma = [&](auto kernel, int nc, size_t smem) -> bool {
+        const bool quad = !aa || (N.m0.map && N.m0.map == N.m1.map && N.m0.map == N.m2.map &&
+                                  N.m0.map == N.m3.map && N.m0.dim == 4 && N.m0.idx == 0 &&
+                                  N.m1.idx == 1 && N.m2.idx == 2 && N.m3.idx == 3);
+        const uintptr_t bases = (uintptr_t)sp->d_ell | (uintptr_t)res | (uintptr_t)qold |
+                                (uintptr_t)adt | (aa ? (uintptr_t)N.m0.map : 0);
+        if (!quad || (bases & 15) || smem > (size_t)rt().smem_optin) return false;
+        static std::vector<std::pair<const void *, size_t>> sized;
+        const void *kp = (const void *)kernel;
+        if (std::find(sized.begin(), sized.end(), std::make_pair(kp, smem)) == sized.end()) {
+          OP2B_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+          sized.emplace_back(kp, smem);
+        }
+        const int threads = (nc + 1) * 32, tc = nc * 32;
+        int per = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) !=
+                cudaSuccess || per < 1)
+          per = 1;
+        const long long tiles = (ncell + tc - 1LL) / tc;
+        const int grid = (int)std::max(1LL, std::min(std::min((long long)rt().num_sms * per,
+                                                              (long long)kMaxRedBlocks), tiles));
+        long long chunk = (ncell + grid - 1LL) / grid;
+        chunk = (chunk + 3) & ~3LL;
+        launch_pdl(kernel, grid, threads, smem, s, ncell, (int)chunk, W, (const int *)sp->d_ell,
+                   (const T *)vals, qold, q, res, (const T *)adt,
+                   (const int4 *)(aa ? N.m0.map : nullptr), xs[0], xs[1], xs[2], xs[3], K,
+                   seqbuf, rslot, red_ticket(), qsave, adt_to ? adt_to : adt);
+        return true;
+      };
+      auto tma = [&](auto k44, auto k83, auto k46, auto k28, bool with_adt) -> bool {
+        const int cfg = tuning("fold_tma_cfg", 1);
+        if (cfg == 2) return launch_tma(k83, 8, with_adt ? fold_tma_smem<T, true, 8, 3>(W)
+                                                         : fold_tma_smem<T, false, 8, 3>(W));
+        if (cfg == 3) return launch_tma(k46, 4, with_adt ? fold_tma_smem<T, true, 4, 6>(W)
+                                                         : fold_tma_smem<T, false, 4, 6>(W));
+        if (cfg == 4) return launch_tma(k28, 2, with_adt ? fold_tma_smem<T, true, 2, 8>(W)
+                                                         : fold_tma_smem<T, false, 2, 8>(W));
+        return launch_tma(k44, 4, with_adt ? fold_tma_smem<T, true, 4, 4>(W)
+                                           : fold_tma_smem<T, false, 4, 4>(W));
+      };
+      constexpr int M6 = sizeof(T) == 4 ? 6 : 3, M3 = sizeof(T) == 4 ? 3 : 2;
+      if (fv == 6) {
+        bool done;
+        if (sa)
+          done = tma(k_fold_tma<T, true, true, 4, 4, M6>, k_fold_tma<T, true, true, 8, 3, M3>,
+                     k_fold_tma<T, true, true, 4, 6, M6>, k_fold_tma<T, true, true, 2, 8, M6>, true);
+        else if (aa)
+          done = tma(k_fold_tma<T, true, false, 4, 4, M6>, k_fold_tma<T, true, false, 8, 3, M3>,
+                     k_fold_tma<T, true, false, 4, 6, M6>, k_fold_tma<T, true, false, 2, 8, M6>, true);
+        else
+          done = tma(k_fold_tma<T, false, false, 4, 4, M6>, k_fold_tma<T, false, false, 8, 3, M3>,
+                     k_fold_tma<T, false, false, 4, 6, M6>, k_fold_tma<T, false, false, 2, 8, M6>,
+                     false);
+        if (done) goto folded;
+      }
       if (sa) {
         if (fv == 4) launch(k_fold_update<T, true, 1, 3, true>);
         else if (fv == 5) launch(k_fold_update_pf<T, true, sizeof(T) == 4 ? 3 : 2, true>);
@@ -1668,6 +1936,7 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
         else if (fv == 5) launch(k_fold_update_pf<T, false, sizeof(T) == 4 ? 4 : 2, false>);
         else launch(k_fold_update<T, false, 1, sizeof(T) == 4 ? 5 : 2>);
       }
+    folded:
       if (seq) {
         T init = *(const T *)ua[4].data;
         k_seq_sum<T><<<1, 32, 0, s>>>(seqbuf, 4LL * ncell, init, result);
@@ -1682,6 +1951,18 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
   return true;
 }
 
+unsigned wait_timeouts(bool reset) {
+  unsigned v = 0;
+  if (!rt().cuda_ready) return 0;
+  OP2B_CUDA(cudaStreamSynchronize(rt().stream));
+  OP2B_CUDA(cudaMemcpyFromSymbol(&v, g_wait_timeouts, sizeof v));
+  if (reset) {
+    const unsigned z = 0;
+    OP2B_CUDA(cudaMemcpyToSymbol(g_wait_timeouts, &z, sizeof z));
+  }
+  return v;
+}
+
 bool run_res_chain(char const *name, op_set rset, const op_arg *ra, op_set bset,
                    const op_arg *ba, const op_arg *ua, const op_arg *aa, const op_arg *sa,
                    void *adt_out, void *save_out, bool flux_done,
@@ -1693,3 +1974,5 @@ bool run_res_chain(char const *name, op_set rset, const op_arg *ra, op_set bset,
 }
 
 }  // namespace op2b
+
+extern "C" unsigned op2b_wait_timeouts(int reset) { return op2b::wait_timeouts(reset != 0); }

@@ -43,6 +43,7 @@ void ensure_cuda() {
   cudaDeviceProp prop;
   OP2B_CUDA(cudaGetDeviceProperties(&prop, R.device));
   R.num_sms = prop.multiProcessorCount;
+  R.smem_optin = (int)prop.sharedMemPerBlockOptin;
   R.device_name = prop.name;
   if (prop.major < 10)
     fail(-1, "op2b error: device %s is sm_%d%d; this library is built for sm_100a\n", prop.name,

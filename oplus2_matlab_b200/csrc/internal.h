@@ -69,6 +69,7 @@ struct Runtime {
   bool gbl_deferred = false;
   int timing = 1;  // 0 off, 1 sampled (every kTimingSample-th call), 2 every call
   int num_sms = 148;
+  int smem_optin = 48 * 1024;  // dynamic shared memory a CTA may opt in to
   std::string device_name;  // queried once per process (the query takes milliseconds)
 
   std::vector<MapDev> maps;  // by op_map index

@@ -161,6 +161,9 @@ def main():
     ap.add_argument("--large", action="store_true")
     ap.add_argument("--only", default="")
     ap.add_argument("--skip-plans", action="store_true")
+    ap.add_argument("--large-plans", action="store_true",
+                    help="plans_large.json: the reference op_plan_core at 720k (part sizes 0, 64, "
+                         "256) and on the 2.88M scrambled mesh (part sizes 0, 256)")
     ap.add_argument("--ref", default=os.environ.get("OP2B_REFERENCE", "/root/reference"),
                     help="the reference tree, from whose sources oracle/_ref is built")
     a = ap.parse_args()
@@ -212,6 +215,18 @@ def main():
                 plans.append(dict(plan_case("jac1_nn%d_res_p%d" % (NN, ps), "res", sets, maps, loops, ps, "jac"),
                                   mesh="jac1_nn%d" % NN))
         json.dump(plans, open(os.path.join(HERE, "plans.json"), "w"), indent=1)
+    if a.large_plans:
+        plans = []
+        for tag, (I, J, scr, parts) in {"400x600": (400, 600, False, (0, 64, 256)),
+                                        "800x1200s": (800, 1200, True, (0, 256))}.items():
+            m = M.naca0012(I, J, scramble=scr)
+            sets, maps, loops = plan_specs_airfoil(m)
+            for loop in ("res_calc", "adt_calc", "bres_calc"):
+                for ps in parts:
+                    print("plan", tag, loop, ps, flush=True)
+                    plans.append(dict(plan_case("%s_%s_p%d" % (tag, loop, ps), loop, sets, maps, loops,
+                                                ps, tag), mesh=tag, mesh_sha256=mesh_hash(m)))
+        json.dump(plans, open(os.path.join(HERE, "plans_large.json"), "w"), indent=1)
     shutil.rmtree(SCRATCH, ignore_errors=True)
 
 
