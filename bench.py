@@ -71,6 +71,12 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-iters", type=int, default=1000)
+    ap.add_argument("--no-forms", action="store_true",
+                    help="plain mode: skip the batched and served measurements that the "
+                         "default line carries")
+    ap.add_argument("--forms-requests", type=int, default=400,
+                    help="plain mode: requests of the served stream at the batched/served "
+                         "workload's 200/s rate (the full workload has 10,000)")
     ap.add_argument("--tune", action="append", default=[],
                     help="kernel-variant knob key=value (op2b_set_tuning)")
     ap.add_argument("--mesh", default="400x600",
@@ -385,6 +391,7 @@ def impl_ours(args, dist):
         A.iteration()
     api.sync()
     assert api.last_error() == "", api.last_error()
+    renumber_s = lib.op2b_renumber_seconds() if args.renumber else None
 
     # one outer iteration as a CUDA graph: a plain one for the timed steps,
     # and one with event nodes around every loop for the per-loop times.
@@ -508,6 +515,19 @@ def impl_ours(args, dist):
     if not args.no_cpu_baseline and dist.rank == 0 and dist.world == 1:
         cpu = cpu_baseline(mesh, args.fp64)
 
+    # the batched and served forms on the same GPU, each with its own clock
+    # record: 64 instances x 500 iterations (the batched workload itself);
+    # the served workload's stream (200 requests/s, stop at 1e-6 x the
+    # first rms or 2000 iterations) shortened to --forms-requests requests;
+    # and a stream at a rate the GPU sustains (20/s) whose looser stopping
+    # test (5% of the first rms) retires small meshes before the cap
+    forms = None
+    if not args.no_forms and dist.world == 1 and not args.fp64 and args.mesh == "400x600":
+        forms = {"batched": measure_batched(args, dist, 64, 500),
+                 "served_200_per_s": measure_served(args, dist, args.forms_requests, 200.0,
+                                                    2000, 1e-6),
+                 "served_20_per_s": measure_served(args, dist, 200, 20.0, 2000, 0.05)}
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
         "steps": args.steps, "warmup": args.warmup,
@@ -515,7 +535,8 @@ def impl_ours(args, dist):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.fp64 else "f32",
         "data": "synthetic: NACA0012 C-mesh from the reference's generator, free-stream start",
         "config": dict(plain_config(mesh.I, mesh.J, mesh_sizes(mesh), args.mesh.endswith("s")),
-                       strategy=args.strategy, renumbered=bool(args.renumber), reduction="tree",
+                       strategy=args.strategy, renumbered=bool(args.renumber),
+                       renumber_seconds=renumber_s, reduction="tree",
                        l2="flushed before every step (untimed read-only sweep of 3x the 126 MB L2)",
                        timing="CUDA events around each graph launch on the library stream",
                        parallelism="replicas" if dist.world > 1 else "single GPU"),
@@ -539,6 +560,26 @@ def impl_ours(args, dist):
         "cpu_baseline": cpu,
         "clocks": clk,
     }
+    if forms:
+        b = forms["batched"]
+        line["batched"] = {"metric": b["metric"], "value": b["value"], "unit": b["unit"],
+                           "plain_back_to_back_solves_per_s":
+                               b["plain_back_to_back"]["solves_per_s"],
+                           "speedup_vs_plain": b["speedup_vs_plain"],
+                           "parity": b["parity_rank0"], "config": b["config"],
+                           "group": b["group"], "gpu_launches": b["gpu_launches"],
+                           "clocks": b["clocks"]}
+        for key in ("served_200_per_s", "served_20_per_s"):
+            v = forms[key]
+            line[key] = {"metric": v["metric"], "value": v["value"], "unit": v["unit"],
+                         "latency": v["latency"], "config": v["config"],
+                         "plain_serial_solves_per_s": v["plain_serial"]["solves_per_s"],
+                         "speedup_vs_plain": v["speedup_vs_plain"],
+                         "retired_by_rms_tolerance": v["retired_by_rms_tolerance"],
+                         "retired_by_iteration_cap": v["retired_by_iteration_cap"],
+                         "iterations": v["iterations"],
+                         "max_active_solves": v["max_active_solves_rank0"],
+                         "plain_serial": v["plain_serial"], "clocks": v["clocks"]}
     if dist.rank == 0:
         print(json.dumps(line))
 
@@ -650,6 +691,18 @@ def free_pinned(keep):
     keep.clear()
 
 
+def gen_meshes(dims):
+    """{(I, J): mesh} for every distinct (I, J) in dims, generated on a pool
+    of host threads (the generator is C++ called through ctypes, which
+    releases the GIL); input preparation, never timed."""
+    import concurrent.futures
+    from oplus2_matlab_b200 import mesh as M
+    want = sorted(set(dims), key=lambda d: -d[0] * d[1])
+    workers = max(1, min(32, (os.cpu_count() or 2) - 1))
+    with concurrent.futures.ThreadPoolExecutor(max_workers=workers) as ex:
+        return dict(zip(want, ex.map(lambda d: M.naca0012(d[0], d[1]), want)))
+
+
 def warm_paths(dt):
     """Untimed: create the CUDA context and load the kernels of both paths
     (lazy module loading) on a tiny mesh, so neither timed region pays the
@@ -667,32 +720,37 @@ def warm_paths(dt):
 
 
 def impl_batched(args, dist):
-    """64 seeded instances (20k-720k cells, Mach 0.3-0.7, alpha -2..6 deg),
-    `iters` iterations each: the group engine (every loop one launch over all
-    instances, edge tile autotuned) against the same instances solved one
-    after another through the plain C API.  Both timed end to end: host
-    arrays in, rms histories and q out; mesh generation (the input) is not
-    timed.  N ranks share the instances by greedy cell balance."""
+    """--mode batched: the batched workload's own JSON line."""
+    line = measure_batched(args, dist, args.instances, args.iters)
+    if dist.rank == 0:
+        print(json.dumps(line))
+
+
+def measure_batched(args, dist, instances, n):
+    """`instances` seeded instances (20k-720k cells, Mach 0.3-0.7, alpha
+    -2..6 deg), n iterations each: the group engine (every loop one launch
+    over all instances, edge tile autotuned) against the same instances
+    solved one after another through the plain C API.  Both timed end to
+    end: host arrays in, rms histories and q out; mesh generation (the
+    input) is not timed.  N ranks share the instances by greedy cell
+    balance.  Returns the measurement as a JSON-able dict."""
     from oplus2_matlab_b200 import group as G
     from oplus2_matlab_b200 import mesh as M
     from oplus2_matlab_b200 import serve as S
     from oplus2_matlab_b200 import api
     dt = np.float64 if args.fp64 else np.float32
-    inst = G.draw_instances(args.instances, cmin=20000, cmax=720000)
+    inst = G.draw_instances(instances, cmin=20000, cmax=720000)
     cells = [3 * I * J for I, J, _, _ in inst]
     mine = S.shard_by_cells(cells, dist.world)[dist.rank]
-    meshes, pins = {}, []
-    for i in mine:
-        I, J = inst[i][:2]
-        if (I, J) not in meshes:
-            meshes[(I, J)] = pinned_mesh(M.naca0012(I, J), pins)
+    pins = []
+    meshes = {k: pinned_mesh(v, pins) for k, v in gen_meshes([inst[i][:2] for i in mine]).items()}
     api.set_error_mode(api.ERRORS_RETURN)
     for kv in args.tune:
         k, v = kv.split("=")
         api.lib().op2b_set_tuning(k.encode(), int(v))
     warm_paths(dt)
-    n = args.iters
 
+    clocks = Clocks(dist.local)
     dist.barrier()
     t0 = time.perf_counter()
     g = G.Group(dt)
@@ -717,6 +775,7 @@ def impl_batched(args, dist):
     t0 = time.perf_counter()
     plain = [G.plain_solve(meshes[inst[i][:2]], inst[i][2], inst[i][3], n, dt) for i in mine]
     t_plain = dist.max(time.perf_counter() - t0)
+    clk = clocks.stop()
 
     exact = sum(int(a.tobytes() == p[0].astype(dt).tobytes()) for a, p in zip(qg, plain))
     rel = max(float(np.max(np.abs(h - p[1]) / np.abs(p[1]))) for h, p in zip(hist, plain))
@@ -754,38 +813,43 @@ def impl_batched(args, dist):
         # list building at admission (6 per solve), autotuner trials (9 of
         # 3 + 1 iterations; the L2-blocked trials launch more per iteration)
         "gpu_launches": 4 * n + 1 + 6 * len(mine) + 9 * 4 * 4,
+        "clocks": clk,
     }
+    return line
+
+
+def impl_served(args, dist):
+    """--mode served: the served workload's own JSON line."""
+    line = measure_served(args, dist, args.requests, args.rate, args.max_iter, args.rel_tol)
     if dist.rank == 0:
         print(json.dumps(line))
 
 
-def impl_served(args, dist):
+def measure_served(args, dist, requests, rate, max_iter, rel_tol):
     """A Poisson request stream (rate, seeded) of meshes of 10k-720k cells,
     each solved until rms < rel_tol x its first rms or max_iter iterations,
     through the continuous-batching server under an HBM budget; p50/p99
     latency from arrival to result and solves/s.  Against: the same
     requests' solves through the plain C API, one after another, timed on a
-    sample and scaled.  Ranks take every N-th request."""
+    sample and scaled.  Ranks take every N-th request.  Returns the
+    measurement as a JSON-able dict."""
     from oplus2_matlab_b200 import group as G
     from oplus2_matlab_b200 import mesh as M
     from oplus2_matlab_b200 import serve as S
     from oplus2_matlab_b200 import api
     dt = np.float64 if args.fp64 else np.float32
-    inst = G.draw_instances(args.requests, seed=M.SEED + 1, cmin=10000, cmax=720000)
+    inst = G.draw_instances(requests, seed=M.SEED + 1, cmin=10000, cmax=720000)
     rng = np.random.default_rng(M.SEED)
-    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, args.requests))
-    mine = list(range(dist.rank, args.requests, dist.world))
-    meshes = {}
-    for i in mine:
-        I, J = inst[i][:2]
-        if (I, J) not in meshes:
-            meshes[(I, J)] = M.naca0012(I, J)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, requests))
+    mine = list(range(dist.rank, requests, dist.world))
+    meshes = gen_meshes([inst[i][:2] for i in mine])
     api.set_error_mode(api.ERRORS_RETURN)
     warm_paths(dt)
     srv = S.Server(dt, budget_bytes=args.budget_gb * 1e9, iters_per_step=args.iters_per_step,
                    max_active=args.max_active, policy=args.policy)
-    reqs = [S.Request(i, meshes[inst[i][:2]], inst[i][2], inst[i][3], args.max_iter,
-                      args.rel_tol, float(arrivals[i])) for i in mine]
+    reqs = [S.Request(i, meshes[inst[i][:2]], inst[i][2], inst[i][3], max_iter,
+                      rel_tol, float(arrivals[i])) for i in mine]
+    clocks = Clocks(dist.local)
     dist.barrier()
     t0 = time.perf_counter()
     srv.clock = lambda: time.perf_counter() - t0
@@ -800,8 +864,10 @@ def impl_served(args, dist):
             continue
         srv.step()
     wall = dist.max(time.perf_counter() - t0)
+    clk = clocks.stop()
     stats = S.latency_stats(srv.done)
     iters = np.array([r.iterations for r in srv.done])
+    by_tol = int(sum(1 for r in srv.done if r.iterations < r.max_iter))
     max_active = srv.peak_active
     srv.close()
 
@@ -815,15 +881,16 @@ def impl_served(args, dist):
         1, sum(r.iterations * r.mesh.ncell for r in srv.done))
     plain_serial_s = t_sample / max(frac, 1e-12)  # the whole stream, scaled by cell-iterations
     line = {
-        "metric": "served airfoil solves/s", "value": args.requests / wall, "unit": "solves/s",
-        "n_gpus": dist.world, "steps": args.requests, "warmup": 0,
-        "ms_per_step": 1e3 * wall / args.requests, "higher_is_better": True,
+        "metric": "served airfoil solves/s", "value": requests / wall, "unit": "solves/s",
+        "n_gpus": dist.world, "steps": requests, "warmup": 0,
+        "ms_per_step": 1e3 * wall / requests, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f64" if args.fp64 else "f32",
         "data": "synthetic: Poisson(%g/s) arrivals, seeded NACA0012 meshes 10k-720k cells, "
-                "Mach U[0.3,0.7], alpha U[-2,6] deg" % args.rate,
+                "Mach U[0.3,0.7], alpha U[-2,6] deg" % rate,
         "config": {"workload": "airfoil served: %d requests, stop at rms < %g x first or %d "
-                               "iterations, %g GB budget" % (args.requests, args.rel_tol,
-                                                              args.max_iter, args.budget_gb),
+                               "iterations, %g GB budget" % (requests, rel_tol,
+                                                              max_iter, args.budget_gb),
+                   "rate_per_s": rate,
                    "iters_per_step": args.iters_per_step, "policy": args.policy,
                    "max_active": args.max_active,
                    "parallelism": "requests dealt round-robin over %d GPU(s)" % dist.world},
@@ -832,14 +899,15 @@ def impl_served(args, dist):
         "iterations": {"mean": float(iters.mean()), "min": int(iters.min()),
                        "max": int(iters.max())},
         "max_active_solves_rank0": max_active,
+        "retired_by_rms_tolerance": by_tol, "retired_by_iteration_cap": len(srv.done) - by_tol,
         "plain_serial": {"sample": len(sample), "sample_seconds": t_sample,
                          "estimated_seconds": plain_serial_s,
-                         "solves_per_s": args.requests / plain_serial_s,
+                         "solves_per_s": requests / plain_serial_s,
                          "scaled_by": "cell-iterations of the sample over the stream"},
         "speedup_vs_plain": plain_serial_s / wall,
+        "clocks": clk,
     }
-    if dist.rank == 0:
-        print(json.dumps(line))
+    return line
 
 
 def run_reference_jac(NN, niter, threads=None):

@@ -46,6 +46,27 @@ enum { OP2B_REDUCE_TREE = 0, OP2B_REDUCE_SEQ = 1 };
  *                   thread in the per-element GATHER kernel (1, 2, 4)
  *   "unroll"        elements per thread in the direct loops (1, 2, 4) */
 int op2b_set_tuning(const char *key, int value);
+/* The value of a tuning knob, or `def` when it is unset. */
+int op2b_get_tuning(const char *key, int def);
+
+/* Autotuner for the launch shapes of the airfoil res_calc chain
+ * (res_calc + bres_calc + update + adt_calc), the choice the reference
+ * leaves to compile-time OP_PART_SIZE / OP_BLOCK_SIZE macros
+ * (airfoil/res_calc_kernel.cu:181-204, common/op_lib_core.c:663-673).  Call
+ * it after one outer iteration has run through the loop API.  If
+ * `cache_path` (may be NULL) holds an entry for this device, real type and
+ * mesh (set sizes), its knobs are applied and 1 is returned.  Otherwise
+ * every candidate -- the persistent one-launch chain at several flux tile
+ * sizes, cells per thread and queue lags, and the two-launch chain with its
+ * per-cell pass variants -- is timed for `iters` launches (each after an L2
+ * flush) on the app's own data, which is saved first and put back after
+ * each candidate; the fastest is applied, appended to the cache file, and 0
+ * is returned.  All these candidates leave every field bit-identical; only
+ * the order of the TREE rms sum follows the launch shape.  allow_reorder
+ * != 0 also times COLOURED (the reference's colouring scheme) at part sizes
+ * 64..512, whose fields differ from op_seq.h's in the last bits.  -1 on
+ * error (no chain has run, captured graphs exist).  Synchronises. */
+int op2b_autotune(const char *cache_path, int iters, int allow_reorder);
 
 /* Renumber every set for locality of the indirect gathers (off by default).
  * Call before the first loop; the first loop call then orders the sets
@@ -57,10 +78,13 @@ int op2b_set_tuning(const char *key, int value);
  * sets, and TREE-mode global sums are summed in another order.  Returns 0,
  * or -1 when turning it off after it has been applied. */
 int op2b_set_renumber(int on);
-/* The new -> old order renumbering would give `set` (computed from the sets
- * and maps declared so far; host only).  Returns 1 if the set is reordered,
+/* The new -> old order renumbering would give `set` (computed on the GPU from
+ * the sets and maps declared so far).  Returns 1 if the set is reordered,
  * 0 if it keeps its numbering (new2old = identity), -1 on bad arguments. */
 int op2b_renumber_order(op_set set, int *new2old);
+/* Seconds the renumbering took at the first loop call (orders computed on
+ * the GPU, maps and datasets moved), 0 before it.  No reference counterpart. */
+double op2b_renumber_seconds(void);
 
 /* Checkpointing (doc/dev.tex:1080-1087 proposes it; the reference has no
  * implementation).  op2b_checkpoint_file(path) names the checkpoint file;

@@ -128,11 +128,14 @@ PROTOTYPES = [
     ("op2b_l2_flush", C.c_int, []),
     ("op2b_wait_timeouts", C.c_uint, [C.c_int]),
     ("op2b_set_tuning", C.c_int, [C.c_char_p, C.c_int]),
+    ("op2b_get_tuning", C.c_int, [C.c_char_p, C.c_int]),
+    ("op2b_autotune", C.c_int, [C.c_char_p, C.c_int, C.c_int]),
     ("op2b_update_noalloc", C.c_int, [C.c_int, _P, _P, _P, _P, _P, _P]),
     ("op2b_set_renumber", C.c_int, [C.c_int]),
     ("op2b_checkpoint_file", C.c_int, [C.c_char_p]),
     ("op_checkpoint", C.c_int, []),
     ("op2b_renumber_order", C.c_int, [op_set, C.POINTER(C.c_int)]),
+    ("op2b_renumber_seconds", C.c_double, []),
     ("op2b_decl_const_named", None, [C.c_int, C.c_char_p, C.c_int, _P, C.c_char_p]),
     ("op2b_capture_begin", C.c_int, [C.c_int]),
     ("op2b_capture_end", _P, []),

@@ -708,214 +708,222 @@ __global__ void __launch_bounds__(256, MINB)
   grid_finish<T, OpSum, OpSum, 1>(v, id, OpSum(), OpSum(), sl, ticket);
 }
 
-// The per-cell pass (ordered fold + update [+ adt_calc] [+ save_soln]) with
-// its contiguous streams staged by the TMA engine.  One warp produces, NC
-// warps consume; a tile is TC = 32 NC consecutive cells, one per consumer
-// thread.  For every tile the producer's elected lane issues one
-// cp.async.bulk per array -- the cells' list entries, pcell rows (the
-// first hop of the gathers: plan and map data, issued before the PDL wait
-// for the first S tiles), res, qold, adt -- into one of S shared-memory
-// stages, completing on the stage's "full" mbarrier.  The consumers take
-// each cell's list and node indices and its res, qold, adt from the stage,
-// hand the stage back ("empty" barrier) as soon as they hold it in
-// registers, gather the listed flux values and the nodes' x (L2), and do
-// the arithmetic of k_fold_update in the same order, so q, res, adt, qold
-// are bit-identical to it.  So the streams of S tiles are in flight per
-// CTA without costing the consumers registers or issue slots.
+// --------------------------------------------- persistent res_calc chain ----
+// res_calc + bres_calc + update [+ adt_calc] [+ save_soln] as ONE persistent
+// launch over a static queue of work items: flux tiles (ET consecutive
+// entries of the flux index space -- res_calc's edges, then bres_calc's
+// boundary edges) and cell tiles (CT consecutive cells: ordered fold of the
+// cells' lists, update, adt_calc, save_soln).  Each CTA takes the next item
+// with an atomic counter, so issue-bound flux tiles and latency-bound cell
+// tiles run side by side on every SM instead of one pass after the other.
 //
-// Cells are split into one balanced contiguous range per CTA (a multiple of
-// 4 cells, so every tile's copies start 16-byte aligned); a tile's copy
-// sizes are rounded down to 16 bytes and the consumers load the few
-// trailing elements past them from global memory.  Each thread folds its
-// del^2 over its cells in tile order, so the TREE sum depends only on the
-// cell count and the grid.  Waits are bounded (tma.cuh): a wait that runs
-// out is counted, its warp skips the remaining tiles, and before the CTA
-// returns its producer waits, bounded again, for copies still in flight.
-template <class T, bool ADT, bool SAVE, int NC, int S, int MINB>
-__global__ void __launch_bounds__((NC + 1) * 32, MINB)
-    k_fold_tma(int n, int chunk, int W, const int *__restrict__ ell, const T *__restrict__ vals,
-               const T *qold, T *q, T *res, const T *adt, const int4 *__restrict__ pcell,
-               const T *__restrict__ x0, const T *__restrict__ x1, const T *__restrict__ x2,
-               const T *__restrict__ x3, AirConsts<T> K, T *seq, RedSlot<T> slot,
-               unsigned *ticket, T *qsave, T *adt_out) {
-  constexpr int TC = NC * 32;
-  extern __shared__ __align__(128) unsigned char stage_mem[];
-  __shared__ __align__(8) unsigned long long full[S], empty[S];
-  __shared__ int timed_out;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int cb = (int)min((long long)n, (long long)blockIdx.x * chunk);
-  const int ce = (int)min((long long)n, (long long)cb + chunk);
-  const int ntile = (ce - cb + TC - 1) / TC;
-  // stage layout: list entries | pcell rows | res | qold | adt
-  const unsigned ell_b = ((unsigned)(TC * W * 4) + 15u) & ~15u;
-  const unsigned nd_b = ADT ? TC * 16u : 0u;
-  const unsigned v4_b = TC * 4u * sizeof(T);
-  const unsigned adt_b = ((unsigned)(TC * sizeof(T)) + 15u) & ~15u;
-  const unsigned stage_b = ell_b + nd_b + 2u * v4_b + adt_b;
-  if (threadIdx.x == 0) {
-    timed_out = 0;
-    for (int i = 0; i < S; i++) {
-      mbar_init(smem_addr(&full[i]), 1);
-      mbar_init(smem_addr(&empty[i]), NC);
-    }
-    mbar_init_fence();
-  }
-  __syncthreads();
-  T rms = T(0);
-  if (warp == NC) {  // ------------------------------------------ producer
-    if (lane == 0) {
-      // bytes of tile t's copies: each array's size rounded down to 16
-      auto sizes = [&](int t, unsigned (&b)[5]) {
-        const int nct = min(TC, ce - (cb + t * TC));
-        b[0] = (unsigned)(nct * W * 4) & ~15u;
-        b[1] = ADT ? nct * 16u : 0u;
-        b[2] = b[3] = nct * 4u * sizeof(T);
-        b[4] = (unsigned)(nct * sizeof(T)) & ~15u;
-      };
-      auto issue = [&](int t, bool plan_part, bool data_part) {
-        unsigned b[5];
-        sizes(t, b);
-        const int c0 = cb + t * TC;
-        const uint32_t st = smem_addr(stage_mem + (size_t)(t % S) * stage_b);
-        const uint32_t bar = smem_addr(&full[t % S]);
-        if (plan_part) {
-          if (b[0]) bulk_load(st, ell + (size_t)c0 * W, b[0], bar);
-          if (ADT) bulk_load(st + ell_b, pcell + c0, b[1], bar);
-        }
-        if (data_part) {
-          bulk_load(st + ell_b + nd_b, res + 4 * (size_t)c0, b[2], bar);
-          bulk_load(st + ell_b + nd_b + v4_b, qold + 4 * (size_t)c0, b[3], bar);
-          if (b[4]) bulk_load(st + ell_b + nd_b + 2 * v4_b, adt + c0, b[4], bar);
-        }
-      };
-      auto arm = [&](int t) {
-        unsigned b[5];
-        sizes(t, b);
-        mbar_arrive_expect_tx(smem_addr(&full[t % S]), b[0] + b[1] + b[2] + b[3] + b[4]);
-      };
-      const int pre = min(ntile, S);
-      for (int t = 0; t < pre; t++) {  // plan and map data: no kernel writes them
-        arm(t);
-        issue(t, true, false);
-      }
-      pdl_wait();
-      for (int t = 0; t < pre; t++) issue(t, false, true);
-      for (int t = S; t < ntile; t++) {
-        if (!mbar_wait(smem_addr(&empty[t % S]), (unsigned)((t / S - 1) & 1))) {
-          timed_out = 1;
-          break;
-        }
-        arm(t);
-        issue(t, true, true);
-      }
-    } else {
-      pdl_wait();
-    }
-    __syncwarp();
-    pdl_trigger();
-  } else {  // ----------------------------------------------------- consumers
-    pdl_wait();
-    pdl_trigger();
-    const int i = warp * 32 + lane;  // this thread's cell within a tile
-    for (int t = 0; t < ntile; t++) {
-      const int sidx = t % S;
-      if (!mbar_wait(smem_addr(&full[sidx]), (unsigned)((t / S) & 1))) {
-        timed_out = 1;
-        break;
-      }
-      const unsigned char *st = stage_mem + (size_t)sidx * stage_b;
-      const int c0 = cb + t * TC, c = c0 + i;
-      const int nct = min(TC, ce - c0);
-      int k[4] = {-1, -1, -1, -1}, nd[4] = {0, 0, 0, 0};
-      T r[4], qo[4], ad = T(1);
-      if (i < nct) {
-        const unsigned ell_copied = (unsigned)(nct * W * 4) & ~15u;
-        if ((unsigned)((i + 1) * W * 4) <= ell_copied) {
-          const int *e = reinterpret_cast<const int *>(st) + i * W;
-          if ((W & 3) == 0) {
-            const int4 kk = *reinterpret_cast<const int4 *>(e);
-            k[0] = kk.x; k[1] = kk.y; k[2] = kk.z; k[3] = kk.w;
-          } else {
-#pragma unroll
-            for (int j = 0; j < 4; j++) k[j] = j < W ? e[j] : -1;
-          }
-        } else {
-          list_head(ell, W, c, k);
-        }
-        if (ADT) {
-          const int4 v = reinterpret_cast<const int4 *>(st + ell_b)[i];
-          nd[0] = v.x; nd[1] = v.y; nd[2] = v.z; nd[3] = v.w;
-        }
-        ldw4(reinterpret_cast<const T *>(st + ell_b + nd_b) + 4 * i, r);
-        ldw4(reinterpret_cast<const T *>(st + ell_b + nd_b + v4_b) + 4 * i, qo);
-        const unsigned adt_copied = (unsigned)(nct * sizeof(T)) & ~15u;
-        ad = (unsigned)((i + 1) * sizeof(T)) <= adt_copied
-                 ? reinterpret_cast<const T *>(st + ell_b + nd_b + 2 * v4_b)[i]
-                 : adt[c];
-      }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(smem_addr(&empty[sidx]));  // the stage is free again
-      if (i >= nct) continue;
-      T f[4][4], xs[4][2];
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-        if (k[j] >= 0) ld4(vals + 4 * (size_t)(k[j] >> 1), f[j]);
-      if (ADT) {
-        ld2(x0 + 2 * (size_t)nd[0], xs[0]);
-        ld2(x1 + 2 * (size_t)nd[1], xs[1]);
-        ld2(x2 + 2 * (size_t)nd[2], xs[2]);
-        ld2(x3 + 2 * (size_t)nd[3], xs[3]);
-      }
-#pragma unroll
-      for (int j = 0; j < 4; j++) add_listed(r, k[j], f[j]);
-      for (int j = 4; j < W; j++) {  // lists longer than 4
-        const int kk = __ldg(ell + (size_t)c * W + j);
-        T g[4];
-        ld4(vals + 4 * (size_t)(kk >> 1), g);
-        add_listed(r, kk, g);
-      }
-      // airfoil/update.h:1-12
-      T adti = rcp(ad);
-      T qn[4], sq[4];
-      for (int d = 0; d < 4; d++) {
-        T del = adti * r[d];
-        qn[d] = qo[d] - del;
-        sq[d] = del * del;
-        rms += sq[d];
-      }
-      st4(q + 4 * (size_t)c, qn);
-      if (SAVE) st4(qsave + 4 * (size_t)c, qn);  // airfoil/save_soln.h:1-3
-      const T z[4] = {T(0), T(0), T(0), T(0)};
-      st4(res + 4 * (size_t)c, z);
-      if (seq) st4(seq + 4 * (size_t)c, sq);
-      if (ADT) adt_out[c] = adt_calc(xs[0], xs[1], xs[2], xs[3], qn, K);
-    }
-  }
-  __syncthreads();
-  if (timed_out && threadIdx.x == NC * 32) {
-    // copies may still be in flight into this CTA's stages: wait for the
-    // last phase of every stage (bounded) before the CTA's memory goes
-    for (int sidx = 0; sidx < S && sidx < ntile; sidx++) {
-      const int last = sidx + ((ntile - 1 - sidx) / S) * S;
-      mbar_wait(smem_addr(&full[sidx]), (unsigned)((last / S) & 1));
-    }
-  }
-  if (seq) return;
-  const T v[1] = {rms}, id[1] = {T(0)};
-  RedSlot<T> sl[1] = {slot};
-  grid_finish<T, OpSum, OpSum, 1>(v, id, OpSum(), OpSum(), sl, ticket);
+// A cell tile may start only when the flux tiles its lists read (at most
+// kChainMaxDeps distinct ones, listed per cell tile at plan time) are done.
+// The queue places each cell tile `lag` flux tiles after the last of them.
+// A flux tile publishes completion with an epoch-tagged flag (block barrier,
+// then a release store by one thread); a CTA about to fold checks its tile's
+// flags with one warp, one flag per lane (acquire loads, in parallel), and
+// a block barrier passes the result on.  Items are taken in queue
+// order and a cell tile waits only on items taken before it, which belong
+// to CTAs that are running (or hold them next, behind an item that waits on
+// still earlier ones): the waits always end.  They are bounded all the same
+// (one second, then counted in op2b_wait_timeouts and skipped).
+//
+// The same dependency covers the chain's write-after-read hazards: a flux
+// tile reads q and adt of the cells of its edges, and every such edge is in
+// those cells' lists, so no cell's q or adt is overwritten before the last
+// flux value that reads it has been computed.  Values written by other CTAs
+// of this launch are read through L2 (ld.global.cg).
+//
+// The arithmetic and its order per cell and per edge are those of
+// k_res_flux_pair and k_fold_update: q, res, adt, qold are bit-identical.
+// The rms: each cell tile's partial (its threads' sums, block tree) goes to
+// partials[tile]; the last CTA folds them in tile order.
+struct ChainSchedDev {
+  const int *queue;    // [nitems]: >= 0 flux tile, < 0 cell tile -(t + 1)
+  const int *dep_off;  // [ncell_tiles + 1]: a cell tile's flux tiles are
+  const int *deps;     //   deps[dep_off[t], dep_off[t+1]) (distinct, <= 64)
+  unsigned *flags;     // [nflux_tiles]: epoch of the last launch that wrote it
+  unsigned *ctl;       // next item, (unused), finish ticket, epoch
+  void *partials;      // [ncell_tiles] rms partials (8-byte slots)
+  int nitems, nflux, ncellt, et, ct;
+};
+constexpr int kChainMaxDeps = 64;  // flux tiles one cell tile may wait for
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned *p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// L2-coherent vector loads of values written by other CTAs of this launch
+__device__ __forceinline__ void ld4cg(const float *p, float v[4]) {
+  float4 t = __ldcg(reinterpret_cast<const float4 *>(p));
+  v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void ld4cg(const double *p, double v[4]) {
+  double2 a = __ldcg(reinterpret_cast<const double2 *>(p));
+  double2 b = __ldcg(reinterpret_cast<const double2 *>(p) + 1);
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 
-// shared memory of one k_fold_tma CTA: S stages for list width W
-template <class T, bool ADT, int NC, int S>
-inline size_t fold_tma_smem(int W) {
-  const size_t TC = NC * 32;
-  const size_t ell_b = (TC * W * 4 + 15) & ~(size_t)15;
-  const size_t nd_b = ADT ? TC * 16 : 0;
-  const size_t v4_b = TC * 4 * sizeof(T);
-  const size_t adt_b = (TC * sizeof(T) + 15) & ~(size_t)15;
-  return S * (ell_b + nd_b + 2 * v4_b + adt_b);
+template <class T, bool ADT, bool SAVE, int U>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
+    k_chain_persist(ChainSchedDev S, int ne, const int2 *__restrict__ pedge,
+                    const int2 *__restrict__ pecell, const T *__restrict__ x,
+                    const T *__restrict__ qf, const T *__restrict__ adtf, BresEdges<T> B,
+                    T *vals, int n, const int *__restrict__ ell, int W, const T *qold, T *q,
+                    T *res, const T *adt, CellNodes N, const T *__restrict__ x0,
+                    const T *__restrict__ x1, const T *__restrict__ x2,
+                    const T *__restrict__ x3, AirConsts<T> K, T *seq, T *result, T *qsave,
+                    T *adt_out) {
+  __shared__ int s_item[2];
+  __shared__ T ws[32];
+  __shared__ bool last;
+  const int tid = threadIdx.x;
+  pdl_wait();
+  pdl_trigger();
+  const unsigned ep = ld_acquire(S.ctl + 3) + 1u;
+  T *partials = reinterpret_cast<T *>(S.partials);
+  const unsigned total = (unsigned)ne + (unsigned)B.n;
+  if (tid == 0) s_item[0] = (int)atomicAdd(S.ctl, 1u);
+  __syncthreads();
+  for (int par = 0;; par ^= 1) {
+    const int it = s_item[par];
+    if (it >= S.nitems) break;
+    if (tid == 0) s_item[par ^ 1] = (int)atomicAdd(S.ctl, 1u);  // in flight meanwhile
+    const int code = __ldg(S.queue + it);
+    if (code >= 0) {  // ------------------------------------- flux tile
+      const unsigned e0 = (unsigned)code * (unsigned)S.et;
+      const unsigned e1 = min(total, e0 + (unsigned)S.et);
+      for (unsigned i = e0 + tid; i < e1; i += 256) {
+        T f[4];
+        if (i < (unsigned)ne) {
+          const int2 nn = __ldg(pedge + i), cc = __ldg(pecell + i);
+          T p[2], s2[2], q1[4], q2[4];
+          ld4(qf + 4u * (unsigned)cc.x, q1);
+          ld4(qf + 4u * (unsigned)cc.y, q2);
+          ld2(x + 2u * (unsigned)nn.x, p);
+          ld2(x + 2u * (unsigned)nn.y, s2);
+          const T d1 = __ldg(adtf + (unsigned)cc.x), d2 = __ldg(adtf + (unsigned)cc.y);
+          res_flux(p, s2, q1, q2, d1, d2, K.gm1, K.eps, f);
+        } else {
+          const int b = (int)(i - (unsigned)ne);
+          int m1, m2;
+          at2(B.x1, B.x2, b, m1, m2);
+          T p[2], s2[2], q1[4];
+          ld2(B.xa + 2 * (size_t)m1, p);
+          ld2(B.xb + 2 * (size_t)m2, s2);
+          ld4(B.q_d + 4 * (size_t)at(B.q, b), q1);
+          const T b1 = __ldg(B.adt + at(B.a, b));
+          bres_contrib(p, s2, q1, b1, __ldg(B.bound_d + at(B.bound, b)), K, f);
+        }
+        st4(vals + 4u * i, f);
+      }
+      __syncthreads();  // the tile's values are written
+      if (tid == 0) st_release(S.flags + code, ep);
+    } else {  // ---------------------------------------------- cell tile
+      const int t = -code - 1;
+      if (tid < 32) {  // one warp checks the tile's flux tiles, a flag per lane
+        const int d0 = __ldg(S.dep_off + t), d1 = __ldg(S.dep_off + t + 1);
+        const int ja = d0 + tid < d1 ? __ldg(S.deps + d0 + tid) : -1;
+        const int jb = d0 + tid + 32 < d1 ? __ldg(S.deps + d0 + tid + 32) : -1;
+        bool da = ja < 0 || ld_acquire(S.flags + ja) == ep;
+        bool db = jb < 0 || ld_acquire(S.flags + jb) == ep;
+        if (!__all_sync(0xffffffffu, da && db)) {
+          const unsigned long long t0 = global_ns();
+          for (;;) {
+            __nanosleep(100);
+            if (!da) da = ld_acquire(S.flags + ja) == ep;
+            if (!db) db = ld_acquire(S.flags + jb) == ep;
+            if (__all_sync(0xffffffffu, da && db)) break;
+            if (global_ns() - t0 > kWaitLimitNs) {  // give up: counted, results wrong
+              if (tid == 0) atomicAdd(&g_wait_timeouts, 1u);
+              break;
+            }
+          }
+        }
+      }
+      __syncthreads();
+      T rms = T(0);
+      const int c0 = t * S.ct;
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int c = c0 + u * 256 + tid;
+        if (c >= n || u * 256 >= S.ct) continue;
+        int k[4];
+        list_head(ell, W, c, k);
+        int nd[4] = {0, 0, 0, 0};
+        if (ADT) {
+          const int4 v = __ldg(reinterpret_cast<const int4 *>(N.m0.map) + c);
+          nd[0] = v.x; nd[1] = v.y; nd[2] = v.z; nd[3] = v.w;
+        }
+        T r[4], qo[4], f[4][4], xs[4][2];
+        ldw4(res + 4 * (size_t)c, r);
+        if (SAVE) ldw4(qold + 4 * (size_t)c, qo);
+        else ld4(qold + 4 * (size_t)c, qo);
+        const T ad = adt[c];
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          if (k[j] >= 0) ld4cg(vals + 4 * (size_t)(k[j] >> 1), f[j]);
+        if (ADT) {
+          ld2(x0 + 2 * (size_t)nd[0], xs[0]);
+          ld2(x1 + 2 * (size_t)nd[1], xs[1]);
+          ld2(x2 + 2 * (size_t)nd[2], xs[2]);
+          ld2(x3 + 2 * (size_t)nd[3], xs[3]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) add_listed(r, k[j], f[j]);
+        for (int j = 4; j < W; j++) {  // lists longer than 4
+          const int kk = __ldg(ell + (size_t)c * W + j);
+          T g[4];
+          ld4cg(vals + 4 * (size_t)(kk >> 1), g);
+          add_listed(r, kk, g);
+        }
+        // airfoil/update.h:1-12
+        T adti = rcp(ad);
+        T qn[4], sq[4];
+        for (int d = 0; d < 4; d++) {
+          T del = adti * r[d];
+          qn[d] = qo[d] - del;
+          sq[d] = del * del;
+          rms += sq[d];
+        }
+        st4(q + 4 * (size_t)c, qn);
+        if (SAVE) st4(qsave + 4 * (size_t)c, qn);  // airfoil/save_soln.h:1-3
+        const T z[4] = {T(0), T(0), T(0), T(0)};
+        st4(res + 4 * (size_t)c, z);
+        if (seq) st4(seq + 4 * (size_t)c, sq);
+        if (ADT) adt_out[c] = adt_calc(xs[0], xs[1], xs[2], xs[3], qn, K);
+      }
+      const T b = block_fold(rms, T(0), OpSum(), ws);
+      if (tid == 0) partials[t] = b;
+    }
+    __syncthreads();  // s_item[par ^ 1] is set; everyone has read s_item[par]
+  }
+  // the last CTA to finish folds the cell tiles' partials in tile order and
+  // re-arms the queue for the next launch
+  if (tid == 0) {
+    __threadfence();
+    last = atomicAdd(S.ctl + 2, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  T xsum = T(0);
+  for (int k = tid; k < S.ncellt; k += 256) xsum += __ldcg(partials + k);
+  xsum = block_fold(xsum, T(0), OpSum(), ws);
+  if (tid == 0) {
+    if (!seq) *result = xsum;
+    S.ctl[0] = 0u;
+    S.ctl[2] = 0u;
+    __threadfence();
+    st_release(S.ctl + 3, ep);
+  }
 }
+
 
 template <class T>
 __global__ void k_fill(T *p, size_t n, T v) {
@@ -1696,6 +1704,128 @@ static void launch_flux(const op_arg *ra, const ResEdges<T> &E, const BresEdges<
     launch_pdl(k_res_flux_list<T, false, sizeof(T) == 4 ? 8 : 4>, fgrid, 256, 0, s, E, B, vals, K);
 }
 
+// the persistent chain's queue for a slot plan (host side of ChainSchedDev)
+struct ChainSched {
+  int et = 0, ct = 0, lag = 0;
+  ChainSchedDev dev;
+};
+
+void release_chain_sched(SlotPlan *sp) {
+  if (!sp->chain) return;
+  ChainSchedDev &d = sp->chain->dev;
+  dev_free((void *)d.queue);
+  dev_free((void *)d.dep_off);
+  dev_free((void *)d.deps);
+  dev_free(d.flags);
+  dev_free(d.ctl);
+  dev_free(d.partials);
+  delete sp->chain;
+  sp->chain = nullptr;
+}
+
+// Build (once per slot plan and tile shape) the work queue: flux tiles in
+// order, each cell tile `lag` flux tiles after the last flux tile its lists
+// read, and each cell tile's distinct flux tiles.  Reads the lists back to
+// the host, so it runs on a loop's first call, before any capture; nullptr
+// when it cannot be built or some cell tile reads more than kChainMaxDeps
+// flux tiles (a numbering without locality: the caller then uses the
+// two-launch chain).
+static ChainSched *chain_sched(SlotPlan *sp, int et, int ct, int lag) {
+  if (sp->chain && sp->chain->et == et && sp->chain->ct == ct && sp->chain->lag == lag)
+    return sp->chain;
+  if (sp->chain_unsuited) return nullptr;
+  if (live_graphs() > 0 && sp->chain) return sp->chain;  // keep what captured graphs use
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  OP2B_CUDA(cudaStreamIsCapturing(rt().stream, &cap));
+  if (cap != cudaStreamCaptureStatusNone) return sp->chain;
+  release_chain_sched(sp);
+  cudaStream_t s = rt().stream;
+  const int nvals = sp->na + sp->nb, ncell = sp->ntarget, W = sp->width;
+  const int nflux = (nvals + et - 1) / et, ncellt = (ncell + ct - 1) / ct;
+  if (nflux < 1 || ncellt < 1) return nullptr;
+  std::vector<int> ell((size_t)ncell * W);
+  OP2B_CUDA(cudaMemcpyAsync(ell.data(), sp->d_ell, sizeof(int) * ell.size(),
+                            cudaMemcpyDeviceToHost, s));
+  OP2B_CUDA(cudaStreamSynchronize(s));
+  std::vector<int> dep_off(ncellt + 1, 0), deps, last(ncellt, -1), tiles;
+  for (int t = 0; t < ncellt; t++) {
+    tiles.clear();
+    const int c1 = std::min(ncell, (t + 1) * ct);
+    for (size_t e = (size_t)t * ct * W; e < (size_t)c1 * W; e++) {
+      const int v = ell[e] >> 1;
+      if (v < nvals) tiles.push_back(v / et);
+    }
+    std::sort(tiles.begin(), tiles.end());
+    tiles.erase(std::unique(tiles.begin(), tiles.end()), tiles.end());
+    if ((int)tiles.size() > kChainMaxDeps) {
+      sp->chain_unsuited = true;
+      return nullptr;
+    }
+    deps.insert(deps.end(), tiles.begin(), tiles.end());
+    dep_off[t + 1] = (int)deps.size();
+    if (!tiles.empty()) last[t] = tiles.back();
+  }
+  // cell tiles by the flux tile after which they are queued (stable)
+  std::vector<std::vector<int>> after(nflux);
+  for (int t = 0; t < ncellt; t++)
+    after[std::min(nflux - 1, std::max(last[t], 0) + lag)].push_back(t);
+  std::vector<int> queue;
+  queue.reserve((size_t)nflux + ncellt);
+  for (int j = 0; j < nflux; j++) {
+    queue.push_back(j);
+    for (int t : after[j]) queue.push_back(-(t + 1));
+  }
+  ChainSched *cs = new ChainSched();
+  cs->et = et;
+  cs->ct = ct;
+  cs->lag = lag;
+  ChainSchedDev &d = cs->dev;
+  d.nitems = (int)queue.size();
+  d.nflux = nflux;
+  d.ncellt = ncellt;
+  d.et = et;
+  d.ct = ct;
+  int *d_queue = (int *)dev_alloc(sizeof(int) * queue.size());
+  int *d_off = (int *)dev_alloc(sizeof(int) * dep_off.size());
+  int *d_deps = (int *)dev_alloc(sizeof(int) * std::max<size_t>(1, deps.size()));
+  d.queue = d_queue;
+  d.dep_off = d_off;
+  d.deps = d_deps;
+  d.flags = (unsigned *)dev_alloc(sizeof(unsigned) * (size_t)nflux);
+  d.ctl = (unsigned *)dev_alloc(4 * sizeof(unsigned));
+  d.partials = dev_alloc(8 * (size_t)ncellt);
+  sp->chain = cs;
+  if (!d_queue || !d_off || !d_deps || !d.flags || !d.ctl || !d.partials) {
+    release_chain_sched(sp);
+    return nullptr;
+  }
+  OP2B_CUDA(cudaMemcpyAsync(d_queue, queue.data(), sizeof(int) * queue.size(),
+                            cudaMemcpyHostToDevice, s));
+  OP2B_CUDA(cudaMemcpyAsync(d_off, dep_off.data(), sizeof(int) * dep_off.size(),
+                            cudaMemcpyHostToDevice, s));
+  if (!deps.empty())
+    OP2B_CUDA(cudaMemcpyAsync(d_deps, deps.data(), sizeof(int) * deps.size(),
+                              cudaMemcpyHostToDevice, s));
+  OP2B_CUDA(cudaMemsetAsync(d.flags, 0, sizeof(unsigned) * (size_t)nflux, s));
+  OP2B_CUDA(cudaMemsetAsync(d.ctl, 0, 4 * sizeof(unsigned), s));
+  OP2B_CUDA(cudaStreamSynchronize(s));  // the host vectors go out of scope
+  return cs;
+}
+
+// res_calc's arguments in the airfoil shape: both x through one dim-2 map
+// (idx 0, 1), q and adt through another, one dataset each, sizes that keep
+// 32-bit index arithmetic
+static bool flux_pair_shape(const op_arg *ra, size_t nval) {
+  auto pair = [](const op_arg &a, const op_arg &b) {
+    return a.map && a.map == b.map && a.map->dim == 2 && a.idx == 0 && b.idx == 1;
+  };
+  return pair(ra[0], ra[1]) && pair(ra[2], ra[3]) && pair(ra[4], ra[5]) &&
+         ra[2].map == ra[4].map && ra[0].dat == ra[1].dat && ra[2].dat == ra[3].dat &&
+         ra[4].dat == ra[5].dat && (long long)nval < (1LL << 30) &&
+         (long long)ra[2].dat->set->size < (1LL << 30) &&
+         (long long)ra[0].dat->set->size < (1LL << 30);
+}
+
 // the plans and value buffer of a res_calc (+ bres_calc) chain; nullptr
 // when the mesh does not suit slots; *err when a plan failed
 template <class T>
@@ -1777,6 +1907,79 @@ bool run_res_flux_ahead(op_set rset, const op_arg *ra, op_set bset, const op_arg
 // res_calc [+ bres_calc [+ update [+ adt_calc]]] over contribution lists:
 // the flux pass, then one per-cell pass that folds the cell's list and, when
 // update follows, applies it (and adt_calc) to the cell before storing
+// res_calc + bres_calc + update [+ adt_calc] [+ save_soln] as one persistent
+// launch (k_chain_persist); false when the shapes do not suit it (the
+// caller then runs the flux pass and the per-cell pass)
+template <class T>
+static bool persist_chain(const std::string &name, SlotPlan *sp, const op_arg *ra,
+                          const ResEdges<T> &E, const BresEdges<T> &B, const op_arg *ua,
+                          const op_arg *aa, const op_arg *sa, void *adt_out, void *save_out,
+                          const AirConsts<T> &K, bool seq, int rslot_id, cudaStream_t s) {
+  const size_t nval = (size_t)sp->na + sp->nb + 1;
+  if (!tuning("chain_persist", 0) || !flux_pair_shape(ra, nval)) return false;
+  if (aa && !(aa[0].map && aa[0].map == aa[1].map && aa[0].map == aa[2].map &&
+              aa[0].map == aa[3].map && aa[0].map->dim == 4 && aa[0].idx == 0 &&
+              aa[1].idx == 1 && aa[2].idx == 2 && aa[3].idx == 3))
+    return false;
+  const int U = tuning("persist_u", 1) == 2 ? 2 : 1;
+  const int et = std::max(256, tuning("persist_et", 1024));
+  const bool adt_calc_on = aa != nullptr, save_on = sa != nullptr;
+  const void *kp;
+  if (save_on)
+    kp = U == 2 ? (const void *)k_chain_persist<T, true, true, 2>
+                : (const void *)k_chain_persist<T, true, true, 1>;
+  else if (adt_calc_on)
+    kp = U == 2 ? (const void *)k_chain_persist<T, true, false, 2>
+                : (const void *)k_chain_persist<T, true, false, 1>;
+  else
+    kp = U == 2 ? (const void *)k_chain_persist<T, false, false, 2>
+                : (const void *)k_chain_persist<T, false, false, 1>;
+  const int grid = std::max(1, resident_ctas(kp, 256) * rt().num_sms);
+  const int lag_knob = tuning("persist_lag", -1);
+  const int lag = lag_knob >= 0 ? lag_knob : grid;
+  ChainSched *cs = chain_sched(sp, et, 256 * U, lag);
+  if (!cs) return false;
+  const int ncell = sp->ntarget;
+  T *seqbuf = seq ? (T *)red_seq_buffer(sizeof(T) * 4 * (size_t)ncell) : nullptr;
+  T *result = (T *)red_slot_ptr(rslot_id);
+  const T *qold = (const T *)ua[0].dat->data_d;
+  T *q = (T *)ua[1].dat->data_d, *adt = (T *)ua[3].dat->data_d, *res = (T *)ua[2].dat->data_d;
+  CellNodes N;
+  memset(&N, 0, sizeof N);
+  const T *xs[4] = {nullptr, nullptr, nullptr, nullptr};
+  if (aa) {
+    N = CellNodes{idx_map(aa[0]), idx_map(aa[1]), idx_map(aa[2]), idx_map(aa[3])};
+    for (int i = 0; i < 4; i++) xs[i] = (const T *)aa[i].dat->data_d;
+  }
+  T *qsave = sa ? (T *)(save_out ? save_out : sa[1].dat->data_d) : nullptr;
+  T *adt_to = aa ? (T *)(adt_out ? adt_out : adt) : nullptr;
+  const int2 *pedge = reinterpret_cast<const int2 *>(map_dev(ra[0].map));
+  const int2 *pecell = reinterpret_cast<const int2 *>(map_dev(ra[2].map));
+  {
+    PhaseScope ph(name + ":persist");
+    auto go = [&](auto kernel) {
+      launch_pdl(kernel, grid, 256, 0, s, cs->dev, E.n, pedge, pecell, E.xa, E.qa, E.adta, B,
+                 (T *)sp->d_buf, ncell, (const int *)sp->d_ell, sp->width, qold, q, res,
+                 (const T *)adt, N, xs[0], xs[1], xs[2], xs[3], K, seqbuf, result, qsave, adt_to);
+    };
+    if (save_on) {
+      if (U == 2) go(k_chain_persist<T, true, true, 2>);
+      else go(k_chain_persist<T, true, true, 1>);
+    } else if (adt_calc_on) {
+      if (U == 2) go(k_chain_persist<T, true, false, 2>);
+      else go(k_chain_persist<T, true, false, 1>);
+    } else {
+      if (U == 2) go(k_chain_persist<T, false, false, 2>);
+      else go(k_chain_persist<T, false, false, 1>);
+    }
+  }
+  if (seq) {
+    T init = *(const T *)ua[4].data;
+    k_seq_sum<T><<<1, 32, 0, s>>>(seqbuf, 4LL * ncell, init, result);
+  }
+  return true;
+}
+
 template <class T>
 static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op_set bset,
                         const op_arg *ba, const op_arg *ua, const op_arg *aa, const op_arg *sa,
@@ -1784,7 +1987,7 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
                         std::vector<GblRequest> *held) {
   // save_soln rides on the one-cell-per-thread fold + update + adt_calc forms
   const int fvar = tuning("fold_variant", 0);
-  if (sa && (!ua || !aa || (fvar != 0 && fvar != 4 && fvar != 5 && fvar != 6))) return false;
+  if (sa && (!ua || !aa || (fvar != 0 && fvar != 4 && fvar != 5))) return false;
   AirConsts<T> K = air_consts<T>();
   if (error_pending()) return true;
   cudaStream_t s = rt().stream;
@@ -1808,10 +2011,14 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
     LoopScope ls(name.c_str(), bytes, 0);
     ResEdges<T> E = res_edges<T>(rset, ra);
     BresEdges<T> B = bres_edges<T>(bset, ba);
+    if (ua && !flux_done && ua[2].dat == ra[6].dat &&
+        persist_chain<T>(name, sp, ra, E, B, ua, aa, sa, adt_out, save_out, K, seq, rslot_id, s))
+      goto chained;
     if (!flux_done) {
       PhaseScope ph(name + ":flux");
       launch_flux<T>(ra, E, B, vals, nval, K, s);
     }
+    {
     PhaseScope ph(name + ":fold");
     T *res = (T *)ra[6].dat->data_d;
     if (!ua) {
@@ -1859,64 +2066,6 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
                    red_ticket(), qsave, adt_to);
       };
       const int fv = fvar;
-      // fold_variant 6: the TMA-staged pass; fold_tma_cfg picks consumer
-      // warps x stages (1: 4 x 4, 2: 8 x 3, 3: 4 x 6, 4: 2 x 8)
-      auto launch_tma = [&](auto kernel, int nc, size_t smem) -> bool {
-        const bool quad = !aa || (N.m0.map && N.m0.map == N.m1.map && N.m0.map == N.m2.map &&
-                                  N.m0.map == N.m3.map && N.m0.dim == 4 && N.m0.idx == 0 &&
-                                  N.m1.idx == 1 && N.m2.idx == 2 && N.m3.idx == 3);
-        const uintptr_t bases = (uintptr_t)sp->d_ell | (uintptr_t)res | (uintptr_t)qold |
-                                (uintptr_t)adt | (aa ? (uintptr_t)N.m0.map : 0);
-        if (!quad || (bases & 15) || smem > (size_t)rt().smem_optin) return false;
-        static std::vector<std::pair<const void *, size_t>> sized;
-        const void *kp = (const void *)kernel;
-        if (std::find(sized.begin(), sized.end(), std::make_pair(kp, smem)) == sized.end()) {
-          OP2B_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem));
-          sized.emplace_back(kp, smem);
-        }
-        const int threads = (nc + 1) * 32, tc = nc * 32;
-        int per = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) !=
-                cudaSuccess || per < 1)
-          per = 1;
-        const long long tiles = (ncell + tc - 1LL) / tc;
-        const int grid = (int)std::max(1LL, std::min(std::min((long long)rt().num_sms * per,
-                                                              (long long)kMaxRedBlocks), tiles));
-        long long chunk = (ncell + grid - 1LL) / grid;
-        chunk = (chunk + 3) & ~3LL;
-        launch_pdl(kernel, grid, threads, smem, s, ncell, (int)chunk, W, (const int *)sp->d_ell,
-                   (const T *)vals, qold, q, res, (const T *)adt,
-                   (const int4 *)(aa ? N.m0.map : nullptr), xs[0], xs[1], xs[2], xs[3], K,
-                   seqbuf, rslot, red_ticket(), qsave, adt_to ? adt_to : adt);
-        return true;
-      };
-      auto tma = [&](auto k44, auto k83, auto k46, auto k28, bool with_adt) -> bool {
-        const int cfg = tuning("fold_tma_cfg", 1);
-        if (cfg == 2) return launch_tma(k83, 8, with_adt ? fold_tma_smem<T, true, 8, 3>(W)
-                                                         : fold_tma_smem<T, false, 8, 3>(W));
-        if (cfg == 3) return launch_tma(k46, 4, with_adt ? fold_tma_smem<T, true, 4, 6>(W)
-                                                         : fold_tma_smem<T, false, 4, 6>(W));
-        if (cfg == 4) return launch_tma(k28, 2, with_adt ? fold_tma_smem<T, true, 2, 8>(W)
-                                                         : fold_tma_smem<T, false, 2, 8>(W));
-        return launch_tma(k44, 4, with_adt ? fold_tma_smem<T, true, 4, 4>(W)
-                                           : fold_tma_smem<T, false, 4, 4>(W));
-      };
-      constexpr int M6 = sizeof(T) == 4 ? 6 : 3, M3 = sizeof(T) == 4 ? 3 : 2;
-      if (fv == 6) {
-        bool done;
-        if (sa)
-          done = tma(k_fold_tma<T, true, true, 4, 4, M6>, k_fold_tma<T, true, true, 8, 3, M3>,
-                     k_fold_tma<T, true, true, 4, 6, M6>, k_fold_tma<T, true, true, 2, 8, M6>, true);
-        else if (aa)
-          done = tma(k_fold_tma<T, true, false, 4, 4, M6>, k_fold_tma<T, true, false, 8, 3, M3>,
-                     k_fold_tma<T, true, false, 4, 6, M6>, k_fold_tma<T, true, false, 2, 8, M6>, true);
-        else
-          done = tma(k_fold_tma<T, false, false, 4, 4, M6>, k_fold_tma<T, false, false, 8, 3, M3>,
-                     k_fold_tma<T, false, false, 4, 6, M6>, k_fold_tma<T, false, false, 2, 8, M6>,
-                     false);
-        if (done) goto folded;
-      }
       if (sa) {
         if (fv == 4) launch(k_fold_update<T, true, 1, 3, true>);
         else if (fv == 5) launch(k_fold_update_pf<T, true, sizeof(T) == 4 ? 3 : 2, true>);
@@ -1936,12 +2085,13 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
         else if (fv == 5) launch(k_fold_update_pf<T, false, sizeof(T) == 4 ? 4 : 2, false>);
         else launch(k_fold_update<T, false, 1, sizeof(T) == 4 ? 5 : 2>);
       }
-    folded:
       if (seq) {
         T init = *(const T *)ua[4].data;
         k_seq_sum<T><<<1, 32, 0, s>>>(seqbuf, 4LL * ncell, init, result);
       }
     }
+    }
+  chained:;
   }
   if (ua) {
     GblRequest rq{ua[4].data, rslot_id, OP_INC, sizeof(T) == 8 ? GBL_F64 : GBL_F32, seq};

@@ -80,12 +80,12 @@ const int *map_dev(op_map m) {
     size_t bytes = sizeof(int) * (size_t)m->dim * m->from->size;
     md.d = (int *)dev_alloc(bytes);
     if (md.d) {
-      // renumbered sets: rows in the from-set's new order, values in the
-      // to-set's new numbering
-      std::vector<int> rn = renumbered_map(m);
-      OP2B_CUDA(cudaMemcpyAsync(md.d, rn.empty() ? (const int *)m->map : rn.data(), bytes,
-                                cudaMemcpyHostToDevice, R.stream));
+      OP2B_CUDA(cudaMemcpyAsync(md.d, (const int *)m->map, bytes, cudaMemcpyHostToDevice,
+                                R.stream));
       OP2B_CUDA(cudaStreamSynchronize(R.stream));
+      // renumbered sets: rows in the from-set's new order, values in the
+      // to-set's new numbering, rewritten on the device
+      renumber_map_device(m, md.d);
     }
   }
   return md.d;

@@ -177,7 +177,7 @@ const int *perm_new2old_dev(op_set s);  // device permutation, nullptr when not 
 const int *perm_old2new_dev(op_set s);
 void permute_dat_in_place(op_dat d);   // a dataset declared after renumbering
 bool fetch_unpermuted(op_dat d, void *host);  // false: not renumbered, nothing done
-std::vector<int> renumbered_map(op_map m);    // empty: map unchanged
+bool renumber_map_device(op_map m, int *d_map);  // false: map unchanged
 
 // op_checkpoint (checkpoint.cpp): fast-forward of a restarted run, and the
 // log of reduction values returned to the app

@@ -250,6 +250,8 @@ std::vector<op_arg> g_seen_adt, g_seen_save;  // the last adt_calc / save_soln c
 // flux pass runs while the host returns the rms and takes the next calls.
 std::vector<op_arg> g_seen_res, g_seen_bres;  // the last res_calc / bres_calc calls
 op_set g_seen_res_set = nullptr, g_seen_bres_set = nullptr;
+std::vector<op_arg> g_seen_upd;  // the last airfoil update call (for the autotuner)
+op_set g_seen_upd_set = nullptr;
 struct NextFlux {
   bool valid = false, adt_committed = false;
   std::vector<op_arg> res_args, bres_args;
@@ -523,12 +525,37 @@ void ahead_reset() {
   g_seen_bres.clear();
   g_expect_bres.clear();
   g_seen_res_set = g_seen_bres_set = g_expect_bres_set = nullptr;
+  g_seen_upd.clear();
+  g_seen_upd_set = nullptr;
   g_seen_jres.clear();
   g_seen_jres_set = nullptr;
   g_seen_jres_variant = 0;
   g_save_after = 0;
   for (void *p : g_spare) dev_free(p);
   g_spare.clear();
+}
+
+// the last res_calc, bres_calc, update and adt_calc calls, when they form
+// the airfoil chain (bres_calc after res_calc, update after both, adt_calc
+// after update): what the autotuner times
+bool last_res_chain(ChainArgs *c) {
+  if (g_seen_res.size() != 8 || g_seen_bres.size() != 6 || g_seen_upd.size() != 5 ||
+      g_seen_adt.size() != 6 || !g_seen_res_set || !g_seen_bres_set || !g_seen_upd_set)
+    return false;
+  if (!bres_follows_res(g_seen_res.data(), g_seen_bres.data()) ||
+      !update_follows_res(g_seen_res.data(), g_seen_upd_set, g_seen_upd.data()) ||
+      !adt_follows_update(g_seen_upd.data(), g_seen_upd_set, g_seen_adt[4].dat->set,
+                          g_seen_adt.data()))
+    return false;
+  c->rset = g_seen_res_set;
+  c->bset = g_seen_bres_set;
+  c->uset = g_seen_upd_set;
+  c->aset = g_seen_adt[4].dat->set;
+  c->ra = g_seen_res;
+  c->ba = g_seen_bres;
+  c->ua = g_seen_upd;
+  c->aa = g_seen_adt;
+  return true;
 }
 
 void flush_pending() {
@@ -597,6 +624,10 @@ void par_loop_run(char const *name, op_set set, int nargs, const op_arg *args) {
   if (k == K_RES) {
     g_seen_res.assign(args, args + nargs);
     g_seen_res_set = set;
+  }
+  if (k == K_AUPDATE) {
+    g_seen_upd.assign(args, args + nargs);
+    g_seen_upd_set = set;
   }
   if (k == K_BRES) {
     g_seen_bres.assign(args, args + nargs);

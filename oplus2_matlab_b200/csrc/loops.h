@@ -77,6 +77,13 @@ bool run_jac_res_ahead(char const *name, op_set set, const op_arg *args, int var
 // every node a target); allocates nothing beyond the res loop's own plan
 bool can_run_jac_res_ahead(char const *name, op_set set, const op_arg *args, int variant);
 
+// the last airfoil res_calc chain's calls (loops.cpp), for the autotuner
+struct ChainArgs {
+  op_set rset = nullptr, bset = nullptr, uset = nullptr, aset = nullptr;
+  std::vector<op_arg> ra, ba, ua, aa;
+};
+bool last_res_chain(ChainArgs *c);
+
 // fused loop pairs (airfoil.cu); false = not applicable, run them separately
 bool run_save_adt(op_set set, const op_arg *save_args, const op_arg *adt_args);
 bool run_update_adt(op_set set, const op_arg *update_args, const op_arg *adt_args);

@@ -79,6 +79,7 @@ constexpr int kTile = 256;
 // then b's in b's order, padded with (na+nb) << 1.  Adding the entries in
 // list order is the order of the sequential back-end running a then b;
 // -0.0 is the exact identity of IEEE addition and r + (-v) equals r - v.
+struct ChainSched;  // airfoil.cu: the persistent chain's work queue over these lists
 struct SlotPlan {
   const GatherPlan *a = nullptr, *b = nullptr;
   int ntarget = 0;
@@ -87,7 +88,11 @@ struct SlotPlan {
   int *d_ell = nullptr;     // [ntarget * width]
   void *d_buf = nullptr;    // the (na + nb + 1) values, allocated by the loop
   size_t buf_bytes = 0;
+  ChainSched *chain = nullptr;  // built by the first persistent chain launch
+  bool chain_unsuited = false;  // a cell tile reads too many flux tiles for it
 };
+// free a slot plan's persistent-chain queue (airfoil.cu)
+void release_chain_sched(SlotPlan *sp);
 
 // widest list the fold kernels accept
 constexpr int kMaxSlotWidth = 8;

@@ -2,20 +2,29 @@
 // indirect gathers (op2b_set_renumber).
 //
 // A mesh whose numbering is scrambled turns each gather into a random
-// access.  When renumbering is on, the first loop call orders every set:
+// access.  When renumbering is on, the first loop call orders every set,
+// all of it computed on the GPU:
 //  - the anchor set is the one most maps point to (ties: the larger);
-//    elements that share a row of a map of dim >= 2 onto it are neighbours,
-//    and a breadth-first walk (Cuthill-McKee, from a least-connected element
-//    of each connected component) gives its order;
+//    elements that share a row of a map of dim >= 2 onto it are neighbours
+//    (a CSR graph built by count, scan and fill kernels), and a
+//    level-synchronous breadth-first walk from a least-connected element of
+//    each connected component gives its order (Cuthill-McKee): each level is
+//    found in one parallel expansion of the previous one and ordered by the
+//    smallest new index among an element's parents, ties by old index (a
+//    counting sort by parent, then a sort within each parent's bucket), so
+//    the order is deterministic whatever the threads' timing;
 //  - every set with a map onto an ordered set follows: its elements sorted
 //    by the smallest new index they point to (ties by old index);
 //  - a set only pointed to by an ordered set takes the order in which the
-//    ordered set's rows first reach it;
+//    ordered set's rows first reach it (unreached elements last, in order);
 //  - anything left keeps its numbering.
+// The host only decides which set follows which and reads one count per
+// level of the walk.
 // Each dataset is then stored permuted on the device (element i of the new
-// order is element P[i] of the app's), each map's device copy has its rows
-// in the new order of its from-set and its values in the new numbering of
-// its to-set, and op_fetch_data puts the app's order back.
+// order is element P[i] of the app's), each map's device copy is rewritten
+// on the device with its rows in the new order of its from-set and its
+// values in the new numbering of its to-set, and op_fetch_data puts the
+// app's order back.
 //
 // Results do not change: per-element arithmetic is the same, and the
 // owner-computes plans order each target's contributions by the APP's
@@ -27,7 +36,7 @@
 #include <limits.h>
 
 #include <algorithm>
-#include <queue>
+#include <chrono>
 #include <vector>
 
 #include "internal.h"
@@ -38,81 +47,282 @@ namespace op2b {
 namespace {
 
 struct SetPerm {
-  std::vector<int> P, Q;  // new -> old, old -> new
-  int *d_P = nullptr, *d_Q = nullptr;
+  std::vector<int> P;                  // new -> old (host copy, for op2b_renumber_order)
+  int *d_P = nullptr, *d_Q = nullptr;  // new -> old, old -> new
 };
 
 std::vector<SetPerm> g_perm;  // by set index; empty P: not permuted
 bool g_enabled = false, g_applied = false, g_computed = false;
+double g_order_seconds = 0.0;  // the last order computation, GPU work included
 
 bool permuted(int set_index) {
-  return set_index < (int)g_perm.size() && !g_perm[set_index].P.empty();
+  return set_index < (int)g_perm.size() && g_perm[set_index].d_P;
 }
 
-// Cuthill-McKee order of the anchor set's neighbour graph
-std::vector<int> anchor_order(op_set s) {
+// ----------------------------------------------------------- kernels ----
+
+#define GRID_STRIDE(i, n)                                                     \
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); \
+       i += (long long)gridDim.x * blockDim.x)
+
+__global__ void k_fill_int(int *p, long long n, int v) {
+  GRID_STRIDE(i, n) p[i] = v;
+}
+
+// every entry of a map row is a neighbour of the dim - 1 others
+__global__ void k_degree(const int *__restrict__ map, long long rows, int dim, int *deg) {
+  GRID_STRIDE(e, rows * dim) atomicAdd(deg + map[e], dim - 1);
+}
+
+__global__ void k_adjacency(const int *__restrict__ map, long long rows, int dim,
+                            const int *__restrict__ off, int *cur, int *adj) {
+  GRID_STRIDE(e, rows * dim) {
+    const long long r = e / dim;
+    const int a = (int)(e % dim), v = map[e];
+    for (int b = 0; b < dim; b++)
+      if (b != a) adj[off[v] + atomicAdd(cur + v, 1)] = map[r * dim + b];
+  }
+}
+
+// least (degree, index) among the elements not yet placed
+__global__ void k_seed(const int *__restrict__ level, const int *__restrict__ deg, long long n,
+                       unsigned long long *best) {
+  unsigned long long mine = ~0ull;
+  GRID_STRIDE(v, n) if (level[v] < 0) {
+    const unsigned long long k = ((unsigned long long)(unsigned)deg[v] << 32) | (unsigned)v;
+    mine = k < mine ? k : mine;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long x = __shfl_down_sync(0xffffffffu, mine, o);
+    mine = x < mine ? x : mine;
+  }
+  if ((threadIdx.x & 31) == 0 && mine != ~0ull) atomicMin(best, mine);
+}
+
+__global__ void k_seed_place(const unsigned long long *best, int *order, int pos, int *level) {
+  const int v = (int)(*best & 0xffffffffull);
+  order[pos] = v;
+  level[v] = 0;
+}
+
+// one breadth-first level: the neighbours of order[fs, fe) not yet reached
+// join level L + 1 (appended to next, unordered); each records the smallest
+// position of a parent (pkey) for the ordering of the level
+__global__ void k_expand(const int *__restrict__ order, int fs, int fe,
+                         const int *__restrict__ off, const int *__restrict__ adj, int *level,
+                         int L, int *pkey, int *next, int *count) {
+  GRID_STRIDE(t, (long long)(fe - fs)) {
+    const int p = fs + (int)t, v = order[p];
+    for (int j = off[v]; j < off[v + 1]; j++) {
+      const int w = adj[j];
+      const int old = atomicCAS(level + w, -1, L + 1);
+      if (old == -1) next[atomicAdd(count, 1)] = w;
+      if (old == -1 || old == L + 1) atomicMin(pkey + w, p);
+    }
+  }
+}
+
+// bucket key of each listed element: its parent's position minus base
+__global__ void k_level_keys(const int *__restrict__ items, int n, const int *__restrict__ pkey,
+                             int base, int *bkey) {
+  GRID_STRIDE(i, (long long)n) bkey[i] = pkey[items[i]] - base;
+}
+
+// bucket key of element e of a set with a map onto an ordered set: the
+// smallest new index it points to
+__global__ void k_row_min_key(const int *__restrict__ map, long long rows, int dim,
+                              const int *__restrict__ Q, int *bkey) {
+  GRID_STRIDE(r, rows) {
+    int m = INT_MAX;
+    for (int a = 0; a < dim; a++) m = min(m, Q[map[r * dim + a]]);
+    bkey[r] = m;
+  }
+}
+
+// first slot (new row x dim + column) of an ordered set's map that reaches
+// each element of the to-set
+__global__ void k_reach_key(const int *__restrict__ map, long long rows, int dim,
+                            const int *__restrict__ Qfrom, int *rkey) {
+  GRID_STRIDE(e, rows * dim) {
+    const long long r = e / dim;
+    atomicMin(rkey + map[e], Qfrom[r] * dim + (int)(e % dim));
+  }
+}
+
+// unreached elements go last, in their old order: key after every slot
+__global__ void k_reach_finish(int *rkey, long long n, long long slots) {
+  GRID_STRIDE(v, n) if (rkey[v] == INT_MAX) rkey[v] = (int)(slots + v);
+}
+
+__global__ void k_bucket_count(const int *__restrict__ bkey, int n, int *cnt) {
+  GRID_STRIDE(i, (long long)n) atomicAdd(cnt + bkey[i], 1);
+}
+
+__global__ void k_bucket_place(const int *__restrict__ items, const int *__restrict__ bkey, int n,
+                               const int *__restrict__ boff, int *cur, int *out) {
+  GRID_STRIDE(i, (long long)n) {
+    const int b = bkey[i];
+    out[boff[b] + atomicAdd(cur + b, 1)] = items ? items[i] : (int)i;
+  }
+}
+
+// each bucket's elements by index (buckets hold a few elements: the
+// neighbours of one parent, the rows whose smallest target is one element)
+__global__ void k_bucket_sort(int *out, const int *__restrict__ boff, int nb, int n) {
+  GRID_STRIDE(b, (long long)nb) {
+    const int lo = boff[b], hi = b + 1 < nb ? boff[b + 1] : n;
+    for (int i = lo + 1; i < hi; i++) {
+      const int x = out[i];
+      int j = i - 1;
+      while (j >= lo && out[j] > x) {
+        out[j + 1] = out[j];
+        j--;
+      }
+      out[j + 1] = x;
+    }
+  }
+}
+
+__global__ void k_inverse(const int *__restrict__ P, long long n, int *Q) {
+  GRID_STRIDE(i, n) Q[P[i]] = (int)i;
+}
+
+// out[i * dim + a] = Qto[in[Pfrom[i] * dim + a]] (either permutation optional)
+__global__ void k_renumber_map(const int *__restrict__ in, long long rows, int dim,
+                               const int *__restrict__ Pfrom, const int *__restrict__ Qto,
+                               int *out) {
+  GRID_STRIDE(e, rows * dim) {
+    const long long i = e / dim;
+    const int a = (int)(e % dim);
+    const long long src = Pfrom ? Pfrom[i] : i;
+    const int v = in[src * dim + a];
+    out[e] = Qto ? Qto[v] : v;
+  }
+}
+
+#undef GRID_STRIDE
+
+// --------------------------------------------------------- host driver ----
+
+int grid_for_n(long long n) {
+  return (int)std::max(1LL, std::min((n + 255) / 256, (long long)rt().num_sms * 8));
+}
+
+struct DevInts {  // scoped device scratch
+  int *p = nullptr;
+  explicit DevInts(long long n) { p = (int *)dev_alloc(sizeof(int) * (size_t)std::max(1LL, n)); }
+  ~DevInts() { dev_free(p); }
+  DevInts(const DevInts &) = delete;
+  DevInts &operator=(const DevInts &) = delete;
+};
+
+// items (0..n-1 when null) ordered by (bkey, item) into out; bkey in [0, nb)
+bool bucket_sort(const int *items, const int *bkey, int n, long long nb, int *out) {
+  if (n <= 0) return true;
+  if (nb <= 0 || nb >= INT_MAX) return false;
+  cudaStream_t s = rt().stream;
+  DevInts cnt(nb), off(nb), cur(nb);
+  if (!cnt.p || !off.p || !cur.p) return false;
+  OP2B_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * (size_t)nb, s));
+  OP2B_CUDA(cudaMemsetAsync(cur.p, 0, sizeof(int) * (size_t)nb, s));
+  k_bucket_count<<<grid_for_n(n), 256, 0, s>>>(bkey, n, cnt.p);
+  exclusive_scan(cnt.p, off.p, (int)nb, s);
+  k_bucket_place<<<grid_for_n(n), 256, 0, s>>>(items, bkey, n, off.p, cur.p, out);
+  k_bucket_sort<<<grid_for_n(nb), 256, 0, s>>>(out, off.p, (int)nb, n);
+  return !error_pending();
+}
+
+// the order d_P (new -> old, device, owned by the set's entry from now on)
+// of set s: its inverse and a host copy
+void set_perm(op_set s, int *d_P) {
+  if ((int)g_perm.size() <= s->index) g_perm.resize(s->index + 1);
+  SetPerm &sp = g_perm[s->index];
+  dev_free(sp.d_P);
+  dev_free(sp.d_Q);
+  sp.d_P = d_P;
+  sp.d_Q = (int *)dev_alloc(sizeof(int) * (size_t)std::max(1, s->size));
+  sp.P.assign(s->size, 0);
+  if (!sp.d_Q) return;
+  k_inverse<<<grid_for_n(s->size), 256, 0, rt().stream>>>(d_P, s->size, sp.d_Q);
+  OP2B_CUDA(cudaMemcpyAsync(sp.P.data(), d_P, sizeof(int) * (size_t)s->size,
+                            cudaMemcpyDeviceToHost, rt().stream));
+  OP2B_CUDA(cudaStreamSynchronize(rt().stream));
+}
+
+// Cuthill-McKee order of the anchor set's neighbour graph, on the device
+int *anchor_order(op_set s) {
+  cudaStream_t st = rt().stream;
   const int n = s->size;
-  std::vector<int> deg(n, 0);
   std::vector<op_map> onto;
   for (int k = 0; k < OP_map_index; k++) {
     op_map m = OP_map_list[k];
     if (m->to == s && m->dim >= 2) onto.push_back(m);
   }
-  // neighbour lists: every pair in a row
+  DevInts deg(n), off(n + 1), cur(n), level(n), pkey(n), next(n), bkey(n), count(1);
+  int *order = (int *)dev_alloc(sizeof(int) * (size_t)std::max(1, n));
+  unsigned long long *best = (unsigned long long *)dev_alloc(sizeof(unsigned long long));
+  auto fail_out = [&]() {
+    dev_free(order);
+    dev_free(best);
+    return (int *)nullptr;
+  };
+  if (!order || !best || !deg.p || !off.p || !cur.p || !level.p || !pkey.p || !next.p ||
+      !bkey.p || !count.p)
+    return fail_out();
+  OP2B_CUDA(cudaMemsetAsync(deg.p, 0, sizeof(int) * (size_t)n, st));
   for (op_map m : onto)
-    for (int r = 0; r < m->from->size; r++)
-      for (int a = 0; a < m->dim; a++) deg[m->map[(size_t)r * m->dim + a]] += m->dim - 1;
-  std::vector<long long> off(n + 1, 0);
-  for (int i = 0; i < n; i++) off[i + 1] = off[i] + deg[i];
-  std::vector<int> adj(off[n]);
-  std::vector<long long> cur(off.begin(), off.end() - 1);
+    k_degree<<<grid_for_n((long long)m->from->size * m->dim), 256, 0, st>>>(
+        map_dev(m), m->from->size, m->dim, deg.p);
+  const long long nnz = exclusive_scan(deg.p, off.p, n, st);
+  if (nnz >= INT_MAX) return fail_out();
+  const int nnz_i = (int)nnz;
+  OP2B_CUDA(cudaMemcpyAsync(off.p + n, &nnz_i, sizeof(int), cudaMemcpyHostToDevice, st));
+  DevInts adj(nnz);
+  if (!adj.p) return fail_out();
+  OP2B_CUDA(cudaMemsetAsync(cur.p, 0, sizeof(int) * (size_t)n, st));
   for (op_map m : onto)
-    for (int r = 0; r < m->from->size; r++) {
-      const int *row = m->map + (size_t)r * m->dim;
-      for (int a = 0; a < m->dim; a++)
-        for (int b = 0; b < m->dim; b++)
-          if (a != b) adj[cur[row[a]]++] = row[b];
+    k_adjacency<<<grid_for_n((long long)m->from->size * m->dim), 256, 0, st>>>(
+        map_dev(m), m->from->size, m->dim, off.p, cur.p, adj.p);
+  k_fill_int<<<grid_for_n(n), 256, 0, st>>>(level.p, n, -1);
+  k_fill_int<<<grid_for_n(n), 256, 0, st>>>(pkey.p, n, INT_MAX);
+  int placed = 0;
+  while (placed < n) {  // one connected component per pass
+    OP2B_CUDA(cudaMemsetAsync(best, 0xff, sizeof(unsigned long long), st));
+    k_seed<<<grid_for_n(n), 256, 0, st>>>(level.p, deg.p, n, best);
+    k_seed_place<<<1, 1, 0, st>>>(best, order, placed, level.p);
+    int fs = placed, fe = placed + 1, L = 0;
+    for (;;) {
+      OP2B_CUDA(cudaMemsetAsync(count.p, 0, sizeof(int), st));
+      k_expand<<<grid_for_n(fe - fs), 256, 0, st>>>(order, fs, fe, off.p, adj.p, level.p, L,
+                                                    pkey.p, next.p, count.p);
+      int c = 0;
+      OP2B_CUDA(cudaMemcpyAsync(&c, count.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+      OP2B_CUDA(cudaStreamSynchronize(st));
+      if (error_pending()) return fail_out();
+      if (c <= 0 || fe + c > n) break;
+      k_level_keys<<<grid_for_n(c), 256, 0, st>>>(next.p, c, pkey.p, fs, bkey.p);
+      if (!bucket_sort(next.p, bkey.p, c, fe - fs, order + fe)) return fail_out();
+      fs = fe;
+      fe += c;
+      L++;
     }
-  std::vector<int> order;
-  order.reserve(n);
-  std::vector<char> seen(n, 0);
-  // start each component at a least-connected element, found in one pass
-  std::vector<int> by_deg(n);
-  for (int i = 0; i < n; i++) by_deg[i] = i;
-  std::stable_sort(by_deg.begin(), by_deg.end(), [&](int a, int b) { return deg[a] < deg[b]; });
-  for (int start : by_deg) {
-    if (seen[start]) continue;
-    std::queue<int> q;
-    q.push(start);
-    seen[start] = 1;
-    while (!q.empty()) {
-      const int v = q.front();
-      q.pop();
-      order.push_back(v);
-      for (long long j = off[v]; j < off[v + 1]; j++) {
-        const int w = adj[j];
-        if (!seen[w]) {
-          seen[w] = 1;
-          q.push(w);
-        }
-      }
-    }
+    placed = fe;
   }
+  dev_free(best);
   return order;
 }
 
-void set_perm(op_set s, std::vector<int> P) {
-  if ((int)g_perm.size() <= s->index) g_perm.resize(s->index + 1);
-  SetPerm &sp = g_perm[s->index];
-  sp.Q.assign(P.size(), 0);
-  for (size_t i = 0; i < P.size(); i++) sp.Q[P[i]] = (int)i;
-  sp.P = std::move(P);
-}
-
 void compute_orders() {
+  for (auto &sp : g_perm) {
+    dev_free(sp.d_P);
+    dev_free(sp.d_Q);
+  }
   g_perm.clear();
   g_perm.resize(OP_set_index);
+  g_computed = true;
   if (OP_set_index == 0) return;
+  ensure_cuda();
+  cudaStream_t st = rt().stream;
   // anchor: most maps onto it, then the larger
   op_set anchor = nullptr;
   int best = -1;
@@ -126,8 +336,10 @@ void compute_orders() {
       anchor = s;
     }
   }
-  if (best <= 0) return;  // no map with shared rows: nothing to gain
-  set_perm(anchor, anchor_order(anchor));
+  if (best <= 0 || anchor->size == 0) return;  // no map with shared rows: nothing to gain
+  int *P = anchor_order(anchor);
+  if (!P) return;
+  set_perm(anchor, P);
   bool progress = true;
   while (progress) {
     progress = false;
@@ -138,49 +350,47 @@ void compute_orders() {
       op_map via = nullptr;
       for (int j = 0; j < OP_map_index && !via; j++) {
         op_map m = OP_map_list[j];
-        if (m->from == s && permuted(m->to->index)) via = m;
+        if (m->from == s && m->dim >= 1 && permuted(m->to->index)) via = m;
       }
       if (via) {
-        const std::vector<int> &Qt = g_perm[via->to->index].Q;
-        std::vector<int> key(s->size);
-        for (int e = 0; e < s->size; e++) {
-          int mn = INT_MAX;
-          for (int a = 0; a < via->dim; a++)
-            mn = std::min(mn, Qt[via->map[(size_t)e * via->dim + a]]);
-          key[e] = mn;
+        DevInts key(s->size);
+        int *dP = (int *)dev_alloc(sizeof(int) * (size_t)s->size);
+        if (!key.p || !dP) return;
+        k_row_min_key<<<grid_for_n(s->size), 256, 0, st>>>(map_dev(via), s->size, via->dim,
+                                                           g_perm[via->to->index].d_Q, key.p);
+        if (!bucket_sort(nullptr, key.p, s->size, via->to->size, dP)) {
+          dev_free(dP);
+          return;
         }
-        std::vector<int> P(s->size);
-        for (int e = 0; e < s->size; e++) P[e] = e;
-        std::stable_sort(P.begin(), P.end(), [&](int a, int b) { return key[a] < key[b]; });
-        set_perm(s, std::move(P));
+        set_perm(s, dP);
         progress = true;
         continue;
       }
       // a map from an ordered set onto s
       for (int j = 0; j < OP_map_index; j++) {
         op_map m = OP_map_list[j];
-        if (m->to != s || !permuted(m->from->index)) continue;
-        const std::vector<int> &Pf = g_perm[m->from->index].P;
-        std::vector<char> seen(s->size, 0);
-        std::vector<int> P;
-        P.reserve(s->size);
-        for (int r : Pf)
-          for (int a = 0; a < m->dim; a++) {
-            const int v = m->map[(size_t)r * m->dim + a];
-            if (!seen[v]) {
-              seen[v] = 1;
-              P.push_back(v);
-            }
-          }
-        for (int v = 0; v < s->size; v++)
-          if (!seen[v]) P.push_back(v);
-        set_perm(s, std::move(P));
+        if (m->to != s || m->dim < 1 || !permuted(m->from->index)) continue;
+        const long long slots = (long long)m->from->size * m->dim;
+        DevInts key(s->size);
+        int *dP = (int *)dev_alloc(sizeof(int) * (size_t)s->size);
+        if (!key.p || !dP || slots + s->size >= INT_MAX) {
+          dev_free(dP);
+          return;
+        }
+        k_fill_int<<<grid_for_n(s->size), 256, 0, st>>>(key.p, s->size, INT_MAX);
+        k_reach_key<<<grid_for_n(slots), 256, 0, st>>>(map_dev(m), m->from->size, m->dim,
+                                                       g_perm[m->from->index].d_Q, key.p);
+        k_reach_finish<<<grid_for_n(s->size), 256, 0, st>>>(key.p, s->size, slots);
+        if (!bucket_sort(nullptr, key.p, s->size, slots + s->size, dP)) {
+          dev_free(dP);
+          return;
+        }
+        set_perm(s, dP);
         progress = true;
         break;
       }
     }
   }
-  g_computed = true;
 }
 
 // out[i] = in[P[i]] (forward) or out[P[i]] = in[i] (back), w words per element
@@ -255,22 +465,24 @@ bool fetch_unpermuted(op_dat d, void *host) {
   return true;
 }
 
-// host copy of a map in the renumbered order, or empty when unchanged
-std::vector<int> renumbered_map(op_map m) {
-  std::vector<int> out;
-  if (!g_applied) return out;
+// rewrite a map's device copy (uploaded in the app's numbering) for the
+// renumbered sets: rows in the from-set's new order, values in the to-set's
+// new numbering; false when neither set is renumbered
+bool renumber_map_device(op_map m, int *d_map) {
+  if (!g_applied) return false;
   const bool pf = permuted(m->from->index), pt = permuted(m->to->index);
-  if (!pf && !pt) return out;
-  const int n = m->from->size, dim = m->dim;
-  out.resize((size_t)n * dim);
-  for (int i = 0; i < n; i++) {
-    const int src = pf ? g_perm[m->from->index].P[i] : i;
-    for (int a = 0; a < dim; a++) {
-      const int v = m->map[(size_t)src * dim + a];
-      out[(size_t)i * dim + a] = pt ? g_perm[m->to->index].Q[v] : v;
-    }
-  }
-  return out;
+  if (!pf && !pt) return false;
+  const long long n = (long long)m->from->size * m->dim;
+  if (n == 0) return true;
+  DevInts tmp(n);
+  if (!tmp.p) return true;
+  cudaStream_t st = rt().stream;
+  OP2B_CUDA(cudaMemcpyAsync(tmp.p, d_map, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+  k_renumber_map<<<grid_for_n(n), 256, 0, st>>>(tmp.p, m->from->size, m->dim,
+                                                 pf ? g_perm[m->from->index].d_P : nullptr,
+                                                 pt ? g_perm[m->to->index].d_Q : nullptr, d_map);
+  OP2B_CUDA(cudaStreamSynchronize(st));  // tmp is freed on return
+  return true;
 }
 
 void release_plans_and_maps();  // device.cu
@@ -278,19 +490,14 @@ void release_plans_and_maps();  // device.cu
 // called by the first loop call: order the sets, move the data
 void renumber_apply() {
   if (!g_enabled || g_applied) return;
+  const auto t0 = std::chrono::steady_clock::now();
   compute_orders();  // from the sets and maps declared by now
-  for (int k = 0; k < (int)g_perm.size(); k++) {
-    SetPerm &sp = g_perm[k];
-    if (sp.P.empty()) continue;
-    sp.d_P = (int *)dev_alloc(sizeof(int) * sp.P.size());
-    sp.d_Q = (int *)dev_alloc(sizeof(int) * sp.Q.size());
-    if (!sp.d_P || !sp.d_Q) return;
-    OP2B_CUDA(cudaMemcpy(sp.d_P, sp.P.data(), sizeof(int) * sp.P.size(), cudaMemcpyHostToDevice));
-    OP2B_CUDA(cudaMemcpy(sp.d_Q, sp.Q.data(), sizeof(int) * sp.Q.size(), cudaMemcpyHostToDevice));
-  }
   g_applied = true;
   release_plans_and_maps();  // device copies of maps and plans follow the new order
   for (int k = 0; k < OP_dat_index; k++) permute_dat_in_place(OP_dat_list[k]);
+  OP2B_CUDA(cudaStreamSynchronize(rt().stream));
+  g_order_seconds =
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
 void renumber_reset() {
@@ -321,7 +528,7 @@ int op2b_set_renumber(int on) {
 int op2b_renumber_order(op_set set, int *new2old) {
   if (!set || !new2old) return -1;
   if (!g_applied) compute_orders();
-  if (permuted(set->index)) {
+  if (permuted(set->index) && (int)g_perm[set->index].P.size() == set->size) {
     std::copy(g_perm[set->index].P.begin(), g_perm[set->index].P.end(), new2old);
     return 1;
   }
@@ -330,3 +537,5 @@ int op2b_renumber_order(op_set set, int *new2old) {
 }
 
 }  // extern "C"
+
+extern "C" double op2b_renumber_seconds(void) { return op2b::g_order_seconds; }

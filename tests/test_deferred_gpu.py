@@ -110,4 +110,5 @@ def test_graph_of_rotated_iteration(op2, case, fold_variant):
         api.set_gbl_deferred(0)
         lib.op2b_set_tuning(b"fold_variant", 0)
     assert op2.last_error() == ""
+    assert lib.op2b_wait_timeouts(1) == 0
     check(g, A, dt)

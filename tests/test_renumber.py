@@ -1,7 +1,8 @@
 """Renumbering for locality (op2b_set_renumber).
 
-On the host: the orders are permutations, and on a scrambled mesh they bring
-the two cells of an edge, and an edge and its cells, close together again.
+The orders (computed on the GPU) are permutations, and on a scrambled mesh
+they bring the two cells of an edge, and an edge and its cells, close
+together again.
 On the device: with renumbering on, the scrambled airfoil's final fields are
 still bit-identical to the reference's sequential build (contributions keep
 the app's element order) and come back from op_fetch_data in the app's
@@ -27,6 +28,7 @@ def sha(a):
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
+@pytest.mark.gpu
 def test_orders_are_permutations_that_restore_locality():
     code = textwrap.dedent("""
         import sys, ctypes as C, numpy as np
