@@ -183,6 +183,99 @@ __global__ void k_bucket_sort(int *out, const int *__restrict__ boff, int nb, in
   }
 }
 
+// The whole walk in one CTA, without host round trips: each level is
+// expanded by all threads (atomics on level and pkey, which are read back
+// through L2 since L1 does not see atomics), then sorted by (parent
+// position, index) with a bitonic sort in shared memory.  status: 0 done,
+// 1 a level wider than kBfsCtaMax (the caller falls back to the
+// multi-launch walk).
+constexpr int kBfsCtaMax = 8192;
+__global__ void __launch_bounds__(1024)
+    k_bfs_cta(int n, const int *__restrict__ off, const int *__restrict__ adj,
+              const int *__restrict__ deg, int *level, int *pkey, int *order, int *next,
+              int *status) {
+  extern __shared__ unsigned long long keys[];  // kBfsCtaMax
+  __shared__ int s_cnt;
+  __shared__ unsigned long long s_best;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  int placed = 0;
+  while (placed < n) {  // one connected component per pass
+    if (tid == 0) s_best = ~0ull;
+    __syncthreads();
+    unsigned long long mine = ~0ull;
+    for (int v = tid; v < n; v += nt)
+      if (__ldcg(level + v) < 0) {
+        const unsigned long long k = ((unsigned long long)(unsigned)deg[v] << 32) | (unsigned)v;
+        mine = k < mine ? k : mine;
+      }
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long x = __shfl_down_sync(0xffffffffu, mine, o);
+      mine = x < mine ? x : mine;
+    }
+    if ((tid & 31) == 0) atomicMin(&s_best, mine);
+    __syncthreads();
+    if (tid == 0) {
+      const int v = (int)(s_best & 0xffffffffull);
+      order[placed] = v;
+      atomicExch(level + v, 0);
+    }
+    int fs = placed, fe = placed + 1, L = 0;
+    __syncthreads();
+    for (;;) {
+      if (tid == 0) s_cnt = 0;
+      __syncthreads();
+      for (int p = fs + tid; p < fe; p += nt) {
+        const int v = order[p];
+        for (int j = off[v]; j < off[v + 1]; j++) {
+          const int w = adj[j];
+          const int old = atomicCAS(level + w, -1, L + 1);
+          if (old == -1) {
+            const int slot = atomicAdd(&s_cnt, 1);
+            if (slot < kBfsCtaMax) next[slot] = w;
+          }
+          if (old == -1 || old == L + 1) atomicMin(pkey + w, p);
+        }
+      }
+      __syncthreads();
+      const int c = s_cnt;
+      if (c == 0) break;
+      if (c > kBfsCtaMax || fe + c > n) {
+        if (tid == 0) *status = 1;
+        return;
+      }
+      int m = 1;
+      while (m < c) m <<= 1;
+      for (int i = tid; i < m; i += nt)
+        keys[i] = i < c ? ((unsigned long long)(unsigned)__ldcg(pkey + next[i]) << 32) |
+                              (unsigned)next[i]
+                        : ~0ull;
+      __syncthreads();
+      for (int k = 2; k <= m; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+          for (int i = tid; i < m; i += nt) {
+            const int ixj = i ^ j;
+            if (ixj > i) {
+              const unsigned long long a = keys[i], b = keys[ixj];
+              if ((a > b) == ((i & k) == 0)) {
+                keys[i] = b;
+                keys[ixj] = a;
+              }
+            }
+          }
+          __syncthreads();
+        }
+      for (int i = tid; i < c; i += nt) order[fe + i] = (int)(keys[i] & 0xffffffffull);
+      __syncthreads();
+      fs = fe;
+      fe += c;
+      L++;
+    }
+    placed = fe;
+    __syncthreads();
+  }
+  if (tid == 0) *status = 0;
+}
+
 __global__ void k_inverse(const int *__restrict__ P, long long n, int *Q) {
   GRID_STRIDE(i, n) Q[P[i]] = (int)i;
 }
@@ -285,6 +378,28 @@ int *anchor_order(op_set s) {
         map_dev(m), m->from->size, m->dim, off.p, cur.p, adj.p);
   k_fill_int<<<grid_for_n(n), 256, 0, st>>>(level.p, n, -1);
   k_fill_int<<<grid_for_n(n), 256, 0, st>>>(pkey.p, n, INT_MAX);
+  {  // the whole walk in one CTA; levels wider than kBfsCtaMax fall back below
+    const size_t smem = sizeof(unsigned long long) * kBfsCtaMax;
+    static bool sized = false;
+    if (!sized) {
+      OP2B_CUDA(cudaFuncSetAttribute(k_bfs_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+      sized = true;
+    }
+    int status = 2;
+    OP2B_CUDA(cudaMemsetAsync(count.p, 0xff, sizeof(int), st));
+    k_bfs_cta<<<1, 1024, smem, st>>>(n, off.p, adj.p, deg.p, level.p, pkey.p, order, next.p,
+                                     count.p);
+    OP2B_CUDA(cudaMemcpyAsync(&status, count.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    OP2B_CUDA(cudaStreamSynchronize(st));
+    if (error_pending()) return fail_out();
+    if (status == 0) {
+      dev_free(best);
+      return order;
+    }
+    k_fill_int<<<grid_for_n(n), 256, 0, st>>>(level.p, n, -1);
+    k_fill_int<<<grid_for_n(n), 256, 0, st>>>(pkey.p, n, INT_MAX);
+  }
   int placed = 0;
   while (placed < n) {  // one connected component per pass
     OP2B_CUDA(cudaMemsetAsync(best, 0xff, sizeof(unsigned long long), st));
