@@ -32,7 +32,16 @@ roofline  the launches that run the step's first res_calc (fused with the
         from event pairs in a profiled copy of the step's graph.
 cpu_baseline / --impl reference  the reference's own OpenMP build
         (oracle/_ref/airfoil_op_f32, compiled from its sources) on this
-        host's cores, timed by its own op_timing_output.
+        host's cores, timed by its own op_timing_output.  The reference arm
+        writes its input with the host-only oracle/_build/gen_grid, so its
+        process loads nothing of this repository's GPU library.
+batched / served_200_per_s / served_20_per_s  (plain mode, one GPU) the
+        batched workload (64 seeded instances x 500 iterations, grouped
+        against the same solves back to back through the plain C API) and
+        two served streams (200 requests/s shortened to --forms-requests,
+        stop at 1e-6 x the first rms or 2000 iterations; and 20 requests/s
+        with a 5% stopping test), each with p50/p99 latency, the plain-path
+        comparison and a clock record of its own timed region.
 With N > 1 (torchrun), every rank runs an independent replica (the path
 does not shard: "replicas only") and value = N*K iterations / max rank time.
 """
@@ -101,7 +110,7 @@ def parse():
                     help="served: cap on solves iterated together (0: memory budget only)")
     ap.add_argument("--policy", default="fifo", choices=["fifo", "shortest"],
                     help="served: admission order")
-    ap.add_argument("--plain-sample", type=int, default=16,
+    ap.add_argument("--plain-sample", type=int, default=32,
                     help="served: requests re-solved with the plain path for its rate")
     return ap.parse_args()
 
@@ -872,7 +881,10 @@ def measure_served(args, dist, requests, rate, max_iter, rel_tol):
     srv.close()
 
     # the plain path on a sample of the same requests, same iteration counts
-    sample = srv.done[:max(1, min(args.plain_sample, len(srv.done)))]
+    # a uniform sample of the stream (in arrival order), not the first to finish
+    by_arrival = sorted(srv.done, key=lambda r: r.arrival)
+    ns = max(1, min(args.plain_sample, len(by_arrival)))
+    sample = [by_arrival[(2 * k + 1) * len(by_arrival) // (2 * ns)] for k in range(ns)]
     t0 = time.perf_counter()
     for r in sample:
         G.plain_solve(r.mesh, r.mach, r.alpha, r.iterations, dt)
