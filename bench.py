@@ -94,6 +94,8 @@ def parse():
     ap.add_argument("--renumber", action="store_true",
                     help="plain mode: renumber the sets for locality (op2b_set_renumber)")
     ap.add_argument("--nn", type=int, default=512, help="jac mode: NN (grid of (NN-1)^2 nodes)")
+    ap.add_argument("--jac-variant", type=int, default=1, choices=[1, 2],
+                    help="jac mode: jac1 (float, one component) or jac2 (A double[3], u[2])")
     ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served", "jac"],
                     help="plain: the 720k single-mesh iteration (default); batched: many "
                          "instances per launch; served: a Poisson request stream")
@@ -922,10 +924,10 @@ def measure_served(args, dist, requests, rate, max_iter, rel_tol):
     return line
 
 
-def run_reference_jac(NN, niter, threads=None):
-    """The reference's OpenMP jac1 (oracle/_ref/jac1_op) at NN, niter; returns
-    (iterations/s from its own op_timing_output, seconds, cores) or None."""
-    binary = os.path.join(ROOT, "oracle", "_ref", "jac1_op")
+def run_reference_jac(NN, niter, threads=None, variant=1):
+    """The reference's OpenMP jac1 or jac2 (oracle/_ref/jac<v>_op) at NN, niter;
+    returns (iterations/s from its own op_timing_output, seconds, cores) or None."""
+    binary = os.path.join(ROOT, "oracle", "_ref", "jac%d_op" % variant)
     if not os.path.exists(binary):
         return None
     cores = threads or os.cpu_count()
@@ -953,13 +955,13 @@ def impl_jac(args, dist):
     from oplus2_matlab_b200 import mesh as M
     lib = api.lib()
     cr = cudart()
-    NN, niter = args.nn, max(args.steps, 1)
-    jm = M.jac(NN, 1)
+    NN, niter, V = args.nn, max(args.steps, 1), args.jac_variant
+    jm = M.jac(NN, V)
     api.set_error_mode(api.ERRORS_RETURN)
     api.op_init([], 0)
     api.set_strategy(api.STRATEGY_GATHER)
     api.set_reduction(api.REDUCE_TREE)
-    J = apps.Jac(jm, 1)
+    J = apps.Jac(jm, V)
     J.iterate(max(3, args.warmup))
     api.sync()
     # e2e first: every iteration returns u_sum and u_max to the host
@@ -1005,24 +1007,29 @@ def impl_jac(args, dist):
     ok = bool(np.isfinite(u).all())
     api.op_exit()
     value = dist.world * niter / total
-    # compulsory bytes per iteration: res = 12 per edge + 12 per node (A, the
-    # map pair, u read, du read+write), update = 20 per node (r, du rw, u rw)
-    it_bytes = 12.0 * jm.nedge + 12.0 * jm.nnode + 20.0 * jm.nnode
+    # compulsory bytes per iteration: res = A and the map pair per edge, u
+    # read and du read+write per node; update = r, du rw, u rw per node.
+    # jac1: 4 + 8 per edge, 4 + 8 + (4 + 8 + 8) per node; jac2 (A double[3],
+    # u float[2], du float[3], r float[2]): 24 + 8, 8 + 24 + (8 + 24 + 16)
+    if V == 1:
+        it_bytes = 12.0 * jm.nedge + 12.0 * jm.nnode + 20.0 * jm.nnode
+    else:
+        it_bytes = 32.0 * jm.nedge + 32.0 * jm.nnode + 48.0 * jm.nnode
     peak, peak_kind = measured_peak()
     cpu = None
     if not args.no_cpu_baseline and dist.rank == 0 and dist.world == 1:
-        r = run_reference_jac(NN, min(niter, 100))
+        r = run_reference_jac(NN, min(niter, 100), variant=V)
         if r and r[0]:
             cpu = {"value": r[0], "unit": "iters/s", "cores": r[2], "kind": "reference",
-                   "sample": "%d iterations at NN=%d (reference jac1_op, OpenMP, sum of its "
-                             "op_timing_output)" % (min(niter, 100), NN)}
+                   "sample": "%d iterations at NN=%d (reference jac%d_op, OpenMP, sum of its "
+                             "op_timing_output)" % (min(niter, 100), NN, V)}
     line = {
-        "metric": "jac1 iters/s", "value": value, "unit": "iters/s", "n_gpus": dist.world,
+        "metric": "jac%d iters/s" % V, "value": value, "unit": "iters/s", "n_gpus": dist.world,
         "steps": niter, "warmup": max(3, args.warmup), "ms_per_step": 1e3 * total / niter,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic: the reference's jac1 grid generator (jac1/jac.cpp:65-117)",
-        "config": {"workload": "jac1 NN=%d: %d nodes, %d edges, one iteration (res + update) "
-                               "per step" % (NN, jm.nnode, jm.nedge),
+        "data": "synthetic: the reference's jac%d grid generator (jac%d/jac.cpp)" % (V, V),
+        "config": {"workload": "jac%d NN=%d: %d nodes, %d edges, one iteration (res + update) "
+                               "per step" % (V, NN, jm.nnode, jm.nedge),
                    "l2": "flushed before every step", "parallelism": "single GPU"},
         "roofline": {"bound": "hbm", "kernel": "res + update (one iteration)",
                      "achieved": it_bytes * value / dist.world / 1e9, "peak": peak,
