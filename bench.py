@@ -863,15 +863,17 @@ def measure_served(args, dist, requests, rate, max_iter, rel_tol):
     clocks = Clocks(dist.local)
     dist.barrier()
     t0 = time.perf_counter()
-    srv.clock = lambda: time.perf_counter() - t0
+    base = srv.now()  # arrivals and latencies on the C++ server's clock
+    for r in reqs:
+        r.arrival += base
     nxt = 0
     while nxt < len(reqs) or not srv.idle():
-        now = srv.clock()
+        now = srv.now()
         while nxt < len(reqs) and reqs[nxt].arrival <= now:
             srv.submit(reqs[nxt])
             nxt += 1
         if srv.idle() and nxt < len(reqs):
-            time.sleep(max(0.0, min(reqs[nxt].arrival - srv.clock(), 0.01)))
+            time.sleep(max(0.0, min(reqs[nxt].arrival - srv.now(), 0.01)))
             continue
         srv.step()
     wall = dist.max(time.perf_counter() - t0)

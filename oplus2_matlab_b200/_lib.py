@@ -78,6 +78,31 @@ class op2b_mesh(C.Structure):
 
 _P = C.c_void_p
 
+_PMESH = C.POINTER(op2b_mesh)
+# include/op2b_serve.h: the group table the server drives, and its records
+ADD_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_longlong, _PMESH, C.c_double, C.c_double, C.c_int,
+                     C.c_double)
+RUN_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int)
+POLL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_int), C.c_int)
+HISTORY_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_int)
+FETCHQ_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_void_p)
+REMOVE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int)
+SOLVE_BYTES_FN = C.CFUNCTYPE(C.c_longlong, C.c_void_p, C.c_longlong, _PMESH, C.c_int)
+DEVICE_BYTES_FN = C.CFUNCTYPE(C.c_longlong, C.c_void_p)
+NOW_FN = C.CFUNCTYPE(C.c_double, C.c_void_p)
+
+
+class op2b_group_ops(C.Structure):
+    _fields_ = [("ctx", C.c_void_p), ("add", ADD_FN), ("run", RUN_FN), ("poll", POLL_FN),
+                ("history", HISTORY_FN), ("fetch_q", FETCHQ_FN), ("remove", REMOVE_FN),
+                ("solve_bytes", SOLVE_BYTES_FN), ("device_bytes", DEVICE_BYTES_FN),
+                ("now", NOW_FN)]
+
+
+class op2b_served(C.Structure):
+    _fields_ = [("rid", C.c_longlong), ("sid", C.c_int), ("iterations", C.c_int),
+                ("arrival", C.c_double), ("admitted", C.c_double), ("finished", C.c_double)]
+
 # (name, restype, argtypes) of every exported entry point
 PROTOTYPES = [
     # op_lib_core.h
@@ -135,6 +160,25 @@ PROTOTYPES = [
     ("op2b_checkpoint_file", C.c_int, [C.c_char_p]),
     ("op_checkpoint", C.c_int, []),
     ("op2b_renumber_order", C.c_int, [op_set, C.POINTER(C.c_int)]),
+    # op2b_serve.h
+    ("op2b_group_ops_fill", C.c_int, [_P, C.POINTER(op2b_group_ops)]),
+    ("op2b_server_create", _P, [C.POINTER(op2b_group_ops), C.c_longlong, C.c_int, C.c_int,
+                                C.c_int, C.c_int, C.c_int]),
+    ("op2b_server_destroy", None, [_P]),
+    ("op2b_server_submit", C.c_int, [_P, C.c_longlong, _PMESH, C.c_double, C.c_double, C.c_int,
+                                     C.c_double, C.c_double]),
+    ("op2b_server_step", C.c_int, [_P]),
+    ("op2b_server_done", C.c_int, [_P, C.POINTER(op2b_served), C.c_int]),
+    ("op2b_server_history", C.c_int, [_P, C.c_longlong, C.POINTER(C.c_double), C.c_int]),
+    ("op2b_server_q", C.c_int, [_P, C.c_longlong, _P]),
+    ("op2b_server_release", None, [_P, C.c_longlong]),
+    ("op2b_server_active", C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_int), C.c_int]),
+    ("op2b_server_queued", C.c_int, [_P]),
+    ("op2b_server_peak_active", C.c_int, [_P]),
+    ("op2b_server_idle", C.c_int, [_P]),
+    ("op2b_server_now", C.c_double, [_P]),
+    ("op2b_server_latency", C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                      C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("op2b_renumber_seconds", C.c_double, []),
     ("op2b_decl_const_named", None, [C.c_int, C.c_char_p, C.c_int, _P, C.c_char_p]),
     ("op2b_capture_begin", C.c_int, [C.c_int]),

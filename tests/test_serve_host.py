@@ -97,3 +97,22 @@ def test_latency_stats():
     st = S.latency_stats(reqs)
     assert abs(st["p50_s"] - 50.5) < 1e-9 and abs(st["p99_s"] - 99.01) < 1e-9
     assert st["max_s"] == 100.0
+
+
+def test_server_latency_record_matches_latency_stats():
+    """The C++ server's own latency record (op2b_server_latency) against the
+    same numbers computed from the finished requests."""
+    import ctypes as C
+    t = iter(range(0, 10000, 3)).__next__
+    srv = S.Server(budget_bytes=350, iters_per_step=4, clock=t, group=StandInGroup())
+    for i in range(7):
+        srv.submit(request(i, 1 + i % 3, 6 + 2 * i, arrival=float(i)))
+    while not srv.idle():
+        srv.step()
+    vals = [C.c_double() for _ in range(4)]
+    assert srv.lib.op2b_server_latency(srv.h, *[C.byref(v) for v in vals]) == 0
+    st = S.latency_stats(srv.done)
+    for got, key in zip(vals, ("p50_s", "p99_s", "mean_s", "max_s")):
+        assert abs(got.value - st[key]) < 1e-12, key
+    assert srv.queued == 0 and not srv.active
+    srv.close()
