@@ -96,7 +96,8 @@ def parse():
     ap.add_argument("--nn", type=int, default=512, help="jac mode: NN (grid of (NN-1)^2 nodes)")
     ap.add_argument("--jac-variant", type=int, default=1, choices=[1, 2],
                     help="jac mode: jac1 (float, one component) or jac2 (A double[3], u[2])")
-    ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served", "jac"],
+    ap.add_argument("--mode", default="plain",
+                    choices=["plain", "batched", "served", "jac", "layout"],
                     help="plain: the 720k single-mesh iteration (default); batched: many "
                          "instances per launch; served: a Poisson request stream")
     ap.add_argument("--instances", type=int, default=64, help="batched: instances")
@@ -1049,6 +1050,44 @@ def impl_jac(args, dist):
         print(json.dumps(line))
 
 
+def impl_layout(args, dist):
+    """--mode layout: res_calc's flux pass on the 720k mesh with the datasets
+    stored AoS (the library's layout) and SoA, same arithmetic, outputs
+    compared bit for bit (op2b_layout_ab); L2 flushed before each launch."""
+    from oplus2_matlab_b200 import api, apps
+    from oplus2_matlab_b200 import mesh as M
+    lib = api.lib()
+    mesh = plain_mesh(args)
+    K = apps.airfoil_consts(np.float32)
+    rng = np.random.default_rng(MESH_SEED)
+    q = (np.tile(K["qinf"], (mesh.ncell, 1)) *
+         (1.0 + 0.01 * rng.standard_normal((mesh.ncell, 4)))).astype(np.float32)
+    adt = rng.uniform(1.0, 50.0, mesh.ncell).astype(np.float32)
+    x = np.ascontiguousarray(mesh.x(np.float32), np.float32)
+    pe = np.ascontiguousarray(mesh.edge, np.int32)
+    pc = np.ascontiguousarray(mesh.ecell, np.int32)
+    ta, ts = C.c_double(), C.c_double()
+    clocks = Clocks(dist.local)
+    rc = lib.op2b_layout_ab(mesh.nedge, mesh.ncell, mesh.nnode, pe.ctypes.data, pc.ctypes.data,
+                            x.ctypes.data, q.ctypes.data, adt.ctypes.data, float(K["gm1"]),
+                            float(K["eps"]), max(3, args.steps), C.byref(ta), C.byref(ts))
+    clk = clocks.stop()
+    # compulsory bytes: pedge + pecell (16 per edge), q (16) and adt (4) per
+    # cell, x (8) per node, the flux record written (16 per edge)
+    algo = 32.0 * mesh.nedge + 20.0 * mesh.ncell + 8.0 * mesh.nnode
+    peak, kind = measured_peak()
+    line = {"metric": "res_calc flux pass us per launch, AoS vs SoA", "unit": "us",
+            "value": ta.value, "higher_is_better": False, "n_gpus": 1, "steps": max(3, args.steps),
+            "warmup": 1, "dtype": "f32", "data": "synthetic: 720k mesh, perturbed free stream",
+            "config": {"workload": "flux pass over %d interior edges" % mesh.nedge},
+            "aos_us": ta.value, "soa_us": ts.value, "soa_over_aos": ts.value / ta.value,
+            "outputs_bit_identical": rc == 0, "rc": rc,
+            "algorithmic_bytes": algo, "aos_gbs": algo / ta.value / 1e3,
+            "soa_gbs": algo / ts.value / 1e3, "peak_gbs": peak, "peak_source": kind,
+            "clocks": clk}
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     dist = Dist()
@@ -1061,6 +1100,8 @@ def main():
             impl_served(args, dist)
         elif args.mode == "jac":
             impl_jac(args, dist)
+        elif args.mode == "layout":
+            impl_layout(args, dist)
         else:
             impl_ours(args, dist)
     finally:

@@ -170,6 +170,18 @@ long op2b_plan_validate(char const *name, op_set set, int part_size, int nargs, 
  * times its size; benchmark drivers call it between timed steps. */
 int op2b_l2_flush(void);
 
+/* Layout measurement (bench.py --mode layout): res_calc's flux pass over
+ * every interior edge of the given mesh and fields, with the datasets stored
+ * element-major (AoS, the library's layout) and component-major (SoA), the
+ * same arithmetic in the same order.  Times `iters` launches of each (L2
+ * flushed before each) into *us_aos and *us_soa (microseconds per launch).
+ * Returns 0 when both wrote bit-identical flux records, 1 when they differ,
+ * -1 on bad arguments or a CUDA failure.  No counterpart in the reference
+ * (its generated kernels stage AoS data through shared memory as SoA). */
+int op2b_layout_ab(int nedge, int ncell, int nnode, const int *pedge, const int *pecell,
+                   const float *x, const float *q, const float *adt, float gm1, float eps,
+                   int iters, double *us_aos, double *us_soa);
+
 /* Bounded waits that ran out in the library's kernels (mbarrier waits of
  * the TMA-staged per-cell pass) since the last reset; reset != 0 clears the
  * count.  Every wait gives up after one second, counts here and lets its

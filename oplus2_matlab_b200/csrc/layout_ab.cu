@@ -1,0 +1,148 @@
+// layout_ab.cu -- the measurement behind the library's choice of AoS device
+// layout: res_calc's flux pass over every interior edge, run once with the
+// datasets element-major (AoS, as the library stores them: q as one 16-byte
+// record per cell, x as one 8-byte record per node) and once component-major
+// (SoA: q as four arrays, x as two, the layout the reference's generated
+// CUDA stubs stage data in, in shared memory).  Both
+// kernels do the same arithmetic in the same order (airfoil/res_calc.h via
+// res_flux) and write the same flux records, so their outputs must be
+// bit-identical; only the gathers differ: AoS fetches a cell's q with one
+// 16-byte load and a node's x with one 8-byte load, SoA with four and two
+// 4-byte loads from separate arrays.
+//
+// op2b_layout_ab is a measurement entry point (bench.py --mode layout), not
+// a loop: it uploads the given mesh and fields, times `iters` launches of
+// each kernel (each after an L2 flush) with CUDA events, and frees
+// everything.
+
+#include <stdio.h>
+#include <string.h>
+
+#include <vector>
+
+#include "airfoil_math.cuh"
+#include "internal.h"
+
+namespace op2b {
+namespace {
+
+__global__ void __launch_bounds__(256) k_flux_aos(int ne, const int2 *__restrict__ pedge,
+                                                  const int2 *__restrict__ pecell,
+                                                  const float *__restrict__ x,
+                                                  const float *__restrict__ q,
+                                                  const float *__restrict__ adt,
+                                                  float *__restrict__ v, float gm1, float eps) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+    const int2 nn = __ldg(pedge + e), cc = __ldg(pecell + e);
+    float p[2], s[2], q1[4], q2[4], f[4];
+    ld4(q + 4 * (size_t)cc.x, q1);
+    ld4(q + 4 * (size_t)cc.y, q2);
+    ld2(x + 2 * (size_t)nn.x, p);
+    ld2(x + 2 * (size_t)nn.y, s);
+    res_flux(p, s, q1, q2, __ldg(adt + cc.x), __ldg(adt + cc.y), gm1, eps, f);
+    st4(v + 4 * (size_t)e, f);
+  }
+}
+
+struct SoA {
+  const float *q0, *q1, *q2, *q3, *x0, *x1;
+};
+
+__global__ void __launch_bounds__(256) k_flux_soa(int ne, const int2 *__restrict__ pedge,
+                                                  const int2 *__restrict__ pecell, SoA d,
+                                                  const float *__restrict__ adt,
+                                                  float *__restrict__ v, float gm1, float eps) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+    const int2 nn = __ldg(pedge + e), cc = __ldg(pecell + e);
+    const float q1[4] = {__ldg(d.q0 + cc.x), __ldg(d.q1 + cc.x), __ldg(d.q2 + cc.x),
+                         __ldg(d.q3 + cc.x)};
+    const float q2[4] = {__ldg(d.q0 + cc.y), __ldg(d.q1 + cc.y), __ldg(d.q2 + cc.y),
+                         __ldg(d.q3 + cc.y)};
+    const float p[2] = {__ldg(d.x0 + nn.x), __ldg(d.x1 + nn.x)};
+    const float s[2] = {__ldg(d.x0 + nn.y), __ldg(d.x1 + nn.y)};
+    float f[4];
+    res_flux(p, s, q1, q2, __ldg(adt + cc.x), __ldg(adt + cc.y), gm1, eps, f);
+    st4(v + 4 * (size_t)e, f);
+  }
+}
+
+}  // namespace
+}  // namespace op2b
+
+using namespace op2b;
+
+extern "C" int op2b_layout_ab(int nedge, int ncell, int nnode, const int *pedge,
+                              const int *pecell, const float *x, const float *q,
+                              const float *adt, float gm1, float eps, int iters,
+                              double *us_aos, double *us_soa) {
+  if (nedge <= 0 || ncell <= 0 || nnode <= 0 || !pedge || !pecell || !x || !q || !adt ||
+      iters < 1 || !us_aos || !us_soa)
+    return -1;
+  ensure_cuda();
+  if (error_pending()) return -1;
+  cudaStream_t s = rt().stream;
+  std::vector<float> qs((size_t)4 * ncell), xs((size_t)2 * nnode);
+  for (int c = 0; c < ncell; c++)
+    for (int d = 0; d < 4; d++) qs[(size_t)d * ncell + c] = q[(size_t)4 * c + d];
+  for (int n = 0; n < nnode; n++)
+    for (int d = 0; d < 2; d++) xs[(size_t)d * nnode + n] = x[(size_t)2 * n + d];
+  const size_t b_map = sizeof(int) * 2 * (size_t)nedge, b_q = sizeof(float) * 4 * (size_t)ncell,
+               b_x = sizeof(float) * 2 * (size_t)nnode, b_a = sizeof(float) * (size_t)ncell,
+               b_v = sizeof(float) * 4 * (size_t)nedge;
+  void *pe = dev_alloc(b_map), *pc = dev_alloc(b_map), *dq = dev_alloc(b_q), *dx = dev_alloc(b_x),
+       *dqs = dev_alloc(b_q), *dxs = dev_alloc(b_x), *da = dev_alloc(b_a), *va = dev_alloc(b_v),
+       *vs = dev_alloc(b_v);
+  int rc = -1;
+  std::vector<cudaEvent_t> ev(4 * iters, nullptr);
+  if (pe && pc && dq && dx && dqs && dxs && da && va && vs) {
+    OP2B_CUDA(cudaMemcpyAsync(pe, pedge, b_map, cudaMemcpyHostToDevice, s));
+    OP2B_CUDA(cudaMemcpyAsync(pc, pecell, b_map, cudaMemcpyHostToDevice, s));
+    OP2B_CUDA(cudaMemcpyAsync(dq, q, b_q, cudaMemcpyHostToDevice, s));
+    OP2B_CUDA(cudaMemcpyAsync(dx, x, b_x, cudaMemcpyHostToDevice, s));
+    OP2B_CUDA(cudaMemcpyAsync(dqs, qs.data(), b_q, cudaMemcpyHostToDevice, s));
+    OP2B_CUDA(cudaMemcpyAsync(dxs, xs.data(), b_x, cudaMemcpyHostToDevice, s));
+    OP2B_CUDA(cudaMemcpyAsync(da, adt, b_a, cudaMemcpyHostToDevice, s));
+    const float *fq = (const float *)dqs, *fx = (const float *)dxs;
+    SoA d{fq, fq + ncell, fq + 2 * (size_t)ncell, fq + 3 * (size_t)ncell, fx, fx + nnode};
+    const int grid = rt().num_sms * 16;
+    for (auto &e : ev) OP2B_CUDA(cudaEventCreate(&e));
+    // one untimed launch each, then alternate, each launch after an L2 flush
+    k_flux_aos<<<grid, 256, 0, s>>>(nedge, (const int2 *)pe, (const int2 *)pc,
+                                    (const float *)dx, (const float *)dq, (const float *)da,
+                                    (float *)va, gm1, eps);
+    k_flux_soa<<<grid, 256, 0, s>>>(nedge, (const int2 *)pe, (const int2 *)pc, d,
+                                    (const float *)da, (float *)vs, gm1, eps);
+    for (int i = 0; i < iters; i++) {
+      op2b_l2_flush();
+      OP2B_CUDA(cudaEventRecord(ev[4 * i], s));
+      k_flux_aos<<<grid, 256, 0, s>>>(nedge, (const int2 *)pe, (const int2 *)pc,
+                                      (const float *)dx, (const float *)dq, (const float *)da,
+                                      (float *)va, gm1, eps);
+      OP2B_CUDA(cudaEventRecord(ev[4 * i + 1], s));
+      op2b_l2_flush();
+      OP2B_CUDA(cudaEventRecord(ev[4 * i + 2], s));
+      k_flux_soa<<<grid, 256, 0, s>>>(nedge, (const int2 *)pe, (const int2 *)pc, d,
+                                      (const float *)da, (float *)vs, gm1, eps);
+      OP2B_CUDA(cudaEventRecord(ev[4 * i + 3], s));
+    }
+    OP2B_CUDA(cudaStreamSynchronize(s));
+    double ta = 0, ts = 0;
+    for (int i = 0; i < iters; i++) {
+      float ms = 0;
+      OP2B_CUDA(cudaEventElapsedTime(&ms, ev[4 * i], ev[4 * i + 1]));
+      ta += ms;
+      OP2B_CUDA(cudaEventElapsedTime(&ms, ev[4 * i + 2], ev[4 * i + 3]));
+      ts += ms;
+    }
+    *us_aos = 1e3 * ta / iters;
+    *us_soa = 1e3 * ts / iters;
+    std::vector<float> ha((size_t)4 * nedge), hs((size_t)4 * nedge);
+    OP2B_CUDA(cudaMemcpy(ha.data(), va, b_v, cudaMemcpyDeviceToHost));
+    OP2B_CUDA(cudaMemcpy(hs.data(), vs, b_v, cudaMemcpyDeviceToHost));
+    rc = memcmp(ha.data(), hs.data(), b_v) == 0 ? 0 : 1;  // 1: outputs differ
+  }
+  for (auto &e : ev)
+    if (e) cudaEventDestroy(e);
+  for (void *p : {pe, pc, dq, dx, dqs, dxs, da, va, vs}) dev_free(p);
+  return error_pending() ? -1 : rc;
+}
