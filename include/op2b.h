@@ -176,8 +176,8 @@ int op2b_l2_flush(void);
  * same arithmetic in the same order.  Times `iters` launches of each (L2
  * flushed before each) into *us_aos and *us_soa (microseconds per launch).
  * Returns 0 when both wrote bit-identical flux records, 1 when they differ,
- * -1 on bad arguments or a CUDA failure.  No counterpart in the reference
- * (its generated kernels stage AoS data through shared memory as SoA). */
+ * -1 on bad arguments or a CUDA failure.  No counterpart in the reference,
+ * whose developer notes weigh the two layouts (doc/dev.tex:529-651). */
 int op2b_layout_ab(int nedge, int ncell, int nnode, const int *pedge, const int *pecell,
                    const float *x, const float *q, const float *adt, float gm1, float eps,
                    int iters, double *us_aos, double *us_soa);

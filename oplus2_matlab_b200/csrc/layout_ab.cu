@@ -2,8 +2,8 @@
 // layout: res_calc's flux pass over every interior edge, run once with the
 // datasets element-major (AoS, as the library stores them: q as one 16-byte
 // record per cell, x as one 8-byte record per node) and once component-major
-// (SoA: q as four arrays, x as two, the layout the reference's generated
-// CUDA stubs stage data in, in shared memory).  Both
+// (SoA: q as four arrays, x as two; the reference's developer notes weigh
+// the two, doc/dev.tex:529-651).  Both
 // kernels do the same arithmetic in the same order (airfoil/res_calc.h via
 // res_flux) and write the same flux records, so their outputs must be
 // bit-identical; only the gathers differ: AoS fetches a cell's q with one
