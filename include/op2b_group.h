@@ -87,15 +87,20 @@ int op2b_group_active(op2b_group g); /* solves in the launches (joined, not stop
  * of values (<= 0, the default: all solves in one block).  Results do not
  * depend on it. */
 int op2b_group_set_block_bytes(op2b_group g, long long bytes);
+/* Blocks are dealt round-robin to n streams (1..8) inside the captured
+ * iteration, so independent blocks' launches overlap (one block's per-cell
+ * pass beside another's flux pass).  Results do not depend on it. */
+int op2b_group_set_streams(op2b_group g, int n);
 
 /* Launch shape of the flux pass: edges per tile (multiple of 256, 256..8192).
  * Results do not depend on it; op2b_group_autotune picks it by timing. */
 int op2b_group_set_edge_tile(op2b_group g, int edges_per_tile);
 int op2b_group_edge_tile(op2b_group g);
 /* Time `iters` iterations at each candidate edge tile, then at each block
- * size (24, 48, 96 MiB, one block), on the current active solves, putting
- * their state back after each trial; keeps the fastest of each and returns
- * the edge tile. */
+ * size and stream count (one block on one stream; 96 or 48 MiB blocks on
+ * one stream; 48 or 24 MiB on two; 24 MiB on three; 12 MiB on four), on the
+ * current active solves, putting their state back after each trial; keeps
+ * the fastest of each and returns the edge tile. */
 int op2b_group_autotune(op2b_group g, int iters);
 
 #ifdef __cplusplus

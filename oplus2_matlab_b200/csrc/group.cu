@@ -398,6 +398,7 @@ struct GroupBase {
   virtual int active() = 0;
   virtual int set_edge_tile(int e) = 0;
   virtual int set_block_bytes(long long bytes) = 0;
+  virtual int set_streams(int n) = 0;
   virtual int edge_tile() = 0;
   virtual int autotune(int iters) = 0;
 };
@@ -420,6 +421,13 @@ struct Group : GroupBase {
   };
 
   cudaStream_t cs = nullptr, us = nullptr;  // iterations; admission
+  // further streams of the captured iteration: blocks of solves are dealt
+  // round-robin to `nstreams` streams (cs first), so independent blocks'
+  // passes overlap (one block's latency-bound per-cell pass beside
+  // another's flux pass); fork and join are events inside the capture
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> side_ev;  // [0] fork, [1..] joins
+  int nstreams = 1;
   std::vector<Solve> solves;
   SolveDev<T> *d_sd = nullptr;
   SolveState *d_st = nullptr;
@@ -468,6 +476,8 @@ struct Group : GroupBase {
     if (mirror_ev) cudaEventDestroy(mirror_ev);
     if (cs) cudaStreamDestroy(cs);
     if (us) cudaStreamDestroy(us);
+    for (cudaStream_t x : side) cudaStreamDestroy(x);
+    for (cudaEvent_t e : side_ev) cudaEventDestroy(e);
   }
 
   void release(Solve &s) {
@@ -694,8 +704,29 @@ struct Group : GroupBase {
     }
     if (nactive == 0) return;
     cudaGraph_t graph = nullptr;
+    const int K = std::max(1, std::min(nstreams, (int)blocks.size()));
+    while ((int)side.size() < K - 1) {  // created outside the capture
+      cudaStream_t x;
+      OP2B_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+      side.push_back(x);
+    }
+    while ((int)side_ev.size() < K) {
+      cudaEvent_t e;
+      OP2B_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      side_ev.push_back(e);
+    }
     OP2B_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    for (const Block &b : blocks) iteration(b);
+    if (K > 1) {
+      OP2B_CUDA(cudaEventRecord(side_ev[0], cs));
+      for (int k = 1; k < K; k++) OP2B_CUDA(cudaStreamWaitEvent(side[k - 1], side_ev[0], 0));
+    }
+    for (size_t i = 0; i < blocks.size(); i++)
+      iteration(blocks[i], i % K == 0 ? cs : side[i % K - 1]);
+    if (K > 1)
+      for (int k = 1; k < K; k++) {
+        OP2B_CUDA(cudaEventRecord(side_ev[k], side[k - 1]));
+        OP2B_CUDA(cudaStreamWaitEvent(cs, side_ev[k], 0));
+      }
     OP2B_CUDA(cudaStreamEndCapture(cs, &graph));
     if (graph) {
       OP2B_CUDA(cudaGraphInstantiate(&exec, graph, 0));
@@ -704,7 +735,7 @@ struct Group : GroupBase {
     changed = false;
   }
 
-  void iteration(const Block &b) {
+  void iteration(const Block &b, cudaStream_t cs) {
     const Tile *ct = d_ct + b.ct0, *et = d_et + b.et0;
     if (!rotate)
       launch_pdl(k_grp_save_adt<T>, b.nct, kThreads, 0, cs, ct, (const SolveDev<T> *)d_sd,
@@ -867,6 +898,16 @@ struct Group : GroupBase {
     return 0;
   }
 
+  int set_streams(int n) override {
+    if (n < 1 || n > 8) {
+      fail(-1, "op2b_group error -- %d streams: 1 to 8\n", n);
+      return -1;
+    }
+    if (n != nstreams) changed = true;
+    nstreams = n;
+    return 0;
+  }
+
   int set_edge_tile(int e) override {
     if (e < kThreads || e > 8192 || e % kThreads) {
       fail(-1, "op2b_group error -- edge tile %d: a multiple of %d in [%d, 8192]\n", e, kThreads,
@@ -941,18 +982,24 @@ struct Group : GroupBase {
       }
     }
     etile = best;
-    const size_t blk[] = {24u << 20, 48u << 20, 96u << 20, ~(size_t)0};
-    size_t best_blk = block_bytes;
+    // blocks of solves (bytes of flux values per block) x streams they are
+    // dealt to; one block on one stream is the plain form
+    const std::pair<size_t, int> blk[] = {{~(size_t)0, 1}, {96u << 20, 1}, {48u << 20, 1},
+                                          {48u << 20, 2}, {24u << 20, 2}, {24u << 20, 3},
+                                          {12u << 20, 4}};
+    std::pair<size_t, int> best_blk{block_bytes, nstreams};
     best_ms = 1e30f;
-    for (size_t bb : blk) {
-      block_bytes = bb;
+    for (const auto &bb : blk) {
+      block_bytes = bb.first;
+      nstreams = bb.second;
       const float ms = trial();
       if (ms < best_ms) {
         best_ms = ms;
         best_blk = bb;
       }
     }
-    block_bytes = best_blk;
+    block_bytes = best_blk.first;
+    nstreams = best_blk.second;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     OP2B_CUDA(cudaFreeAsync(snap, cs));
@@ -1032,6 +1079,7 @@ int op2b_group_set_block_bytes(op2b_group g, long long bytes) {
   GROUP_CALL(set_block_bytes(bytes));
 }
 int op2b_group_edge_tile(op2b_group g) { GROUP_CALL(edge_tile()); }
+int op2b_group_set_streams(op2b_group g, int n) { GROUP_CALL(set_streams(n)); }
 int op2b_group_autotune(op2b_group g, int iters) { GROUP_CALL(autotune(iters)); }
 
 }  // extern "C"

@@ -56,11 +56,17 @@ def flow_qinf(mach, alpha_deg, dtype=np.float32):
     return q, c
 
 
-def plain_solve(mesh, mach, alpha_deg, niter, dtype=np.float32, strategy=1):
-    """One solve through the OP2 C API; returns (q, rms history, AppTiming)."""
+def plain_solve(mesh, mach, alpha_deg, niter, dtype=np.float32, strategy=1, q_out=None):
+    """One solve through the OP2 C API; returns (q, rms history, AppTiming).
+    q_out: an (ncell, 4) array of dtype to hold q (e.g. in pinned memory);
+    default a new one."""
     dt = np.dtype(dtype)
     qinf, _ = flow_qinf(mach, alpha_deg, dt)
-    q = np.ascontiguousarray(np.tile(qinf, (mesh.ncell, 1)))
+    if q_out is None:
+        q = np.ascontiguousarray(np.tile(qinf, (mesh.ncell, 1)))
+    else:
+        q = q_out
+        q[...] = qinf
     rms = np.zeros(niter, np.float64)
     m, keep = M.as_struct(mesh)
     t = AppTiming()
@@ -158,8 +164,8 @@ class Group:
                                                       min(n, max_n)), "op2b_group_history")
         return out[:got]
 
-    def fetch_q(self, sid):
-        q = np.zeros((self.ncell[sid], 4), self.dtype)
+    def fetch_q(self, sid, out=None):
+        q = np.zeros((self.ncell[sid], 4), self.dtype) if out is None else out
         self._check(self.lib.op2b_group_fetch_q(self.h, sid, q.ctypes.data), "op2b_group_fetch_q")
         return q
 
@@ -183,6 +189,9 @@ class Group:
     @edge_tile.setter
     def edge_tile(self, e):
         self._check(self.lib.op2b_group_set_edge_tile(self.h, int(e)), "op2b_group_set_edge_tile")
+
+    def set_streams(self, n):
+        self._check(self.lib.op2b_group_set_streams(self.h, int(n)), "op2b_group_set_streams")
 
     def set_block_bytes(self, nbytes):
         self._check(self.lib.op2b_group_set_block_bytes(self.h, int(nbytes)),

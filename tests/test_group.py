@@ -170,3 +170,27 @@ def test_autotune_keeps_state_and_results(op2):
     b.run(niter)
     assert b.fetch_q(ib).tobytes() == qa.tobytes()
     b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("block_bytes,streams", [(1 << 20, 2), (1 << 19, 3), (-1, 4)])
+def test_blocks_on_several_streams_give_the_same_solves(op2, block_bytes, streams):
+    """Blocks of solves dealt to several streams of the captured iteration
+    (their passes overlap) leave every solve bit-identical, including one
+    that stops early inside the run."""
+    niter = 15
+    specs = [((40, 60), 0.45, -1.0, niter), ((30, 45), 0.6, 2.0, niter),
+             ((20, 30), 0.35, 5.0, 7), ((30, 45), 0.5, 0.0, niter), ((20, 30), 0.7, 3.0, niter)]
+    ref = G.Group()
+    ids = [ref.add(mesh(*ij), m, a, n) for ij, m, a, n in specs]
+    ref.run(niter)
+    want = [(ref.fetch_q(i).tobytes(), ref.history(i).tobytes()) for i in ids]
+    ref.close()
+    g = G.Group()
+    g.set_block_bytes(block_bytes)
+    g.set_streams(streams)
+    ids = [g.add(mesh(*ij), m, a, n) for ij, m, a, n in specs]
+    g.run(niter)
+    got = [(g.fetch_q(i).tobytes(), g.history(i).tobytes()) for i in ids]
+    g.close()
+    assert got == want
