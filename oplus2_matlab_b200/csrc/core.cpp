@@ -6,7 +6,10 @@
 #include <stdarg.h>
 #include <sys/time.h>
 
+#include <algorithm>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "internal.h"
 
@@ -147,6 +150,32 @@ op_set op_decl_set(int size, char const *name) {
 }
 
 // common/op_lib_core.c:121-169
+// 1 when some entry of imap[0, n) is outside [0, lim): one vectorisable
+// pass, split over host threads for large maps (the check reads every entry
+// of a multi-million-entry map; one thread streams it at about 15 GB/s)
+static unsigned range_check(const int *imap, size_t n, unsigned lim) {
+  auto part = [&](size_t a, size_t b) {
+    unsigned bad = 0;
+    for (size_t i = a; i < b; i++) bad |= (unsigned)((unsigned)imap[i] >= lim);
+    return bad;
+  };
+  const unsigned hw = std::thread::hardware_concurrency();
+  const size_t nt = n < ((size_t)1 << 20) || hw < 2 ? 1 : std::min<size_t>(8, hw);
+  if (nt == 1) return part(0, n);
+  std::vector<unsigned> bad(nt, 0);
+  std::vector<std::thread> th;
+  const size_t chunk = (n + nt - 1) / nt;
+  for (size_t t = 1; t < nt; t++)
+    th.emplace_back([&, t] { bad[t] = part(std::min(n, t * chunk), std::min(n, (t + 1) * chunk)); });
+  bad[0] = part(0, std::min(n, chunk));
+  unsigned any = bad[0];
+  for (size_t t = 1; t < nt; t++) {
+    th[t - 1].join();
+    any |= bad[t];
+  }
+  return any;
+}
+
 op_map op_decl_map(op_set from, op_set to, int dim, int *imap, char const *name) {
   if (from == nullptr) {
     fail(-1, " op_decl_map error -- invalid 'from' set for map %s\n", name);
@@ -165,8 +194,7 @@ op_map op_decl_map(op_set from, op_set to, int dim, int *imap, char const *name)
   // bad entry for the message
   const size_t nent = (size_t)dim * from->size;
   const unsigned lim = (unsigned)to->size;
-  unsigned bad = 0;
-  for (size_t i = 0; i < nent; i++) bad |= (unsigned)((unsigned)imap[i] >= lim);
+  unsigned bad = range_check(imap, nent, lim);
   if (bad)
     for (int d = 0; d < dim; d++)
       for (int n = 0; n < from->size; n++) {

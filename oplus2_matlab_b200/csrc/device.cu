@@ -112,6 +112,14 @@ cudaMemPool_t pool() {
 }
 }  // namespace
 
+// stream-ordered scratch (plan building, the group engine's solves) from
+// the same pool: cudaMallocAsync's default pool hands freed memory back at
+// once, so each allocation maps pages again
+cudaError_t pool_malloc_async(void **p, size_t bytes, cudaStream_t s) {
+  cudaMemPool_t mp = pool();
+  return mp ? cudaMallocFromPoolAsync(p, bytes, mp, s) : cudaMallocAsync(p, bytes, s);
+}
+
 void *dev_alloc(size_t bytes) {
   void *p = nullptr;
   if (bytes == 0) bytes = 16;

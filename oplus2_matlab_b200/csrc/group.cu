@@ -538,7 +538,7 @@ struct Group : GroupBase {
     s.tol = tol;
     size_t off[16];
     const size_t tot = layout(s.nnode, s.ncell, s.nedge, s.nbedge, max_iter, off);
-    if (cudaMallocAsync(&s.block, tot, us) != cudaSuccess) {
+    if (pool_malloc_async(&s.block, tot, us) != cudaSuccess) {
       cudaGetLastError();
       fail(-1, "op2b_group_add error -- out of device memory (%zu bytes)\n", tot);
       return -1;
@@ -585,7 +585,7 @@ struct Group : GroupBase {
       return -1;
     }
     d.W = W;
-    if (cudaMallocAsync((void **)&s.ell, sizeof(int) * W * (size_t)s.ncell, us) != cudaSuccess) {
+    if (pool_malloc_async((void **)&s.ell, sizeof(int) * W * (size_t)s.ncell, us) != cudaSuccess) {
       cudaGetLastError();
       cudaFreeAsync(s.block, us);
       fail(-1, "op2b_group_add error -- out of device memory\n");
@@ -615,8 +615,8 @@ struct Group : GroupBase {
     while (nc < n) nc *= 2;
     SolveDev<T> *sd = nullptr;
     SolveState *st = nullptr, *hs = nullptr;
-    OP2B_CUDA(cudaMallocAsync((void **)&sd, sizeof(SolveDev<T>) * nc, cs));
-    OP2B_CUDA(cudaMallocAsync((void **)&st, sizeof(SolveState) * nc, cs));
+    OP2B_CUDA(pool_malloc_async((void **)&sd, sizeof(SolveDev<T>) * nc, cs));
+    OP2B_CUDA(pool_malloc_async((void **)&st, sizeof(SolveState) * nc, cs));
     OP2B_CUDA(cudaMallocHost((void **)&hs, sizeof(SolveState) * nc));
     OP2B_CUDA(cudaMemsetAsync(st, 0, sizeof(SolveState) * nc, cs));
     if (cap) {
@@ -643,7 +643,7 @@ struct Group : GroupBase {
     const size_t need = std::max<size_t>(h.size(), 1);
     if (need > dcap) {
       if (dptr) OP2B_CUDA(cudaFreeAsync(dptr, cs));
-      OP2B_CUDA(cudaMallocAsync((void **)&dptr, sizeof(Tile) * need, cs));
+      OP2B_CUDA(pool_malloc_async((void **)&dptr, sizeof(Tile) * need, cs));
       dcap = need;
     }
     if (!h.empty())
@@ -941,7 +941,7 @@ struct Group : GroupBase {
     size_t tot = 0;
     for (auto &r : regions) tot += align256(r.second);
     void *snap = nullptr;
-    if (cudaMallocAsync(&snap, tot, cs) != cudaSuccess) {
+    if (pool_malloc_async(&snap, tot, cs) != cudaSuccess) {
       cudaGetLastError();
       return etile;  // no room to snapshot: keep the current tile
     }

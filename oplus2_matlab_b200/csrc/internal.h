@@ -133,6 +133,8 @@ void flush_pending();
 // device memory helpers (long-lived allocations)
 void *dev_alloc(size_t bytes);
 void dev_free(void *p);
+// stream-ordered scratch from the library's pool; free with cudaFreeAsync
+cudaError_t pool_malloc_async(void **p, size_t bytes, cudaStream_t s);
 void ensure_cuda();  // op_init's device part, also run lazily
 
 // timing around one loop call

@@ -479,7 +479,7 @@ long long exclusive_scan(const int *d_in, int *d_out, int n, cudaStream_t s) {
   int nch = (n + chunk - 1) / chunk;
   if (n <= 0) return 0;
   int *sums = nullptr;
-  OP2B_CUDA(cudaMallocAsync((void **)&sums, sizeof(int) * (nch + 1), s));
+  OP2B_CUDA(pool_malloc_async((void **)&sums, sizeof(int) * (nch + 1), s));
   k_scan_chunks<<<nch, 1024, 0, s>>>(d_in, d_out, n, sums, chunk);
   if (nch > 1) {
     exclusive_scan(sums, sums, nch, s);
@@ -640,10 +640,10 @@ static void build_plan(DevPlan &p) {
   for (int m = 0; m < ni; m++) tmp_total += (long long)pp.ind_k[m] * p.bsize * nb;
   int *tmp = nullptr, *d_nind = nullptr;
   long long *d_lines = nullptr, *d_lines3 = nullptr;
-  OP2B_CUDA(cudaMallocAsync((void **)&tmp, sizeof(int) * (tmp_total ? tmp_total : 1), s));
-  OP2B_CUDA(cudaMallocAsync((void **)&d_nind, sizeof(int) * (ni ? ni : 1), s));
-  OP2B_CUDA(cudaMallocAsync((void **)&d_lines, sizeof(long long) * nb * (ni ? ni : 1), s));
-  OP2B_CUDA(cudaMallocAsync((void **)&d_lines3, sizeof(long long) * nb * (ni ? ni : 1), s));
+  OP2B_CUDA(pool_malloc_async((void **)&tmp, sizeof(int) * (tmp_total ? tmp_total : 1), s));
+  OP2B_CUDA(pool_malloc_async((void **)&d_nind, sizeof(int) * (ni ? ni : 1), s));
+  OP2B_CUDA(pool_malloc_async((void **)&d_lines, sizeof(long long) * nb * (ni ? ni : 1), s));
+  OP2B_CUDA(pool_malloc_async((void **)&d_lines3, sizeof(long long) * nb * (ni ? ni : 1), s));
 
   IndOut io;
   memset(&io, 0, sizeof io);
@@ -693,7 +693,7 @@ static void build_plan(DevPlan &p) {
     int m = pp.inc_ind[sl];
     if (ind_w[m] < 0) {
       unsigned *w = nullptr;
-      OP2B_CUDA(cudaMallocAsync((void **)&w, sizeof(unsigned) * (size_t)to_sizes[m], s));
+      OP2B_CUDA(pool_malloc_async((void **)&w, sizeof(unsigned) * (size_t)to_sizes[m], s));
       ind_w[m] = (int)warr.size();
       warr.push_back(w);
       wsz.push_back(to_sizes[m]);
@@ -704,11 +704,11 @@ static void build_plan(DevPlan &p) {
   unsigned **d_warr = nullptr;
   int *d_wsz = nullptr, *d_blkcol = nullptr, *d_ncolblk = nullptr, *d_ncolors = nullptr;
   int nw = (int)warr.size();
-  OP2B_CUDA(cudaMallocAsync((void **)&d_warr, sizeof(unsigned *) * (nw ? nw : 1), s));
-  OP2B_CUDA(cudaMallocAsync((void **)&d_wsz, sizeof(int) * (nw ? nw : 1), s));
-  OP2B_CUDA(cudaMallocAsync((void **)&d_blkcol, sizeof(int) * nb, s));
-  OP2B_CUDA(cudaMallocAsync((void **)&d_ncolblk, sizeof(int) * nb, s));
-  OP2B_CUDA(cudaMallocAsync((void **)&d_ncolors, sizeof(int), s));
+  OP2B_CUDA(pool_malloc_async((void **)&d_warr, sizeof(unsigned *) * (nw ? nw : 1), s));
+  OP2B_CUDA(pool_malloc_async((void **)&d_wsz, sizeof(int) * (nw ? nw : 1), s));
+  OP2B_CUDA(pool_malloc_async((void **)&d_blkcol, sizeof(int) * nb, s));
+  OP2B_CUDA(pool_malloc_async((void **)&d_ncolblk, sizeof(int) * nb, s));
+  OP2B_CUDA(pool_malloc_async((void **)&d_ncolors, sizeof(int), s));
   if (nw) {
     OP2B_CUDA(cudaMemcpyAsync(d_warr, warr.data(), sizeof(unsigned *) * nw, cudaMemcpyHostToDevice, s));
     OP2B_CUDA(cudaMemcpyAsync(d_wsz, wsz.data(), sizeof(int) * nw, cudaMemcpyHostToDevice, s));
@@ -899,13 +899,13 @@ long validate_plan(const DevPlan &p) {
   if (!fill_params(pp, p, to_sizes)) return 1;
   unsigned long long *err = nullptr;
   int *d_to = nullptr, *seen = nullptr;
-  OP2B_CUDA(cudaMallocAsync((void **)&err, sizeof(unsigned long long), s));
+  OP2B_CUDA(pool_malloc_async((void **)&err, sizeof(unsigned long long), s));
   OP2B_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned long long), s));
-  OP2B_CUDA(cudaMallocAsync((void **)&d_to, sizeof(int) * (p.ninds ? p.ninds : 1), s));
+  OP2B_CUDA(pool_malloc_async((void **)&d_to, sizeof(int) * (p.ninds ? p.ninds : 1), s));
   if (p.ninds)
     OP2B_CUDA(cudaMemcpyAsync(d_to, to_sizes.data(), sizeof(int) * p.ninds,
                               cudaMemcpyHostToDevice, s));
-  OP2B_CUDA(cudaMallocAsync((void **)&seen, sizeof(int) * p.nblocks, s));
+  OP2B_CUDA(pool_malloc_async((void **)&seen, sizeof(int) * p.nblocks, s));
   OP2B_CUDA(cudaMemsetAsync(seen, 0, sizeof(int) * p.nblocks, s));
   IndOut io;
   memset(&io, 0, sizeof io);
@@ -931,7 +931,7 @@ long validate_plan(const DevPlan &p) {
     int m = pp.inc_ind[sl];
     if (ind_w[m] < 0) {
       unsigned *w = nullptr;
-      OP2B_CUDA(cudaMallocAsync((void **)&w, sizeof(int) * (size_t)to_sizes[m], s));
+      OP2B_CUDA(pool_malloc_async((void **)&w, sizeof(int) * (size_t)to_sizes[m], s));
       ind_w[m] = (int)owners.size();
       owners.push_back(w);
       osz.push_back(to_sizes[m]);
@@ -1102,19 +1102,19 @@ GatherPlan *get_gather_plan(op_set set, const op_arg *args, const std::vector<in
     return nullptr;
   }
   int *cnt = nullptr, *flags = nullptr, *pos = nullptr, *acnt = nullptr;
-  OP2B_CUDA(cudaMallocAsync((void **)&cnt, sizeof(int) * T, s));
+  OP2B_CUDA(pool_malloc_async((void **)&cnt, sizeof(int) * T, s));
   OP2B_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * T, s));
   const int grid = R.num_sms * 8;
   k_gather_count<<<grid, 256, 0, s>>>(sm, g.nslots, n, cnt);
-  OP2B_CUDA(cudaMallocAsync((void **)&flags, sizeof(int) * T, s));
-  OP2B_CUDA(cudaMallocAsync((void **)&pos, sizeof(int) * T, s));
+  OP2B_CUDA(pool_malloc_async((void **)&flags, sizeof(int) * T, s));
+  OP2B_CUDA(pool_malloc_async((void **)&pos, sizeof(int) * T, s));
   k_flags<<<grid, 256, 0, s>>>(cnt, T, flags);
   g.nactive = (int)exclusive_scan(flags, pos, T, s);
   int *rowcnt = cnt;
   const int *slot_of_target = nullptr;
   if (g.nactive < T) {
     g.d_active = (int *)dev_alloc(sizeof(int) * std::max(1, g.nactive));
-    OP2B_CUDA(cudaMallocAsync((void **)&acnt, sizeof(int) * std::max(1, g.nactive), s));
+    OP2B_CUDA(pool_malloc_async((void **)&acnt, sizeof(int) * std::max(1, g.nactive), s));
     k_compact_active<<<grid, 256, 0, s>>>(cnt, pos, T, g.d_active, acnt);
     rowcnt = acnt;
     slot_of_target = pos;
@@ -1125,7 +1125,7 @@ GatherPlan *get_gather_plan(op_set set, const op_arg *args, const std::vector<in
   int tot32 = (int)total;
   OP2B_CUDA(cudaMemcpyAsync(g.d_row + g.nactive, &tot32, sizeof(int), cudaMemcpyHostToDevice, s));
   int *cursor = nullptr, *long_rows = nullptr, *nlong = nullptr, *maxlen = nullptr;
-  OP2B_CUDA(cudaMallocAsync((void **)&cursor, sizeof(int) * ((size_t)g.nactive + 1), s));
+  OP2B_CUDA(pool_malloc_async((void **)&cursor, sizeof(int) * ((size_t)g.nactive + 1), s));
   OP2B_CUDA(cudaMemcpyAsync(cursor, g.d_row, sizeof(int) * ((size_t)g.nactive + 1),
                             cudaMemcpyDeviceToDevice, s));
   k_gather_scatter<<<grid, 256, 0, s>>>(sm, g.nslots, n, slot_of_target, cursor, g.d_keys);
@@ -1134,8 +1134,8 @@ GatherPlan *get_gather_plan(op_set set, const op_arg *args, const std::vector<in
   const int *to_orig = perm_new2old_dev(set), *to_dev = perm_old2new_dev(set);
   if (to_orig && nkeys)
     k_keys_through<<<grid, 256, 0, s>>>(g.d_keys, nkeys, g.nslots, to_orig);
-  OP2B_CUDA(cudaMallocAsync((void **)&long_rows, sizeof(int) * std::max(1, g.nactive), s));
-  OP2B_CUDA(cudaMallocAsync((void **)&nlong, sizeof(int) * 2, s));
+  OP2B_CUDA(pool_malloc_async((void **)&long_rows, sizeof(int) * std::max(1, g.nactive), s));
+  OP2B_CUDA(pool_malloc_async((void **)&nlong, sizeof(int) * 2, s));
   maxlen = nlong + 1;
   OP2B_CUDA(cudaMemsetAsync(nlong, 0, sizeof(int) * 2, s));
   k_sort_rows<<<grid, 256, 0, s>>>(g.d_row, g.nactive, g.d_keys, long_rows, nlong, maxlen);
@@ -1224,7 +1224,7 @@ SlotPlan *get_slot_plan(const GatherPlan *a, const GatherPlan *b) {
     cudaStream_t s = rt().stream;
     const int grid = rt().num_sms * 8;
     int *cnt = nullptr;
-    OP2B_CUDA(cudaMallocAsync((void **)&cnt, sizeof(int) * ((size_t)p.ntarget + 1), s));
+    OP2B_CUDA(pool_malloc_async((void **)&cnt, sizeof(int) * ((size_t)p.ntarget + 1), s));
     int *mx = cnt + p.ntarget;
     OP2B_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)p.ntarget + 1), s));
     k_ell_count<<<grid, 256, 0, s>>>(a->nactive, a->d_active, a->d_row, cnt);
