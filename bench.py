@@ -91,8 +91,10 @@ def parse():
     ap.add_argument("--mesh", default="400x600",
                     help="plain mode: IxJ of the NACA0012 C-mesh (3IJ cells); a trailing 's' "
                          "renumbers cells, nodes, edges and bedges from the seed (scrambled)")
-    ap.add_argument("--renumber", action="store_true",
-                    help="plain mode: renumber the sets for locality (op2b_set_renumber)")
+    ap.add_argument("--renumber", nargs="?", const="cm", default=None, choices=["cm", "rcb"],
+                    help="plain mode: renumber the sets for locality (op2b_set_renumber): "
+                         "cm = Cuthill-McKee (the default), rcb = recursive coordinate "
+                         "bisection of the node coordinates (op2b_set_renumber_coords)")
     ap.add_argument("--nn", type=int, default=512, help="jac mode: NN (grid of (NN-1)^2 nodes)")
     ap.add_argument("--jac-variant", type=int, default=1, choices=[1, 2],
                     help="jac mode: jac1 (float, one component) or jac2 (A double[3], u[2])")
@@ -396,6 +398,8 @@ def impl_ours(args, dist):
         k, v = kv.split("=")
         lib.op2b_set_tuning(k.encode(), int(v))
     A = apps.Airfoil(mesh, dt)
+    if args.renumber == "rcb":
+        assert lib.op2b_set_renumber_coords(A.p_x) == 0, api.last_error()
     stream = lib.op2b_get_stream()
 
     # warm-up: builds the plans, uploads the maps
@@ -517,7 +521,8 @@ def impl_ours(args, dist):
     e2e = None
     if not args.no_e2e:
         # three complete solves; the median is reported (the host is shared)
-        runs = [run_e2e(mesh, args.fp64, args.e2e_iters, args.strategy, dist) for _ in range(3)]
+        runs = [run_e2e(mesh, args.fp64, args.e2e_iters, args.strategy, dist, args.renumber)
+                for _ in range(3)]
         runs = [r for r in runs if r]
         if runs:
             runs.sort(key=lambda r: r["value"])
@@ -547,7 +552,7 @@ def impl_ours(args, dist):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.fp64 else "f32",
         "data": "synthetic: NACA0012 C-mesh from the reference's generator, free-stream start",
         "config": dict(plain_config(mesh.I, mesh.J, mesh_sizes(mesh), args.mesh.endswith("s")),
-                       strategy=args.strategy, renumbered=bool(args.renumber),
+                       strategy=args.strategy, renumbered=args.renumber or False,
                        renumber_seconds=renumber_s, reduction="tree",
                        l2="flushed before every step (untimed read-only sweep of 3x the 126 MB L2)",
                        timing="CUDA events around each graph launch on the library stream",
@@ -601,7 +606,7 @@ class AppTiming(C.Structure):
                 ("t_total", C.c_double), ("h2d_bytes", C.c_longlong), ("d2h_bytes", C.c_longlong)]
 
 
-def run_e2e(mesh, fp64, niter, strategy, dist):
+def run_e2e(mesh, fp64, niter, strategy, dist, renumber=None):
     """A complete solve through the C API (oplus2_matlab_b200/apps/airfoil_app.cpp):
     declarations from pinned host arrays, niter iterations with the rms read
     back after every update, q fetched to the host.  Wall-clock timed."""
@@ -610,8 +615,9 @@ def run_e2e(mesh, fp64, niter, strategy, dist):
     cr = cudart()
     lib = _lib.load()
     app = C.CDLL(os.path.join(ROOT, "oplus2_matlab_b200", "lib", "libop2b200_apps.so"))
-    app.op2b_airfoil_app.argtypes = [C.POINTER(_lib.op2b_mesh), C.c_int, C.c_int, C.c_void_p,
-                                     C.c_void_p, C.c_int, C.POINTER(AppTiming)]
+    app.op2b_airfoil_app_renumbered.argtypes = [C.POINTER(_lib.op2b_mesh), C.c_int, C.c_int,
+                                                C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                                C.POINTER(AppTiming)]
     dt = np.float64 if fp64 else np.float32
     # pinned host copies of every input
     keep = []
@@ -640,8 +646,9 @@ def run_e2e(mesh, fp64, niter, strategy, dist):
     t = AppTiming()
     api.set_error_mode(api.ERRORS_RETURN)
     dist.barrier()
-    rc = app.op2b_airfoil_app(C.byref(m), 1 if fp64 else 0, niter, q.ctypes.data,
-                              rms.ctypes.data, 1 if strategy == "gather" else 2, C.byref(t))
+    rc = app.op2b_airfoil_app_renumbered(C.byref(m), 1 if fp64 else 0, niter, q.ctypes.data,
+                                         rms.ctypes.data, 1 if strategy == "gather" else 2,
+                                         {None: 0, "cm": 1, "rcb": 2}[renumber], C.byref(t))
     total = dist.max(t.t_total)
     for p in keep:
         cr.cudaFreeHost(p)

@@ -78,6 +78,16 @@ int op2b_autotune(const char *cache_path, int iters, int allow_reorder);
  * sets, and TREE-mode global sums are summed in another order.  Returns 0,
  * or -1 when turning it off after it has been applied. */
 int op2b_set_renumber(int on);
+/* Renumber by recursive coordinate bisection (the reference's developer
+ * notes propose it, doc/dev.tex:191-210) instead of Cuthill-McKee:
+ * `coords` (1 to 3 float or double components per element) orders its own
+ * set -- each segment of the order halved at its median along its longest
+ * extent, down to single elements, coordinates compared rounded to float,
+ * ties by element number -- and the other sets follow through the maps as
+ * above.  Turns renumbering on; NULL returns to Cuthill-McKee.  Call before
+ * the first loop.  Returns 0, or -1 (bad coordinates, or after the first
+ * loop).  No reference counterpart. */
+int op2b_set_renumber_coords(op_dat coords);
 /* The new -> old order renumbering would give `set` (computed on the GPU from
  * the sets and maps declared so far).  Returns 1 if the set is reordered,
  * 0 if it keeps its numbering (new2old = identity), -1 on bad arguments. */

@@ -163,6 +163,7 @@ PROTOTYPES = [
     ("op2b_checkpoint_file", C.c_int, [C.c_char_p]),
     ("op_checkpoint", C.c_int, []),
     ("op2b_renumber_order", C.c_int, [op_set, C.POINTER(C.c_int)]),
+    ("op2b_set_renumber_coords", C.c_int, [op_dat]),
     # op2b_serve.h
     ("op2b_group_ops_fill", C.c_int, [_P, C.POINTER(op2b_group_ops)]),
     ("op2b_server_create", _P, [C.POINTER(op2b_group_ops), C.c_longlong, C.c_int, C.c_int,

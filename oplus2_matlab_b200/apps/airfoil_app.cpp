@@ -34,6 +34,10 @@ int op2b_airfoil_app(const op2b_mesh *m, int fp64, int niter, void *q, double *r
 // the same solve at another flow condition (Mach number, alpha in degrees)
 int op2b_airfoil_app_flow(const op2b_mesh *m, int fp64, int niter, double mach, double alpha_deg,
                           void *q, double *rms_hist, int strategy, op2b_app_timing *t);
+// with the sets renumbered (1: Cuthill-McKee, 2: coordinate bisection)
+int op2b_airfoil_app_renumbered(const op2b_mesh *m, int fp64, int niter, void *q,
+                                double *rms_hist, int strategy, int renumber,
+                                op2b_app_timing *t);
 }
 
 static double now() {
@@ -44,7 +48,7 @@ static double now() {
 
 template <class T>
 static int run(const op2b_mesh *m, int niter, double mach_d, double alpha_deg, T *q,
-               double *rms_hist, op2b_app_timing *tm) {
+               double *rms_hist, op2b_app_timing *tm, int renumber = 0) {
   const char *tn = sizeof(T) == 8 ? "double" : "float";
   double t0 = now();
   // airfoil/airfoil.cpp:134-149: the constants and the free stream, with the
@@ -84,6 +88,8 @@ static int run(const op2b_mesh *m, int niter, double mach_d, double alpha_deg, T
   op_decl_const2("mach", 1, tn, &mach);
   op_decl_const2("alpha", 1, tn, &alpha);
   op_decl_const2("qinf", 4, tn, qinf);
+  if (renumber == 1) op2b_set_renumber(1);
+  if (renumber == 2) op2b_set_renumber_coords(p_x);
   op2b_sync();
   double t1 = now();
 
@@ -158,4 +164,16 @@ extern "C" int op2b_airfoil_app_flow(const op2b_mesh *m, int fp64, int niter, do
   op2b_set_strategy(strategy);
   return fp64 ? run<double>(m, niter, mach, alpha_deg, (double *)q, rms_hist, t)
               : run<float>(m, niter, mach, alpha_deg, (float *)q, rms_hist, t);
+}
+
+// the same solve with the sets renumbered for locality at the first loop
+// (renumber 1: Cuthill-McKee, 2: recursive coordinate bisection of the node
+// coordinates); the ordering is timed with the iterations
+extern "C" int op2b_airfoil_app_renumbered(const op2b_mesh *m, int fp64, int niter, void *q,
+                                           double *rms_hist, int strategy, int renumber,
+                                           op2b_app_timing *t) {
+  if (renumber < 0 || renumber > 2) return -1;
+  op2b_set_strategy(strategy);
+  return fp64 ? run<double>(m, niter, 0.4, 0.0, (double *)q, rms_hist, t, renumber)
+              : run<float>(m, niter, 0.4, 0.0, (float *)q, rms_hist, t, renumber);
 }

@@ -4,7 +4,10 @@
 // A mesh whose numbering is scrambled turns each gather into a random
 // access.  When renumbering is on, the first loop call orders every set,
 // all of it computed on the GPU:
-//  - the anchor set is the one most maps point to (ties: the larger);
+//  - with coordinates given (op2b_set_renumber_coords), the anchor set is
+//    the coordinates' set, ordered by recursive coordinate bisection
+//    (rcb_order below);
+//  - otherwise the anchor set is the one most maps point to (ties: the larger);
 //    elements that share a row of a map of dim >= 2 onto it are neighbours
 //    (a CSR graph built by count, scan and fill kernels), and a
 //    level-synchronous breadth-first walk from a least-connected element of
@@ -34,6 +37,7 @@
 // renumbered sets.
 
 #include <limits.h>
+#include <string.h>
 
 #include <algorithm>
 #include <chrono>
@@ -53,6 +57,7 @@ struct SetPerm {
 
 std::vector<SetPerm> g_perm;  // by set index; empty P: not permuted
 bool g_enabled = false, g_applied = false, g_computed = false;
+op_dat g_rcb = nullptr;  // coordinates: order by bisection instead of Cuthill-McKee
 double g_order_seconds = 0.0;  // the last order computation, GPU work included
 
 bool permuted(int set_index) {
@@ -293,6 +298,141 @@ __global__ void k_renumber_map(const int *__restrict__ in, long long rows, int d
   }
 }
 
+// ------------------------------------- recursive coordinate bisection ----
+
+// unsigned key with the order of the float f (-0 before +0)
+__device__ __forceinline__ unsigned float_key(float f) {
+  const unsigned u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// component a of every element's coordinates, rounded to float, into cf,
+// and the sort keys (coordinate key, element) padded with ~0 up to m
+template <class T>
+__global__ void k_rcb_keys(const T *__restrict__ xyz, long long n, int dim, int a, long long m,
+                           float *cf, unsigned long long *key) {
+  GRID_STRIDE(i, m) {
+    if (i < n) {
+      const float f = (float)xyz[i * dim + a];
+      cf[i] = f;
+      key[i] = ((unsigned long long)float_key(f) << 32) | (unsigned)i;
+    } else {
+      key[i] = ~0ull;
+    }
+  }
+}
+
+// Bitonic sort of 64-bit keys in chunks of c (a power of two <= kSortChunk)
+// in shared memory: with k = 0 every chunk is sorted (stages 2..c, each
+// chunk ascending or descending by its place in the whole array); with
+// k > c the steps j = c/2 .. 1 of stage k, after k_bitonic_step has done
+// the steps j >= c that cross chunks.
+constexpr int kSortChunk = 2048;
+__global__ void __launch_bounds__(1024)
+    k_bitonic_chunk(unsigned long long *a, int c, long long k) {
+  __shared__ unsigned long long s[kSortChunk];
+  const long long base = (long long)blockIdx.x * c;
+  for (int i = threadIdx.x; i < c; i += blockDim.x) s[i] = a[base + i];
+  __syncthreads();
+  const long long k0 = k ? k : 2, k1 = k ? k : c;
+  for (long long kk = k0; kk <= k1; kk <<= 1)
+    for (int j = (int)(kk < c ? kk : c) >> 1; j > 0; j >>= 1) {
+      for (int t = threadIdx.x; t < c / 2; t += blockDim.x) {
+        const int i = 2 * j * (t / j) + t % j, l = i + j;
+        const bool up = ((base + i) & kk) == 0;
+        const unsigned long long x = s[i], y = s[l];
+        if ((x > y) == up) {
+          s[i] = y;
+          s[l] = x;
+        }
+      }
+      __syncthreads();
+    }
+  for (int i = threadIdx.x; i < c; i += blockDim.x) a[base + i] = s[i];
+}
+
+// one step (stage k, distance j) of the bitonic sort over the whole array
+__global__ void k_bitonic_step(unsigned long long *a, long long m, long long k, long long j) {
+  GRID_STRIDE(t, m / 2) {
+    const long long i = 2 * j * (t / j) + t % j, l = i + j;
+    const bool up = (i & k) == 0;
+    const unsigned long long x = a[i], y = a[l];
+    if ((x > y) == up) {
+      a[i] = y;
+      a[l] = x;
+    }
+  }
+}
+
+__global__ void k_rcb_list(const unsigned long long *__restrict__ key, int n, int *La) {
+  GRID_STRIDE(p, (long long)n) La[p] = (int)(unsigned)(key[p] & 0xffffffffull);
+}
+
+// The lists L (one per axis, n positions each) hold the same elements in
+// every segment [lo, hi); list a orders a segment by coordinate a.  Each
+// segment of two or more is halved at mid = lo + (hi - lo) / 2 along the
+// axis of its largest extent (last minus first coordinate in that axis'
+// list; ties: the lower axis): the elements at positions >= mid of that
+// axis' list take side 1, the rest side 0.  Every element gets its side
+// from exactly one position.
+__global__ void k_rcb_side(const int *__restrict__ L, const float *__restrict__ cf, int n, int dim,
+                           const int *__restrict__ seg_lo, const int *__restrict__ seg_hi,
+                           int *side) {
+  GRID_STRIDE(p, (long long)n) {
+    const int lo = seg_lo[p], hi = seg_hi[p];
+    if (hi - lo < 2) {
+      side[L[p]] = 0;
+      continue;
+    }
+    int ax = 0;
+    float best = 0.0f;
+    for (int a = 0; a < dim; a++) {
+      const int *La = L + (size_t)a * n;
+      const float *ca = cf + (size_t)a * n;
+      const float e = ca[La[hi - 1]] - ca[La[lo]];
+      if (a == 0 || e > best) {
+        best = e;
+        ax = a;
+      }
+    }
+    side[L[(size_t)ax * n + p]] = (int)p >= lo + (hi - lo) / 2;
+  }
+}
+
+__global__ void k_rcb_flags(const int *__restrict__ La, const int *__restrict__ side, int n,
+                            int *f) {
+  GRID_STRIDE(p, (long long)n) f[p] = side[La[p]];
+}
+
+// stable partition of list a within each halved segment: side 0 to
+// [lo, mid), side 1 to [mid, hi), each in its list order (S: exclusive scan
+// of the flags f)
+__global__ void k_rcb_scatter(const int *__restrict__ La, const int *__restrict__ f,
+                              const int *__restrict__ S, int n, const int *__restrict__ seg_lo,
+                              const int *__restrict__ seg_hi, int *out) {
+  GRID_STRIDE(p, (long long)n) {
+    const int lo = seg_lo[p], hi = seg_hi[p];
+    int q = (int)p;
+    if (hi - lo >= 2) {
+      const int mid = lo + (hi - lo) / 2, ones = S[p] - S[lo];
+      q = f[p] ? mid + ones : (int)p - ones;
+      if (q < lo || q >= hi) continue;  // cannot happen: every list holds the segment's elements
+    }
+    out[q] = La[p];
+  }
+}
+
+__global__ void k_rcb_halve(int n, int *seg_lo, int *seg_hi) {
+  GRID_STRIDE(p, (long long)n) {
+    const int lo = seg_lo[p], hi = seg_hi[p];
+    if (hi - lo >= 2) {
+      const int mid = lo + (hi - lo) / 2;
+      if ((int)p < mid) seg_hi[p] = mid;
+      else seg_lo[p] = mid;
+    }
+  }
+}
+
 #undef GRID_STRIDE
 
 // --------------------------------------------------------- host driver ----
@@ -427,6 +567,80 @@ int *anchor_order(op_set s) {
   return order;
 }
 
+// sorts the m 64-bit keys at a (m a power of two) ascending
+bool bitonic_sort(unsigned long long *a, long long m, cudaStream_t st) {
+  if (m < 2) return true;
+  const int c = (int)std::min<long long>(kSortChunk, m);
+  const int threads = std::min(1024, c / 2);
+  const unsigned chunks = (unsigned)(m / c);
+  k_bitonic_chunk<<<chunks, threads, 0, st>>>(a, c, 0);
+  for (long long k = 2LL * c; k <= m; k <<= 1) {
+    for (long long j = k >> 1; j >= c; j >>= 1)
+      k_bitonic_step<<<grid_for_n(m / 2), 256, 0, st>>>(a, m, k, j);
+    k_bitonic_chunk<<<chunks, threads, 0, st>>>(a, c, k);
+  }
+  return !error_pending();
+}
+
+// Recursive coordinate bisection of the coordinates' set (the reference's
+// developer notes propose it for renumbering, doc/dev.tex:191-210): every
+// segment of the order -- at first the whole set -- is halved at its median
+// along the axis of its largest extent, the lower half first, until every
+// segment holds one element.  Coordinates are compared rounded to float,
+// ties by element number; each axis is sorted once (bitonic), and each
+// level is a stable partition of every axis' list by the halves (one scan
+// per axis), so the order is deterministic.
+int *rcb_order(op_dat xyz) {
+  cudaStream_t st = rt().stream;
+  const int n = xyz->set->size, dim = xyz->dim;
+  const bool dbl = strcmp(xyz->type, "double") == 0;
+  long long m = 1;
+  while (m < n) m <<= 1;
+  DevInts L((long long)dim * n), L2((long long)dim * n), lo(n), hi(n), side(n), f(n), S(n);
+  float *cf = (float *)dev_alloc(sizeof(float) * (size_t)dim * std::max(1, n));
+  unsigned long long *key = (unsigned long long *)dev_alloc(sizeof(unsigned long long) * (size_t)m);
+  int *order = (int *)dev_alloc(sizeof(int) * (size_t)std::max(1, n));
+  bool ok = cf && key && order && L.p && L2.p && lo.p && hi.p && side.p && f.p && S.p;
+  for (int a = 0; ok && a < dim; a++) {
+    if (dbl)
+      k_rcb_keys<double><<<grid_for_n(m), 256, 0, st>>>((const double *)xyz->data_d, n, dim, a,
+                                                          m, cf + (size_t)a * n, key);
+    else
+      k_rcb_keys<float><<<grid_for_n(m), 256, 0, st>>>((const float *)xyz->data_d, n, dim, a, m,
+                                                         cf + (size_t)a * n, key);
+    ok = bitonic_sort(key, m, st);
+    k_rcb_list<<<grid_for_n(n), 256, 0, st>>>(key, n, L.p + (size_t)a * n);
+  }
+  if (ok) {
+    k_fill_int<<<grid_for_n(n), 256, 0, st>>>(lo.p, n, 0);
+    k_fill_int<<<grid_for_n(n), 256, 0, st>>>(hi.p, n, n);
+  }
+  int *cur = L.p, *nxt = L2.p;
+  for (long long longest = n; ok && longest >= 2; longest = (longest + 1) / 2) {
+    k_rcb_side<<<grid_for_n(n), 256, 0, st>>>(cur, cf, n, dim, lo.p, hi.p, side.p);
+    for (int a = 0; a < dim; a++) {
+      const int *La = cur + (size_t)a * n;
+      k_rcb_flags<<<grid_for_n(n), 256, 0, st>>>(La, side.p, n, f.p);
+      exclusive_scan(f.p, S.p, n, st);
+      k_rcb_scatter<<<grid_for_n(n), 256, 0, st>>>(La, f.p, S.p, n, lo.p, hi.p,
+                                                   nxt + (size_t)a * n);
+    }
+    k_rcb_halve<<<grid_for_n(n), 256, 0, st>>>(n, lo.p, hi.p);
+    std::swap(cur, nxt);
+    ok = !error_pending();
+  }
+  if (ok)
+    OP2B_CUDA(cudaMemcpyAsync(order, cur, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+  OP2B_CUDA(cudaStreamSynchronize(st));  // the scratch is freed on return
+  dev_free(cf);
+  dev_free(key);
+  if (!ok || error_pending()) {
+    dev_free(order);
+    return nullptr;
+  }
+  return order;
+}
+
 void compute_orders() {
   for (auto &sp : g_perm) {
     dev_free(sp.d_P);
@@ -438,10 +652,18 @@ void compute_orders() {
   if (OP_set_index == 0) return;
   ensure_cuda();
   cudaStream_t st = rt().stream;
-  // anchor: most maps onto it, then the larger
+  // anchor: the coordinates' set under coordinate bisection; else most
+  // maps onto it, then the larger
   op_set anchor = nullptr;
   int best = -1;
-  for (int k = 0; k < OP_set_index; k++) {
+  if (g_rcb) {
+    if (g_rcb->set->size == 0) return;
+    int *P = rcb_order(g_rcb);
+    if (!P) return;
+    set_perm(g_rcb->set, P);
+    anchor = g_rcb->set;
+  }
+  for (int k = 0; k < OP_set_index && !anchor; k++) {
     op_set s = OP_set_list[k];
     int score = 0;
     for (int j = 0; j < OP_map_index; j++)
@@ -451,10 +673,12 @@ void compute_orders() {
       anchor = s;
     }
   }
-  if (best <= 0 || anchor->size == 0) return;  // no map with shared rows: nothing to gain
-  int *P = anchor_order(anchor);
-  if (!P) return;
-  set_perm(anchor, P);
+  if (!g_rcb) {
+    if (best <= 0 || anchor->size == 0) return;  // no map with shared rows: nothing to gain
+    int *P = anchor_order(anchor);
+    if (!P) return;
+    set_perm(anchor, P);
+  }
   bool progress = true;
   while (progress) {
     progress = false;
@@ -623,6 +847,7 @@ void renumber_reset() {
   g_perm.clear();
   g_applied = g_computed = false;
   g_enabled = false;
+  g_rcb = nullptr;
 }
 
 }  // namespace op2b
@@ -637,6 +862,23 @@ int op2b_set_renumber(int on) {
     return -1;
   }
   g_enabled = on != 0;
+  return 0;
+}
+
+int op2b_set_renumber_coords(op_dat coords) {
+  if (g_applied) {
+    fail(-1, "op2b error -- the renumbering order cannot change after the first loop\n");
+    return -1;
+  }
+  if (coords && (coords->dim < 1 || coords->dim > 3 || !coords->data_d ||
+                 (strcmp(coords->type, "float") != 0 && strcmp(coords->type, "double") != 0))) {
+    fail(-1, "op2b error -- coordinates for bisection must be 1 to 3 float or double "
+             "components\n");
+    return -1;
+  }
+  g_rcb = coords;
+  g_computed = false;
+  if (coords) g_enabled = true;
   return 0;
 }
 
