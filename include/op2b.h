@@ -44,7 +44,17 @@ enum { OP2B_REDUCE_TREE = 0, OP2B_REDUCE_SEQ = 1 };
  *                   (default); 0: one pass, each cell recomputes its fluxes
  *   "gather_batch"  contributions whose loads are issued together per
  *                   thread in the per-element GATHER kernel (1, 2, 4)
- *   "unroll"        elements per thread in the direct loops (1, 2, 4) */
+ *   "unroll"        elements per thread in the direct loops (1, 2, 4)
+ *   "fold_variant", "flux_ctas_per_sm"
+ *                   launch shapes of the two-launch res_calc chain
+ *   "chain_persist" 1: the res_calc chain as one persistent launch over a
+ *                   dependency-ordered queue of flux and cell tiles
+ *                   ("persist_et", "persist_u", "persist_lag" shape it)
+ *   "chain_tiled"   1: the res_calc chain as one launch in which each CTA
+ *                   computes its tile's fluxes into shared memory and
+ *                   updates the tile's cells ("tile_threads" 1024 or 512
+ *                   per CTA, "tile_cells" the tile size, 0 automatic)
+ * Every setting leaves the fields bit-identical. */
 int op2b_set_tuning(const char *key, int value);
 /* The value of a tuning knob, or `def` when it is unset. */
 int op2b_get_tuning(const char *key, int def);
@@ -57,8 +67,9 @@ int op2b_get_tuning(const char *key, int def);
  * `cache_path` (may be NULL) holds an entry for this device, real type and
  * mesh (set sizes), its knobs are applied and 1 is returned.  Otherwise
  * every candidate -- the persistent one-launch chain at several flux tile
- * sizes, cells per thread and queue lags, and the two-launch chain with its
- * per-cell pass variants -- is timed for `iters` launches (each after an L2
+ * sizes, cells per thread and queue lags, the tiled one-launch chain at
+ * 1024 and 512 threads per CTA, and the two-launch chain with its per-cell
+ * pass variants -- is timed for `iters` launches (each after an L2
  * flush) on the app's own data, which is saved first and put back after
  * each candidate; the fastest is applied, appended to the cache file, and 0
  * is returned.  All these candidates leave every field bit-identical; only
@@ -192,13 +203,22 @@ int op2b_layout_ab(int nedge, int ncell, int nnode, const int *pedge, const int 
                    const float *x, const float *q, const float *adt, float gm1, float eps,
                    int iters, double *us_aos, double *us_soa);
 
-/* Bounded waits that ran out in the library's kernels (mbarrier waits of
- * the TMA-staged per-cell pass) since the last reset; reset != 0 clears the
- * count.  Every wait gives up after one second, counts here and lets its
- * kernel return, so a lost completion shows up as a nonzero count (and
- * wrong results) instead of a hung GPU; 0 in every correct run.
- * Synchronises the library stream.  No counterpart in the reference. */
+/* Bounded waits that ran out in the library's kernels (the persistent
+ * chain's waits for the flux tiles a cell tile reads) since the last reset;
+ * reset != 0 clears the count.  Every wait gives up after one second, counts
+ * here and lets its kernel return, so a lost completion shows up as a
+ * nonzero count (and wrong results) instead of a hung GPU; 0 in every
+ * correct run.  Synchronises the library stream.  No counterpart in the
+ * reference. */
 unsigned op2b_wait_timeouts(int reset);
+
+/* Launches of the tiled res_calc chain (tuning knob "chain_tiled": one
+ * launch per res_calc + bres_calc + update [+ adt_calc] [+ save_soln], each
+ * CTA computing its tile's fluxes into shared memory and updating the tile's
+ * cells, q and adt written to second buffers that are swapped in) queued or
+ * captured since the last reset; reset != 0 clears the count.  No
+ * counterpart in the reference. */
+unsigned long long op2b_tiled_launches(int reset);
 
 /* The airfoil update loop (q = qold - res/adt, res = 0, *rms += sum of
  * del^2) for callers that must not allocate device memory: code that cannot

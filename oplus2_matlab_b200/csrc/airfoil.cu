@@ -1980,6 +1980,489 @@ static bool persist_chain(const std::string &name, SlotPlan *sp, const op_arg *r
   return true;
 }
 
+// ------------------------------------------------ tiled res_calc chain ----
+// res_calc + bres_calc + update [+ adt_calc] [+ save_soln] as ONE launch
+// with no wait between CTAs: the cells are cut into tiles of consecutive
+// cells, and a CTA takes a whole tile.  It computes the flux of every edge
+// and boundary edge in its cells' lists into shared memory (an edge whose
+// two cells lie in different tiles is computed by both tiles, with the same
+// arithmetic, so both get the same value), then folds each cell's list from
+// there in list order, applies update and adt_calc to the cell, and stores.
+// The flux reads q and adt of cells of other tiles, which those tiles update
+// in the same launch: update writes the new q, and adt_calc the new adt,
+// into a second buffer of each dataset, which becomes the dataset's when
+// the launch has been queued (the old one becomes the second buffer).
+// Nothing else changes: each cell's fold, update and adt_calc are those of
+// k_fold_update, each flux that of k_res_flux_pair, so q, res, adt and qold
+// are bit-identical; only the order of the TREE rms sum follows the grid.
+//
+// The tile plan (per slot plan, built on the device): every list entry gives
+// the key (tile << 32 | flux index); the sorted, de-duplicated keys are each
+// tile's flux list in ascending flux order (toff: where each tile's run
+// starts), and each cell's list is rewritten as (slot in its tile's run << 1
+// | side).
+struct TilePlan {
+  int want = 0;  // the tile size asked for (ct is smaller when that did not fit)
+  int ct = 0, ntile = 0, maxcnt = 0;
+  int *d_toff = nullptr;   // [ntile + 1]
+  int *d_tflux = nullptr;  // [toff[ntile]]
+  int *d_tell = nullptr;   // [ncell * width]
+};
+
+static void free_tile_plan(TilePlan *tp) {
+  if (!tp) return;
+  dev_free(tp->d_toff);
+  dev_free(tp->d_tflux);
+  dev_free(tp->d_tell);
+  delete tp;
+}
+
+void release_tile_plan(SlotPlan *sp) {
+  free_tile_plan(sp->tile);
+  sp->tile = nullptr;
+}
+
+__global__ void k_tile_keys(const int *__restrict__ ell, int W, int ncell, int ct, long long m,
+                            unsigned long long *key) {
+  const long long n = (long long)ncell * W;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m;
+       i += (long long)gridDim.x * blockDim.x) {
+    unsigned long long k = ~0ull;
+    if (i < n) {
+      const int e = ell[i];
+      if (e >= 0) k = ((unsigned long long)(unsigned)((int)(i / W) / ct) << 32) | (unsigned)(e >> 1);
+    }
+    key[i] = k;
+  }
+}
+
+// 1 at the first of each run of equal (valid) keys
+__global__ void k_tile_first(const unsigned long long *__restrict__ key, int n, int *flag) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    flag[i] = key[i] != ~0ull && (i == 0 || key[i] != key[i - 1]);
+}
+
+// the distinct keys' flux indices in order; toff[t] = position of tile t's
+// first key for every tile after the previous key's tile (toff holds the
+// total beforehand, for tiles past the last key)
+__global__ void k_tile_place(const unsigned long long *__restrict__ key,
+                             const int *__restrict__ flag, const int *__restrict__ pos, int n,
+                             int *tflux, int *toff) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (!flag[i]) continue;
+    const int p = pos[i], t = (int)(key[i] >> 32);
+    tflux[p] = (int)(unsigned)(key[i] & 0xffffffffull);
+    const int prev = i == 0 ? -1 : (int)(key[i - 1] >> 32);
+    for (int u = prev + 1; u <= t; u++) toff[u] = p;
+  }
+}
+
+// each list entry as its slot in the tile's flux run (binary search)
+__global__ void k_tile_lists(const int *__restrict__ ell, int W, int ncell, int ct,
+                             const int *__restrict__ toff, const int *__restrict__ tflux,
+                             int *tell) {
+  const long long n = (long long)ncell * W;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int e = ell[i];
+    if (e < 0) {
+      tell[i] = -1;
+      continue;
+    }
+    const int t = (int)(i / W) / ct, f = e >> 1;
+    int lo = toff[t], hi = toff[t + 1];
+    const int base = lo;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (tflux[mid] < f) lo = mid + 1;
+      else hi = mid;
+    }
+    tell[i] = ((lo - base) << 1) | (e & 1);
+  }
+}
+
+// Tile plan for tiles of ct cells; nullptr when it cannot be built.
+// Synchronises (reads the tile offsets back): a loop's first call, never
+// inside a capture.
+static TilePlan *build_tile_plan(const SlotPlan *sp, int ct) {
+  cudaStream_t s = rt().stream;
+  const int ncell = sp->ntarget, W = sp->width;
+  const long long n = (long long)ncell * W;
+  if (ncell < 1 || ct < 1 || n >= (1LL << 31)) return nullptr;
+  const int ntile = (ncell + ct - 1) / ct;
+  long long m = 1;
+  while (m < n) m <<= 1;
+  unsigned long long *key = (unsigned long long *)dev_alloc(sizeof(unsigned long long) * m);
+  int *flag = (int *)dev_alloc(sizeof(int) * n), *pos = (int *)dev_alloc(sizeof(int) * n);
+  TilePlan *tp = new TilePlan();
+  tp->ct = ct;
+  tp->ntile = ntile;
+  tp->d_toff = (int *)dev_alloc(sizeof(int) * (ntile + 1));
+  tp->d_tell = (int *)dev_alloc(sizeof(int) * n);
+  bool ok = key && flag && pos && tp->d_toff && tp->d_tell;
+  const int g = rt().num_sms * 8;
+  std::vector<int> toff(ntile + 1);
+  if (ok) {
+    k_tile_keys<<<g, 256, 0, s>>>((const int *)sp->d_ell, W, ncell, ct, m, key);
+    ok = sort_keys_u64(key, m, s);
+  }
+  if (ok) {
+    k_tile_first<<<g, 256, 0, s>>>(key, (int)n, flag);
+    const long long total = exclusive_scan(flag, pos, (int)n, s);
+    tp->d_tflux = (int *)dev_alloc(sizeof(int) * std::max(1LL, total));
+    ok = tp->d_tflux != nullptr && total < (1LL << 30);
+    if (ok) {
+      std::fill(toff.begin(), toff.end(), (int)total);
+      OP2B_CUDA(cudaMemcpyAsync(tp->d_toff, toff.data(), sizeof(int) * (ntile + 1),
+                                cudaMemcpyHostToDevice, s));
+      k_tile_place<<<g, 256, 0, s>>>(key, flag, pos, (int)n, tp->d_tflux, tp->d_toff);
+      k_tile_lists<<<g, 256, 0, s>>>((const int *)sp->d_ell, W, ncell, ct, tp->d_toff,
+                                     tp->d_tflux, tp->d_tell);
+      OP2B_CUDA(cudaMemcpyAsync(toff.data(), tp->d_toff, sizeof(int) * (ntile + 1),
+                                cudaMemcpyDeviceToHost, s));
+    }
+  }
+  OP2B_CUDA(cudaStreamSynchronize(s));
+  dev_free(key);
+  dev_free(flag);
+  dev_free(pos);
+  if (ok && !error_pending()) {
+    for (int t = 0; t < ntile; t++) tp->maxcnt = std::max(tp->maxcnt, toff[t + 1] - toff[t]);
+    return tp;
+  }
+  free_tile_plan(tp);
+  return nullptr;
+}
+
+struct TileView {
+  int ct, ntile, W;
+  const int *toff, *tflux, *tell;
+};
+
+template <class T, bool ADT, bool SAVE, int BS>
+__global__ void __launch_bounds__(BS, 1024 / BS)
+    k_chain_tiled(TileView P, int ne, const int2 *__restrict__ pedge,
+                  const int2 *__restrict__ pecell, const T *__restrict__ x,
+                  const T *__restrict__ q, const T *__restrict__ adt, BresEdges<T> B, int ncell,
+                  const T *qold, T *__restrict__ qout, T *__restrict__ res,
+                  const int4 *__restrict__ pcell, const T *__restrict__ xc, AirConsts<T> K,
+                  T *seq, RedSlot<T> slot, unsigned *ticket, T *qsave, T *__restrict__ adt_out) {
+  extern __shared__ __align__(16) unsigned char tile_smem[];
+  T *fv = reinterpret_cast<T *>(tile_smem);  // [maxcnt][4]
+  const unsigned n_e = (unsigned)ne;
+  T rms = T(0);
+  int *fidx = reinterpret_cast<int *>(fv);
+  constexpr int kSlotInts = 4 * (int)sizeof(T) / (int)sizeof(int);
+  for (int t = blockIdx.x; t < P.ntile; t += gridDim.x) {
+    const int beg = __ldg(P.toff + t), cnt = __ldg(P.toff + t + 1) - beg;
+    // the tile's flux indices (plan data, so the first tile's are read
+    // before the previous kernel has finished) into shared memory, each in
+    // the first word of the slot its flux will take; then the fluxes, one
+    // per thread per pass, the next pass's map entries fetched while this
+    // one gathers
+    for (int i = threadIdx.x; i < cnt; i += BS) fidx[kSlotInts * i] = __ldg(P.tflux + beg + i);
+    if (t == (int)blockIdx.x) {
+      pdl_wait();
+      pdl_trigger();
+    }
+    __syncthreads();
+    int i = threadIdx.x;
+    unsigned f = i < cnt ? (unsigned)fidx[kSlotInts * i] : ~0u;
+    int2 nn = make_int2(0, 0), cc = make_int2(0, 0);
+    if (f < n_e) {
+      nn = __ldg(pedge + f);
+      cc = __ldg(pecell + f);
+    }
+    for (; i < cnt; i += BS) {
+      const int in = i + BS;
+      const unsigned fn = in < cnt ? (unsigned)fidx[kSlotInts * in] : ~0u;
+      T r[4];
+      if (f < n_e) {
+        T p[2], sx[2], q1[4], q2[4];
+        ld4(q + 4u * (unsigned)cc.x, q1);
+        ld4(q + 4u * (unsigned)cc.y, q2);
+        ld2(x + 2u * (unsigned)nn.x, p);
+        ld2(x + 2u * (unsigned)nn.y, sx);
+        const T d1 = __ldg(adt + (unsigned)cc.x), d2 = __ldg(adt + (unsigned)cc.y);
+        if (fn < n_e) {
+          nn = __ldg(pedge + fn);
+          cc = __ldg(pecell + fn);
+        }
+        res_flux(p, sx, q1, q2, d1, d2, K.gm1, K.eps, r);
+      } else {
+        if (f - n_e < (unsigned)B.n) {
+          const int b = (int)(f - n_e);
+          int m1, m2;
+          at2(B.x1, B.x2, b, m1, m2);
+          T p[2], sx[2], q1[4];
+          ld2(B.xa + 2 * (size_t)m1, p);
+          ld2(B.xb + 2 * (size_t)m2, sx);
+          ld4(B.q_d + 4 * (size_t)at(B.q, b), q1);
+          bres_contrib(p, sx, q1, __ldg(B.adt + at(B.a, b)),
+                       __ldg(B.bound_d + at(B.bound, b)), K, r);
+        } else {  // the lists' padding value: -0.0, the identity of addition
+          r[0] = r[1] = r[2] = r[3] = -T(0);
+        }
+        if (fn < n_e) {
+          nn = __ldg(pedge + fn);
+          cc = __ldg(pecell + fn);
+        }
+      }
+      st4(fv + 4 * i, r);
+      f = fn;
+    }
+    __syncthreads();
+    // cells: fold from shared memory in list order, update, adt_calc; the
+    // next cell's list, nodes and own streams fetched while this one works
+    const int c1 = min(ncell, (t + 1) * P.ct);
+    auto fetch = [&](int c, int (&k)[4], int (&nd)[4], T (&r)[4], T (&qo)[4], T &ad) {
+      list_head(P.tell, P.W, c, k);
+      if (ADT) {
+        const int4 v = __ldg(pcell + c);
+        nd[0] = v.x; nd[1] = v.y; nd[2] = v.z; nd[3] = v.w;
+      }
+      ldw4(res + 4 * (size_t)c, r);
+      if (SAVE) ldw4(qold + 4 * (size_t)c, qo);
+      else ld4(qold + 4 * (size_t)c, qo);
+      ad = __ldg(adt + c);
+    };
+    int c = t * P.ct + threadIdx.x;
+    int k[4] = {-1, -1, -1, -1}, nd[4] = {0, 0, 0, 0};
+    T r[4], qo[4], ad = T(1);
+    if (c < c1) fetch(c, k, nd, r, qo, ad);
+    for (; c < c1; c += BS) {
+      T xs[4][2];
+      if (ADT)
+#pragma unroll
+        for (int j = 0; j < 4; j++) ld2(xc + 2 * (size_t)nd[j], xs[j]);
+      const int cn = c + BS;
+      int kn[4] = {-1, -1, -1, -1}, ndn[4] = {0, 0, 0, 0};
+      T rn[4], qon[4], adn = T(1);
+      if (cn < c1) fetch(cn, kn, ndn, rn, qon, adn);
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (k[j] >= 0) {
+          T fj[4];
+          ldw4(fv + 4 * (k[j] >> 1), fj);
+          add_listed(r, k[j], fj);
+        }
+      for (int j = 4; j < P.W; j++) {  // lists longer than 4
+        const int kk = __ldg(P.tell + (size_t)c * P.W + j);
+        if (kk < 0) continue;
+        T fj[4];
+        ldw4(fv + 4 * (kk >> 1), fj);
+        add_listed(r, kk, fj);
+      }
+      // airfoil/update.h:1-12
+      const T adti = rcp(ad);
+      T qn[4], sq[4];
+      for (int d = 0; d < 4; d++) {
+        const T del = adti * r[d];
+        qn[d] = qo[d] - del;
+        sq[d] = del * del;
+        rms += sq[d];
+      }
+      st4(qout + 4 * (size_t)c, qn);
+      if (SAVE) st4(qsave + 4 * (size_t)c, qn);  // airfoil/save_soln.h:1-3
+      const T z[4] = {T(0), T(0), T(0), T(0)};
+      st4(res + 4 * (size_t)c, z);
+      if (seq) st4(seq + 4 * (size_t)c, sq);
+      if (ADT) adt_out[c] = adt_calc(xs[0], xs[1], xs[2], xs[3], qn, K);
+      if (cn < c1) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          k[j] = kn[j];
+          nd[j] = ndn[j];
+          r[j] = rn[j];
+          qo[j] = qon[j];
+        }
+        ad = adn;
+      }
+    }
+    __syncthreads();  // the next tile reuses the shared fluxes
+  }
+  if (seq) return;
+  const T v[1] = {rms}, id[1] = {T(0)};
+  RedSlot<T> sl[1] = {slot};
+  grid_finish<T, OpSum, OpSum, 1>(v, id, OpSum(), OpSum(), sl, ticket);
+}
+
+// The second buffers of datasets the tiled chain writes (by dataset index),
+// and the swaps made while a graph is being captured (a graph must leave
+// each dataset in the buffer it found it in: an odd count is undone at the
+// end of the capture by a copy inside the graph).
+static std::vector<void *> g_alt;
+static std::vector<int> g_alt_flips;
+static unsigned long long g_tiled_launches = 0;  // tiled chain launches queued or captured
+
+static void *alt_of(op_dat d) {
+  if (g_alt.size() <= (size_t)d->index) g_alt.resize(d->index + 1, nullptr);
+  if (!g_alt[d->index]) g_alt[d->index] = dev_alloc((size_t)d->size * d->set->size);
+  return g_alt[d->index];
+}
+
+static void flip(op_dat d, bool capturing) {
+  std::swap(d->data_d, reinterpret_cast<char *&>(g_alt[d->index]));
+  if (capturing) {
+    if (g_alt_flips.size() <= (size_t)d->index) g_alt_flips.resize(d->index + 1, 0);
+    g_alt_flips[d->index]++;
+  }
+}
+
+void tile_capture_begin() { g_alt_flips.clear(); }
+
+void tile_capture_end() {  // still capturing: the copies become graph nodes
+  for (size_t i = 0; i < g_alt_flips.size(); i++) {
+    if (!(g_alt_flips[i] & 1)) continue;
+    op_dat d = OP_dat_list[i];
+    OP2B_CUDA(cudaMemcpyAsync(g_alt[i], d->data_d, (size_t)d->size * d->set->size,
+                              cudaMemcpyDeviceToDevice, rt().stream));
+    std::swap(d->data_d, reinterpret_cast<char *&>(g_alt[i]));
+  }
+  g_alt_flips.clear();
+}
+
+void release_tile_alts() {
+  for (void *p : g_alt) dev_free(p);
+  g_alt.clear();
+  g_alt_flips.clear();
+}
+
+// res_calc + bres_calc + update [+ adt_calc] [+ save_soln] as one tiled
+// launch; false when it does not apply (the caller runs the two passes)
+template <class T>
+static bool tiled_chain(const std::string &name, SlotPlan *sp, const op_arg *ra,
+                        const op_arg *ba, const ResEdges<T> &E, const BresEdges<T> &B,
+                        const op_arg *ua, const op_arg *aa, const op_arg *sa, void *adt_out,
+                        void *save_out, const AirConsts<T> &K, bool seq, int rslot_id,
+                        cudaStream_t s) {
+  const size_t nval = (size_t)sp->na + sp->nb + 1;
+  if (!tuning("chain_tiled", 0) || !flux_pair_shape(ra, nval) || sp->tile_unsuited) return false;
+  // CTAs of 1024 threads (one per SM) or 512 (two per SM, each on its own tile)
+  const int threads = tuning("tile_threads", 1024) == 512 ? 512 : 1024;
+  const int per_sm = 1024 / threads;
+  op_dat q = ua[1].dat, adt = ua[3].dat;
+  // the flux reads q and adt -- the datasets update and adt_calc write, into
+  // second buffers -- and must read nothing else the cell phase writes
+  // (res in place, save_soln's output)
+  if (ra[2].dat != q || ra[4].dat != adt || ra[0].dat == q || ra[0].dat == adt) return false;
+  if (aa && !(aa[0].map && aa[0].map == aa[1].map && aa[0].map == aa[2].map &&
+              aa[0].map == aa[3].map && aa[0].map->dim == 4 && aa[0].idx == 0 &&
+              aa[1].idx == 1 && aa[2].idx == 2 && aa[3].idx == 3 && aa[0].dat == aa[1].dat &&
+              aa[0].dat == aa[2].dat && aa[0].dat == aa[3].dat && aa[5].dat == adt &&
+              aa[4].dat == q))
+    return false;
+  {
+    const op_dat written[2] = {ua[2].dat, sa && !save_out ? sa[1].dat : nullptr};
+    std::vector<op_dat> read = {ra[0].dat, q, adt};
+    if (aa) read.push_back(aa[0].dat);
+    if (ba)
+      for (int i : {0, 1, 2, 3, 5}) read.push_back(ba[i].dat);
+    for (op_dat r : read)
+      if (r == written[0] || (written[1] && r == written[1])) return false;
+    if (written[1] && (written[1] == q || written[1] == adt)) return false;
+  }
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  OP2B_CUDA(cudaStreamIsCapturing(s, &cap));
+  const bool capturing = cap != cudaStreamCaptureStatusNone;
+  // a graph holds the buffers it was captured with: no swaps between launches
+  if (!capturing && live_graphs() > 0) return false;
+  const int ncell = sp->ntarget;
+  const size_t static_smem = 1024,
+               budget = (size_t)rt().smem_optin / per_sm - static_smem;
+  // tile size: the knob, else one tile per resident CTA; shrunk until a
+  // tile's fluxes fit the CTA's shared memory
+  const long long ctas = (long long)rt().num_sms * per_sm;
+  const int want = tuning("tile_cells", 0) > 0
+                       ? tuning("tile_cells", 0)
+                       : (int)std::max(64LL, (ncell + ctas - 1) / ctas);
+  if (!sp->tile || sp->tile->want != want ||
+      (size_t)sp->tile->maxcnt * 4 * sizeof(T) > budget) {
+    if (capturing) return false;  // plans are built before a capture
+    release_tile_plan(sp);
+    for (int ct = want;; ct = ct * 3 / 4) {
+      if (ct < 16) {
+        sp->tile_unsuited = true;
+        return false;
+      }
+      TilePlan *tp = build_tile_plan(sp, ct);
+      if (!tp) {
+        sp->tile_unsuited = true;
+        return false;
+      }
+      if ((size_t)tp->maxcnt * 4 * sizeof(T) <= budget) {
+        tp->want = want;
+        sp->tile = tp;
+        break;
+      }
+      free_tile_plan(tp);
+    }
+  }
+  TilePlan *tp = sp->tile;
+  const size_t smem = (size_t)tp->maxcnt * 4 * sizeof(T);
+  void *qout = alt_of(q);
+  void *adt_to = nullptr;
+  bool flip_adt = false;
+  if (aa) {
+    adt_to = adt_out;
+    if (!adt_to) {
+      adt_to = alt_of(adt);
+      flip_adt = true;
+    }
+  }
+  if (!qout || (aa && !adt_to) || error_pending()) return false;
+  const void *kp =
+      threads == 512
+          ? (sa ? (const void *)k_chain_tiled<T, true, true, 512>
+                : aa ? (const void *)k_chain_tiled<T, true, false, 512>
+                     : (const void *)k_chain_tiled<T, false, false, 512>)
+          : (sa ? (const void *)k_chain_tiled<T, true, true, 1024>
+                : aa ? (const void *)k_chain_tiled<T, true, false, 1024>
+                     : (const void *)k_chain_tiled<T, false, false, 1024>);
+  static size_t sized[2][2][3] = {};
+  size_t &have = sized[sizeof(T) == 8][threads == 512][sa ? 2 : aa ? 1 : 0];
+  if (smem > have) {
+    OP2B_CUDA(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    have = smem;
+  }
+  T *seqbuf = seq ? (T *)red_seq_buffer(sizeof(T) * 4 * (size_t)ncell) : nullptr;
+  T *result = (T *)red_slot_ptr(rslot_id);
+  RedSlot<T> rslot{(T *)red_partials(0), result};
+  const int grid = std::min(tp->ntile, std::min(kMaxRedBlocks, rt().num_sms * per_sm));
+  TileView P{tp->ct, tp->ntile, sp->width, tp->d_toff, tp->d_tflux, tp->d_tell};
+  const T *xc = aa ? (const T *)aa[0].dat->data_d : nullptr;
+  const int4 *pcell = aa ? reinterpret_cast<const int4 *>(map_dev(aa[0].map)) : nullptr;
+  T *qsave = sa ? (T *)(save_out ? save_out : sa[1].dat->data_d) : nullptr;
+  {
+    PhaseScope ph(name + ":tiled");
+    auto go = [&](auto kernel) {
+      launch_pdl(kernel, grid, threads, smem, s, P, E.n,
+                 reinterpret_cast<const int2 *>(map_dev(ra[0].map)),
+                 reinterpret_cast<const int2 *>(map_dev(ra[2].map)), E.xa, E.qa, E.adta, B,
+                 ncell, (const T *)ua[0].dat->data_d, (T *)qout, (T *)ua[2].dat->data_d, pcell,
+                 xc, K, seqbuf, rslot, red_ticket(), qsave, (T *)adt_to);
+    };
+    if (threads == 512) {
+      if (sa) go(k_chain_tiled<T, true, true, 512>);
+      else if (aa) go(k_chain_tiled<T, true, false, 512>);
+      else go(k_chain_tiled<T, false, false, 512>);
+    } else {
+      if (sa) go(k_chain_tiled<T, true, true, 1024>);
+      else if (aa) go(k_chain_tiled<T, true, false, 1024>);
+      else go(k_chain_tiled<T, false, false, 1024>);
+    }
+  }
+  if (error_pending()) return true;
+  g_tiled_launches++;
+  flip(q, capturing);
+  if (flip_adt) flip(adt, capturing);
+  if (seq) {
+    T init = *(const T *)ua[4].data;
+    k_seq_sum<T><<<1, 32, 0, s>>>(seqbuf, 4LL * ncell, init, result);
+  }
+  return true;
+}
+
 template <class T>
 static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op_set bset,
                         const op_arg *ba, const op_arg *ua, const op_arg *aa, const op_arg *sa,
@@ -2011,6 +2494,10 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
     LoopScope ls(name.c_str(), bytes, 0);
     ResEdges<T> E = res_edges<T>(rset, ra);
     BresEdges<T> B = bres_edges<T>(bset, ba);
+    if (ua && !flux_done && ua[2].dat == ra[6].dat &&
+        tiled_chain<T>(name, sp, ra, ba, E, B, ua, aa, sa, adt_out, save_out, K, seq, rslot_id,
+                       s))
+      goto chained;
     if (ua && !flux_done && ua[2].dat == ra[6].dat &&
         persist_chain<T>(name, sp, ra, E, B, ua, aa, sa, adt_out, save_out, K, seq, rslot_id, s))
       goto chained;
@@ -2126,3 +2613,9 @@ bool run_res_chain(char const *name, op_set rset, const op_arg *ra, op_set bset,
 }  // namespace op2b
 
 extern "C" unsigned op2b_wait_timeouts(int reset) { return op2b::wait_timeouts(reset != 0); }
+
+extern "C" unsigned long long op2b_tiled_launches(int reset) {
+  const unsigned long long n = op2b::g_tiled_launches;
+  if (reset) op2b::g_tiled_launches = 0;
+  return n;
+}

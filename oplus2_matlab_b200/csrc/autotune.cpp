@@ -54,7 +54,8 @@ struct Candidate {
 
 // every knob any candidate sets, with the library's defaults
 const Knobs kDefaults = {{"chain_persist", 0}, {"persist_et", 1024}, {"persist_u", 1},
-                         {"persist_lag", -1},  {"fold_variant", 0},  {"flux_ctas_per_sm", 16}};
+                         {"persist_lag", -1},  {"fold_variant", 0},  {"flux_ctas_per_sm", 16},
+                         {"chain_tiled", 0},   {"tile_threads", 1024}};
 
 std::vector<Candidate> candidates(bool allow_reorder) {
   std::vector<Candidate> out;
@@ -72,6 +73,11 @@ std::vector<Candidate> candidates(bool allow_reorder) {
                    {"persist_lag", lag}};
         out.push_back(c);
       }
+  for (int th : {1024, 512}) {  // the tiled one-launch chain
+    Candidate c;
+    c.knobs = {{"chain_tiled", 1}, {"tile_threads", th}};
+    out.push_back(c);
+  }
   if (allow_reorder)
     for (int ps : {64, 128, 256, 512}) {
       Candidate c;

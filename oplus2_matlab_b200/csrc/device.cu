@@ -413,6 +413,7 @@ void op_exit(void) {
   checkpoint_reset();
   ahead_reset();
   noalloc_reset();
+  release_tile_alts();
   for (auto &m : R.maps) dev_free(m.d);
   R.maps.clear();
   for (int i = 0; i < OP_dat_index; i++) dev_free(OP_dat_list[i]->data_d);

@@ -41,6 +41,7 @@ int op2b_capture_begin(int profile) {
   Runtime &R = rt();
   flush_pending();  // loops held back before the capture run outside the graph
   ahead_drop();     // a graph bakes dataset pointers: nothing may be swapped in later
+  tile_capture_begin();
   deliver_deferred();
   g_pending_mark = red_pending_count();
   R.capture_events.clear();
@@ -59,6 +60,7 @@ int op2b_capture_begin(int profile) {
 
 void *op2b_capture_end(void) {
   flush_pending();
+  tile_capture_end();  // the graph leaves every dataset in the buffer it found
   Runtime &R = rt();
   Graph *g = new Graph();
   cudaError_t e = cudaStreamEndCapture(R.stream, &g->graph);

@@ -170,6 +170,11 @@ void ahead_drop();   // discard what was run ahead (constants, capture, restore)
 void ahead_reset();  // op_exit: also free the spare buffers
 void noalloc_reset();  // op_exit: forget op2b_update_noalloc's cached scratch addresses
 int live_graphs();   // captured graphs not yet destroyed (graph.cu)
+void tile_capture_begin();  // graph capture: count the tiled chain's buffer swaps
+void tile_capture_end();    // ... and undo an odd count inside the graph
+void release_tile_alts();   // op_exit: free the tiled chain's second buffers
+// sorts the m 64-bit keys at a (m a power of two) ascending on stream s
+bool sort_keys_u64(unsigned long long *a, long long m, cudaStream_t s);
 
 // renumbering of the sets for locality (renumber.cu)
 bool renumber_enabled();

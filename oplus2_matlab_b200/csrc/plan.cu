@@ -1265,6 +1265,7 @@ using namespace op2b;
 void op2b_release_plans() {
   for (auto &up : g_slot_plans) {
     release_chain_sched(up.get());
+    release_tile_plan(up.get());
     dev_free(up->d_ell);
     dev_free(up->d_buf);
   }

@@ -80,6 +80,7 @@ constexpr int kTile = 256;
 // list order is the order of the sequential back-end running a then b;
 // -0.0 is the exact identity of IEEE addition and r + (-v) equals r - v.
 struct ChainSched;  // airfoil.cu: the persistent chain's work queue over these lists
+struct TilePlan;    // airfoil.cu: the tiled chain's per-tile flux lists
 struct SlotPlan {
   const GatherPlan *a = nullptr, *b = nullptr;
   int ntarget = 0;
@@ -90,9 +91,12 @@ struct SlotPlan {
   size_t buf_bytes = 0;
   ChainSched *chain = nullptr;  // built by the first persistent chain launch
   bool chain_unsuited = false;  // a cell tile reads too many flux tiles for it
+  TilePlan *tile = nullptr;     // built by the first tiled chain launch
+  bool tile_unsuited = false;   // no tile size fits shared memory
 };
-// free a slot plan's persistent-chain queue (airfoil.cu)
+// free a slot plan's persistent-chain queue and tile plan (airfoil.cu)
 void release_chain_sched(SlotPlan *sp);
+void release_tile_plan(SlotPlan *sp);
 
 // widest list the fold kernels accept
 constexpr int kMaxSlotWidth = 8;

@@ -771,6 +771,10 @@ void permute_launch(const void *in, void *out, const int *dP, long long n, int s
 
 bool renumber_enabled() { return g_enabled; }
 
+bool sort_keys_u64(unsigned long long *a, long long m, cudaStream_t s) {
+  return bitonic_sort(a, m, s);
+}
+
 // the set's device permutation (new -> old / old -> new), or nullptr
 const int *perm_new2old_dev(op_set s) {
   return s && permuted(s->index) && g_applied ? g_perm[s->index].d_P : nullptr;
