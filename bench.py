@@ -86,6 +86,10 @@ def parse():
     ap.add_argument("--forms-requests", type=int, default=400,
                     help="plain mode: requests of the served stream at the batched/served "
                          "workload's 200/s rate (the full workload has 10,000)")
+    ap.add_argument("--op-arg", action="append", default=[],
+                    help="plain mode: an op_init argument, e.g. OP_BLOCK_SIZE=256 or "
+                         "OP_PART_SIZE=256 (the reference's run-time launch-shape options; "
+                         "COLOURED reads them)")
     ap.add_argument("--tune", action="append", default=[],
                     help="kernel-variant knob key=value (op2b_set_tuning)")
     ap.add_argument("--mesh", default="400x600",
@@ -389,7 +393,7 @@ def impl_ours(args, dist):
 
     mesh = plain_mesh(args)
     api.set_error_mode(api.ERRORS_RETURN)
-    api.op_init([], 0)
+    api.op_init(args.op_arg, 0)
     api.set_strategy(api.STRATEGY_GATHER if args.strategy == "gather" else api.STRATEGY_COLOURED)
     api.set_reduction(api.REDUCE_TREE)
     if args.renumber:
@@ -581,7 +585,8 @@ def impl_ours(args, dist):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.fp64 else "f32",
         "data": "synthetic: NACA0012 C-mesh from the reference's generator, free-stream start",
         "config": dict(plain_config(mesh.I, mesh.J, mesh_sizes(mesh), args.mesh.endswith("s")),
-                       strategy=args.strategy, renumbered=args.renumber or False,
+                       strategy=args.strategy, op_init_args=args.op_arg,
+                       renumbered=args.renumber or False,
                        renumber_seconds=renumber_s, reduction="tree",
                        l2="flushed before every step (untimed read-only sweep of 3x the 126 MB L2)",
                        timing="CUDA events around each graph launch on the library stream",

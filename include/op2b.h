@@ -75,7 +75,9 @@ int op2b_get_tuning(const char *key, int def);
  * is returned.  All these candidates leave every field bit-identical; only
  * the order of the TREE rms sum follows the launch shape.  allow_reorder
  * != 0 also times COLOURED (the reference's colouring scheme) at part sizes
- * 64..512, whose fields differ from op_seq.h's in the last bits.  -1 on
+ * 64..512 with 64..512 threads per block (the run-time OP_PART_SIZE and
+ * OP_BLOCK_SIZE of op_init), whose fields differ from op_seq.h's in the
+ * last bits.  -1 on
  * error (no chain has run, captured graphs exist).  Synchronises. */
 int op2b_autotune(const char *cache_path, int iters, int allow_reorder);
 

@@ -49,7 +49,7 @@ typedef std::vector<std::pair<std::string, int>> Knobs;
 struct Candidate {
   Knobs knobs;
   int strategy = OP2B_STRATEGY_GATHER;
-  int part_size = 0;
+  int part_size = 0, block_size = 0;  // COLOURED: the plan's part size, threads per block
 };
 
 // every knob any candidate sets, with the library's defaults
@@ -78,11 +78,13 @@ std::vector<Candidate> candidates(bool allow_reorder) {
     c.knobs = {{"chain_tiled", 1}, {"tile_threads", th}};
     out.push_back(c);
   }
-  if (allow_reorder)
-    for (int ps : {64, 128, 256, 512}) {
+  if (allow_reorder)  // part size and threads per block of the colouring scheme
+    for (auto pb : {std::make_pair(512, 512), std::make_pair(512, 256), std::make_pair(256, 256),
+                    std::make_pair(256, 128), std::make_pair(128, 128), std::make_pair(64, 64)}) {
       Candidate c;
       c.strategy = OP2B_STRATEGY_COLOURED;
-      c.part_size = ps;
+      c.part_size = pb.first;
+      c.block_size = pb.second;
       out.push_back(c);
     }
   return out;
@@ -91,7 +93,8 @@ std::vector<Candidate> candidates(bool allow_reorder) {
 std::string describe(const Candidate &c) {
   std::string s;
   if (c.strategy == OP2B_STRATEGY_COLOURED)
-    return "strategy=coloured,part_size=" + std::to_string(c.part_size);
+    return "strategy=coloured,part_size=" + std::to_string(c.part_size) +
+           ",block_size=" + std::to_string(c.block_size);
   for (auto &kv : c.knobs) {
     if (!s.empty()) s += ",";
     s += kv.first + "=" + std::to_string(kv.second);
@@ -103,7 +106,7 @@ std::string describe(const Candidate &c) {
 bool parse(const std::string &text, Candidate *c) {
   c->knobs.clear();
   c->strategy = OP2B_STRATEGY_GATHER;
-  c->part_size = 0;
+  c->part_size = c->block_size = 0;
   size_t pos = 0;
   while (pos < text.size()) {
     size_t end = text.find(',', pos);
@@ -120,6 +123,7 @@ bool parse(const std::string &text, Candidate *c) {
       const long x = strtol(v.c_str(), &e, 10);
       if (!e || *e) return false;
       if (k == "part_size") c->part_size = (int)x;
+      else if (k == "block_size") c->block_size = (int)x;
       else c->knobs.emplace_back(k, (int)x);
     }
     pos = end + 1;
@@ -143,7 +147,10 @@ void apply(const Candidate &c) {
   for (auto &kv : kDefaults) rt().tuning[kv.first] = kv.second;
   for (auto &kv : c.knobs) rt().tuning[kv.first] = kv.second;
   rt().strategy = c.strategy;
-  if (c.strategy == OP2B_STRATEGY_COLOURED) OP_part_size = c.part_size;
+  if (c.strategy == OP2B_STRATEGY_COLOURED) {
+    OP_part_size = c.part_size;
+    if (c.block_size > 0) OP_block_size = c.block_size;
+  }
 }
 
 }  // namespace
@@ -272,7 +279,8 @@ extern "C" int op2b_autotune(const char *cache_path, int iters, int allow_reorde
   }
   // 2. time every candidate on the app's data, putting the data back after each
   if (iters < 1) iters = 3;
-  const int old_strategy = rt().strategy, old_part = OP_part_size, old_mode = rt().error_mode;
+  const int old_strategy = rt().strategy, old_part = OP_part_size, old_block = OP_block_size,
+            old_mode = rt().error_mode;
   std::vector<std::pair<std::string, int>> old_knobs;
   for (auto &kv : kDefaults) old_knobs.emplace_back(kv.first, tuning(kv.first.c_str(), kv.second));
   Snapshot snap;
@@ -296,9 +304,12 @@ extern "C" int op2b_autotune(const char *cache_path, int iters, int allow_reorde
     for (auto &kv : old_knobs) rt().tuning[kv.first] = kv.second;
     rt().strategy = old_strategy;
     OP_part_size = old_part;
+    OP_block_size = old_block;
     fail(-1, "op2b_autotune error: no candidate launch shape ran\n");
     return -1;
   }
+  OP_part_size = old_part;  // a COLOURED winner sets its own
+  OP_block_size = old_block;
   apply(cands[best]);
   if (cache_path) {
     if (FILE *f = fopen(cache_path, "a")) {
