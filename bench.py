@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-iters", type=int, default=1000)
+    ap.add_argument("--group-tiled", action="store_true",
+                    help="batched and served forms: the tiled chain (op2b_group_set_tiled)")
     ap.add_argument("--no-forms", action="store_true",
                     help="plain mode: skip the batched and served measurements that the "
                          "default line carries")
@@ -768,7 +770,7 @@ def gen_meshes(dims):
         return dict(zip(want, ex.map(lambda d: M.naca0012(d[0], d[1]), want)))
 
 
-def warm_paths(dt):
+def warm_paths(dt, tiled=False):
     """Untimed: create the CUDA context and load the kernels of both paths
     (lazy module loading) on a tiny mesh, so neither timed region pays the
     process's one-time start-up."""
@@ -776,6 +778,8 @@ def warm_paths(dt):
     from oplus2_matlab_b200 import mesh as M
     tiny = M.naca0012(10, 15)
     g = G.Group(dt)
+    if tiled:
+        g.set_tiled(True)
     g.add(tiny, 0.5, 1.0, 3)
     g.autotune(1)
     g.run(3)
@@ -816,12 +820,14 @@ def measure_batched(args, dist, instances, n):
     for kv in args.tune:
         k, v = kv.split("=")
         api.lib().op2b_set_tuning(k.encode(), int(v))
-    warm_paths(dt)
+    warm_paths(dt, args.group_tiled)
 
     clocks = Clocks(dist.local)
     dist.barrier()
     t0 = time.perf_counter()
     g = G.Group(dt)
+    if args.group_tiled:
+        g.set_tiled(True)
     ids = [g.add(meshes[inst[i][:2]], inst[i][2], inst[i][3], n) for i in mine]
     g.sync()
     t_add = time.perf_counter() - t0
@@ -869,7 +875,7 @@ def measure_batched(args, dist, instances, n):
         "group": {"seconds": t_group, "iterate_seconds_rank0": t_iter,
                   "phases_s_rank0": {"admit": t_add, "autotune": t_tune,
                                      "iterate": t_iter, "fetch": t_fetch},
-                  "edge_tile_autotuned": tile, "device_bytes_rank0": gbytes,
+                  "edge_tile_autotuned": tile, "tiled_chain": bool(args.group_tiled), "device_bytes_rank0": gbytes,
                   "autotuned": "edge tile and L2 block size",
                   "iteration_gbs_rank0": my_bytes / t_iter / 1e9},
         "plain_back_to_back": {"seconds": t_plain, "solves_per_s": total / t_plain,
@@ -913,9 +919,12 @@ def measure_served(args, dist, requests, rate, max_iter, rel_tol):
     mine = list(range(dist.rank, requests, dist.world))
     meshes = gen_meshes([inst[i][:2] for i in mine])
     api.set_error_mode(api.ERRORS_RETURN)
-    warm_paths(dt)
+    warm_paths(dt, args.group_tiled)
+    grp = G.Group(dt)
+    if args.group_tiled:
+        grp.set_tiled(True)
     srv = S.Server(dt, budget_bytes=args.budget_gb * 1e9, iters_per_step=args.iters_per_step,
-                   max_active=args.max_active, policy=args.policy)
+                   max_active=args.max_active, policy=args.policy, group=grp)
     reqs = [S.Request(i, meshes[inst[i][:2]], inst[i][2], inst[i][3], max_iter,
                       rel_tol, float(arrivals[i])) for i in mine]
     clocks = Clocks(dist.local)

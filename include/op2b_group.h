@@ -91,6 +91,18 @@ int op2b_group_set_block_bytes(op2b_group g, long long bytes);
  * iteration, so independent blocks' launches overlap (one block's per-cell
  * pass beside another's flux pass).  Results do not depend on it. */
 int op2b_group_set_streams(op2b_group g, int n);
+/* The tiled chain: each update and the loops fused with it as ONE launch
+ * over all solves, a CTA per tile of consecutive cells of one solve, the
+ * flux values in shared memory (edges between tiles computed by both)
+ * instead of written to and read back from device memory; update and
+ * adt_calc write to second buffers of q and adt (20 bytes per cell in FP32,
+ * plus the tile lists, counted by op2b_group_solve_bytes while it is on).
+ * Fields are bit-identical to the two-launch form; each solve's rms is
+ * folded over its own tiles, so the rms history differs from the two-launch
+ * form's in the last bits and is the same alone or in any mix.  on = 0
+ * (the default) or 1; returns 0.  op2b_group_tiled returns the mode. */
+int op2b_group_set_tiled(op2b_group g, int on);
+int op2b_group_tiled(op2b_group g);
 
 /* Launch shape of the flux pass: edges per tile (multiple of 256, 256..8192).
  * Results do not depend on it; op2b_group_autotune picks it by timing. */

@@ -225,6 +225,8 @@ PROTOTYPES = [
     ("op2b_group_set_edge_tile", C.c_int, [_P, C.c_int]),
     ("op2b_group_set_block_bytes", C.c_int, [_P, C.c_longlong]),
     ("op2b_group_set_streams", C.c_int, [_P, C.c_int]),
+    ("op2b_group_set_tiled", C.c_int, [_P, C.c_int]),
+    ("op2b_group_tiled", C.c_int, [_P]),
     ("op2b_group_edge_tile", C.c_int, [_P]),
     ("op2b_group_autotune", C.c_int, [_P, C.c_int]),
 ]

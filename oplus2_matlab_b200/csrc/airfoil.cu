@@ -22,6 +22,7 @@
 #include <algorithm>
 
 #include "airfoil_math.cuh"
+#include "tile_chain.cuh"
 #include "launch.cuh"
 #include "loops.h"
 #include "reduce.cuh"
@@ -2002,18 +2003,13 @@ static bool persist_chain(const std::string &name, SlotPlan *sp, const op_arg *r
 // starts), and each cell's list is rewritten as (slot in its tile's run << 1
 // | side).
 struct TilePlan {
-  int want = 0;  // the tile size asked for (ct is smaller when that did not fit)
-  int ct = 0, ntile = 0, maxcnt = 0;
-  int *d_toff = nullptr;   // [ntile + 1]
-  int *d_tflux = nullptr;  // [toff[ntile]]
-  int *d_tell = nullptr;   // [ncell * width]
+  int want = 0;  // the tile size asked for (tl.ct is smaller when that did not fit)
+  TileLists tl;
 };
 
 static void free_tile_plan(TilePlan *tp) {
   if (!tp) return;
-  dev_free(tp->d_toff);
-  dev_free(tp->d_tflux);
-  dev_free(tp->d_tell);
+  free_tile_lists(&tp->tl, rt().stream);
   delete tp;
 }
 
@@ -2081,56 +2077,77 @@ __global__ void k_tile_lists(const int *__restrict__ ell, int W, int ncell, int 
   }
 }
 
-// Tile plan for tiles of ct cells; nullptr when it cannot be built.
-// Synchronises (reads the tile offsets back): a loop's first call, never
-// inside a capture.
-static TilePlan *build_tile_plan(const SlotPlan *sp, int ct) {
-  cudaStream_t s = rt().stream;
-  const int ncell = sp->ntarget, W = sp->width;
+// Tile lists for tiles of ct consecutive cells over the contribution lists
+// ell (ncell x W entries, (index << 1 | side)): device arrays from the pool,
+// allocated and built on stream s, which this synchronises (it reads the
+// tile offsets back for the largest tile).  False when they cannot be built.
+bool build_tile_lists(const int *ell, int ncell, int W, int ct, cudaStream_t s, TileLists *out) {
+  *out = TileLists();
   const long long n = (long long)ncell * W;
-  if (ncell < 1 || ct < 1 || n >= (1LL << 31)) return nullptr;
+  if (ncell < 1 || W < 1 || ct < 1 || n >= (1LL << 31)) return false;
   const int ntile = (ncell + ct - 1) / ct;
   long long m = 1;
   while (m < n) m <<= 1;
-  unsigned long long *key = (unsigned long long *)dev_alloc(sizeof(unsigned long long) * m);
-  int *flag = (int *)dev_alloc(sizeof(int) * n), *pos = (int *)dev_alloc(sizeof(int) * n);
-  TilePlan *tp = new TilePlan();
-  tp->ct = ct;
-  tp->ntile = ntile;
-  tp->d_toff = (int *)dev_alloc(sizeof(int) * (ntile + 1));
-  tp->d_tell = (int *)dev_alloc(sizeof(int) * n);
-  bool ok = key && flag && pos && tp->d_toff && tp->d_tell;
+  unsigned long long *key = nullptr;
+  int *flag = nullptr, *pos = nullptr;
+  TileLists tl;
+  tl.ct = ct;
+  tl.ntile = ntile;
+  bool ok = pool_malloc_async((void **)&key, sizeof(unsigned long long) * m, s) == cudaSuccess &&
+            pool_malloc_async((void **)&flag, sizeof(int) * n, s) == cudaSuccess &&
+            pool_malloc_async((void **)&pos, sizeof(int) * n, s) == cudaSuccess &&
+            pool_malloc_async((void **)&tl.toff, sizeof(int) * (ntile + 1), s) == cudaSuccess &&
+            pool_malloc_async((void **)&tl.tell, sizeof(int) * n, s) == cudaSuccess;
+  if (!ok) cudaGetLastError();
   const int g = rt().num_sms * 8;
   std::vector<int> toff(ntile + 1);
   if (ok) {
-    k_tile_keys<<<g, 256, 0, s>>>((const int *)sp->d_ell, W, ncell, ct, m, key);
+    k_tile_keys<<<g, 256, 0, s>>>(ell, W, ncell, ct, m, key);
     ok = sort_keys_u64(key, m, s);
   }
   if (ok) {
     k_tile_first<<<g, 256, 0, s>>>(key, (int)n, flag);
     const long long total = exclusive_scan(flag, pos, (int)n, s);
-    tp->d_tflux = (int *)dev_alloc(sizeof(int) * std::max(1LL, total));
-    ok = tp->d_tflux != nullptr && total < (1LL << 30);
+    ok = total < (1LL << 30) &&
+         pool_malloc_async((void **)&tl.tflux, sizeof(int) * std::max(1LL, total), s) ==
+             cudaSuccess;
     if (ok) {
       std::fill(toff.begin(), toff.end(), (int)total);
-      OP2B_CUDA(cudaMemcpyAsync(tp->d_toff, toff.data(), sizeof(int) * (ntile + 1),
+      OP2B_CUDA(cudaMemcpyAsync(tl.toff, toff.data(), sizeof(int) * (ntile + 1),
                                 cudaMemcpyHostToDevice, s));
-      k_tile_place<<<g, 256, 0, s>>>(key, flag, pos, (int)n, tp->d_tflux, tp->d_toff);
-      k_tile_lists<<<g, 256, 0, s>>>((const int *)sp->d_ell, W, ncell, ct, tp->d_toff,
-                                     tp->d_tflux, tp->d_tell);
-      OP2B_CUDA(cudaMemcpyAsync(toff.data(), tp->d_toff, sizeof(int) * (ntile + 1),
+      k_tile_place<<<g, 256, 0, s>>>(key, flag, pos, (int)n, tl.tflux, tl.toff);
+      k_tile_lists<<<g, 256, 0, s>>>(ell, W, ncell, ct, tl.toff, tl.tflux, tl.tell);
+      OP2B_CUDA(cudaMemcpyAsync(toff.data(), tl.toff, sizeof(int) * (ntile + 1),
                                 cudaMemcpyDeviceToHost, s));
+    } else {
+      cudaGetLastError();
     }
   }
+  for (void *p : {(void *)key, (void *)flag, (void *)pos})
+    if (p) cudaFreeAsync(p, s);
   OP2B_CUDA(cudaStreamSynchronize(s));
-  dev_free(key);
-  dev_free(flag);
-  dev_free(pos);
   if (ok && !error_pending()) {
-    for (int t = 0; t < ntile; t++) tp->maxcnt = std::max(tp->maxcnt, toff[t + 1] - toff[t]);
-    return tp;
+    for (int t = 0; t < ntile; t++) tl.maxcnt = std::max(tl.maxcnt, toff[t + 1] - toff[t]);
+    *out = tl;
+    return true;
   }
-  free_tile_plan(tp);
+  free_tile_lists(&tl, s);
+  return false;
+}
+
+void free_tile_lists(TileLists *tl, cudaStream_t s) {
+  for (void *p : {(void *)tl->toff, (void *)tl->tflux, (void *)tl->tell})
+    if (p) cudaFreeAsync(p, s);
+  *tl = TileLists();
+}
+
+// the plain path's tile plan for tiles of ct cells; nullptr when it cannot
+// be built (synchronises: a loop's first call, never inside a capture)
+static TilePlan *build_tile_plan(const SlotPlan *sp, int ct) {
+  TilePlan *tp = new TilePlan();
+  if (build_tile_lists((const int *)sp->d_ell, sp->ntarget, sp->width, ct, rt().stream, &tp->tl))
+    return tp;
+  delete tp;
   return nullptr;
 }
 
@@ -2149,137 +2166,31 @@ __global__ void __launch_bounds__(BS, 1024 / BS)
                   T *seq, RedSlot<T> slot, unsigned *ticket, T *qsave, T *__restrict__ adt_out) {
   extern __shared__ __align__(16) unsigned char tile_smem[];
   T *fv = reinterpret_cast<T *>(tile_smem);  // [maxcnt][4]
-  const unsigned n_e = (unsigned)ne;
   T rms = T(0);
-  int *fidx = reinterpret_cast<int *>(fv);
-  constexpr int kSlotInts = 4 * (int)sizeof(T) / (int)sizeof(int);
+  auto bres = [&](int b, T (&r)[4]) {
+    int m1, m2;
+    at2(B.x1, B.x2, b, m1, m2);
+    T p[2], sx[2], q1[4];
+    ld2(B.xa + 2 * (size_t)m1, p);
+    ld2(B.xb + 2 * (size_t)m2, sx);
+    ld4(B.q_d + 4 * (size_t)at(B.q, b), q1);
+    bres_contrib(p, sx, q1, __ldg(B.adt + at(B.a, b)), __ldg(B.bound_d + at(B.bound, b)), K, r);
+  };
   for (int t = blockIdx.x; t < P.ntile; t += gridDim.x) {
     const int beg = __ldg(P.toff + t), cnt = __ldg(P.toff + t + 1) - beg;
-    // the tile's flux indices (plan data, so the first tile's are read
-    // before the previous kernel has finished) into shared memory, each in
-    // the first word of the slot its flux will take; then the fluxes, one
-    // per thread per pass, the next pass's map entries fetched while this
-    // one gathers
-    for (int i = threadIdx.x; i < cnt; i += BS) fidx[kSlotInts * i] = __ldg(P.tflux + beg + i);
+    // plan data, so the first tile's indices are staged before the previous
+    // kernel has finished
+    tile_stage<T, BS>(P.tflux, beg, cnt, fv);
     if (t == (int)blockIdx.x) {
       pdl_wait();
       pdl_trigger();
     }
     __syncthreads();
-    int i = threadIdx.x;
-    unsigned f = i < cnt ? (unsigned)fidx[kSlotInts * i] : ~0u;
-    int2 nn = make_int2(0, 0), cc = make_int2(0, 0);
-    if (f < n_e) {
-      nn = __ldg(pedge + f);
-      cc = __ldg(pecell + f);
-    }
-    for (; i < cnt; i += BS) {
-      const int in = i + BS;
-      const unsigned fn = in < cnt ? (unsigned)fidx[kSlotInts * in] : ~0u;
-      T r[4];
-      if (f < n_e) {
-        T p[2], sx[2], q1[4], q2[4];
-        ld4(q + 4u * (unsigned)cc.x, q1);
-        ld4(q + 4u * (unsigned)cc.y, q2);
-        ld2(x + 2u * (unsigned)nn.x, p);
-        ld2(x + 2u * (unsigned)nn.y, sx);
-        const T d1 = __ldg(adt + (unsigned)cc.x), d2 = __ldg(adt + (unsigned)cc.y);
-        if (fn < n_e) {
-          nn = __ldg(pedge + fn);
-          cc = __ldg(pecell + fn);
-        }
-        res_flux(p, sx, q1, q2, d1, d2, K.gm1, K.eps, r);
-      } else {
-        if (f - n_e < (unsigned)B.n) {
-          const int b = (int)(f - n_e);
-          int m1, m2;
-          at2(B.x1, B.x2, b, m1, m2);
-          T p[2], sx[2], q1[4];
-          ld2(B.xa + 2 * (size_t)m1, p);
-          ld2(B.xb + 2 * (size_t)m2, sx);
-          ld4(B.q_d + 4 * (size_t)at(B.q, b), q1);
-          bres_contrib(p, sx, q1, __ldg(B.adt + at(B.a, b)),
-                       __ldg(B.bound_d + at(B.bound, b)), K, r);
-        } else {  // the lists' padding value: -0.0, the identity of addition
-          r[0] = r[1] = r[2] = r[3] = -T(0);
-        }
-        if (fn < n_e) {
-          nn = __ldg(pedge + fn);
-          cc = __ldg(pecell + fn);
-        }
-      }
-      st4(fv + 4 * i, r);
-      f = fn;
-    }
+    tile_fluxes<T, BS>(cnt, (unsigned)ne, (unsigned)B.n, pedge, pecell, x, q, adt, K, fv, bres);
     __syncthreads();
-    // cells: fold from shared memory in list order, update, adt_calc; the
-    // next cell's list, nodes and own streams fetched while this one works
-    const int c1 = min(ncell, (t + 1) * P.ct);
-    auto fetch = [&](int c, int (&k)[4], int (&nd)[4], T (&r)[4], T (&qo)[4], T &ad) {
-      list_head(P.tell, P.W, c, k);
-      if (ADT) {
-        const int4 v = __ldg(pcell + c);
-        nd[0] = v.x; nd[1] = v.y; nd[2] = v.z; nd[3] = v.w;
-      }
-      ldw4(res + 4 * (size_t)c, r);
-      if (SAVE) ldw4(qold + 4 * (size_t)c, qo);
-      else ld4(qold + 4 * (size_t)c, qo);
-      ad = __ldg(adt + c);
-    };
-    int c = t * P.ct + threadIdx.x;
-    int k[4] = {-1, -1, -1, -1}, nd[4] = {0, 0, 0, 0};
-    T r[4], qo[4], ad = T(1);
-    if (c < c1) fetch(c, k, nd, r, qo, ad);
-    for (; c < c1; c += BS) {
-      T xs[4][2];
-      if (ADT)
-#pragma unroll
-        for (int j = 0; j < 4; j++) ld2(xc + 2 * (size_t)nd[j], xs[j]);
-      const int cn = c + BS;
-      int kn[4] = {-1, -1, -1, -1}, ndn[4] = {0, 0, 0, 0};
-      T rn[4], qon[4], adn = T(1);
-      if (cn < c1) fetch(cn, kn, ndn, rn, qon, adn);
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-        if (k[j] >= 0) {
-          T fj[4];
-          ldw4(fv + 4 * (k[j] >> 1), fj);
-          add_listed(r, k[j], fj);
-        }
-      for (int j = 4; j < P.W; j++) {  // lists longer than 4
-        const int kk = __ldg(P.tell + (size_t)c * P.W + j);
-        if (kk < 0) continue;
-        T fj[4];
-        ldw4(fv + 4 * (kk >> 1), fj);
-        add_listed(r, kk, fj);
-      }
-      // airfoil/update.h:1-12
-      const T adti = rcp(ad);
-      T qn[4], sq[4];
-      for (int d = 0; d < 4; d++) {
-        const T del = adti * r[d];
-        qn[d] = qo[d] - del;
-        sq[d] = del * del;
-        rms += sq[d];
-      }
-      st4(qout + 4 * (size_t)c, qn);
-      if (SAVE) st4(qsave + 4 * (size_t)c, qn);  // airfoil/save_soln.h:1-3
-      const T z[4] = {T(0), T(0), T(0), T(0)};
-      st4(res + 4 * (size_t)c, z);
-      if (seq) st4(seq + 4 * (size_t)c, sq);
-      if (ADT) adt_out[c] = adt_calc(xs[0], xs[1], xs[2], xs[3], qn, K);
-      if (cn < c1) {
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-          k[j] = kn[j];
-          nd[j] = ndn[j];
-          r[j] = rn[j];
-          qo[j] = qon[j];
-        }
-        ad = adn;
-      }
-    }
-    __syncthreads();  // the next tile reuses the shared fluxes
+    rms += tile_cells<T, ADT, SAVE, BS>(t * P.ct, min(ncell, (t + 1) * P.ct), P.tell, P.W, pcell,
+                                        xc, qold, adt, qout, res, qsave, adt_out, seq, K, fv);
+    __syncthreads();  // the next tile reuses the shared values
   }
   if (seq) return;
   const T v[1] = {rms}, id[1] = {T(0)};
@@ -2377,7 +2288,7 @@ static bool tiled_chain(const std::string &name, SlotPlan *sp, const op_arg *ra,
                        ? tuning("tile_cells", 0)
                        : (int)std::max(64LL, (ncell + ctas - 1) / ctas);
   if (!sp->tile || sp->tile->want != want ||
-      (size_t)sp->tile->maxcnt * 4 * sizeof(T) > budget) {
+      (size_t)sp->tile->tl.maxcnt * 4 * sizeof(T) > budget) {
     if (capturing) return false;  // plans are built before a capture
     release_tile_plan(sp);
     for (int ct = want;; ct = ct * 3 / 4) {
@@ -2390,7 +2301,7 @@ static bool tiled_chain(const std::string &name, SlotPlan *sp, const op_arg *ra,
         sp->tile_unsuited = true;
         return false;
       }
-      if ((size_t)tp->maxcnt * 4 * sizeof(T) <= budget) {
+      if ((size_t)tp->tl.maxcnt * 4 * sizeof(T) <= budget) {
         tp->want = want;
         sp->tile = tp;
         break;
@@ -2399,7 +2310,7 @@ static bool tiled_chain(const std::string &name, SlotPlan *sp, const op_arg *ra,
     }
   }
   TilePlan *tp = sp->tile;
-  const size_t smem = (size_t)tp->maxcnt * 4 * sizeof(T);
+  const size_t smem = (size_t)tp->tl.maxcnt * 4 * sizeof(T);
   void *qout = alt_of(q);
   void *adt_to = nullptr;
   bool flip_adt = false;
@@ -2428,8 +2339,8 @@ static bool tiled_chain(const std::string &name, SlotPlan *sp, const op_arg *ra,
   T *seqbuf = seq ? (T *)red_seq_buffer(sizeof(T) * 4 * (size_t)ncell) : nullptr;
   T *result = (T *)red_slot_ptr(rslot_id);
   RedSlot<T> rslot{(T *)red_partials(0), result};
-  const int grid = std::min(tp->ntile, std::min(kMaxRedBlocks, rt().num_sms * per_sm));
-  TileView P{tp->ct, tp->ntile, sp->width, tp->d_toff, tp->d_tflux, tp->d_tell};
+  const int grid = std::min(tp->tl.ntile, std::min(kMaxRedBlocks, rt().num_sms * per_sm));
+  TileView P{tp->tl.ct, tp->tl.ntile, sp->width, tp->tl.toff, tp->tl.tflux, tp->tl.tell};
   const T *xc = aa ? (const T *)aa[0].dat->data_d : nullptr;
   const int4 *pcell = aa ? reinterpret_cast<const int4 *>(map_dev(aa[0].map)) : nullptr;
   T *qsave = sa ? (T *)(save_out ? save_out : sa[1].dat->data_d) : nullptr;

@@ -42,6 +42,7 @@
 #include "launch.cuh"
 #include "op2b_group.h"
 #include "reduce.cuh"
+#include "tile_chain.cuh"
 
 namespace op2b {
 namespace {
@@ -58,6 +59,10 @@ struct SolveDev {  // device view of one solve; written by the host only
   const int *pedge, *pecell, *pbedge, *pbecell, *bound, *pcell, *ell;
   int ncell, nedge, nbedge, W, ntiles, pad;
   T qinf[4];
+  // the tiled chain: second buffers of q and adt, and the tile lists
+  T *q2, *adt2;
+  const int *toff, *tflux, *tell;
+  int tct, tntile;
 };
 
 struct SolveState {  // written by the kernels
@@ -79,6 +84,43 @@ __device__ __forceinline__ AirConsts<T> with_qinf(AirConsts<T> K, const SolveDev
 #pragma unroll
   for (int i = 0; i < 4; i++) K.qinf[i] = d->qinf[i];
   return K;
+}
+
+// The end of an iteration's second update: this CTA's rms partial (its
+// threads' sums, block tree) into the solve's slot for the tile; the
+// solve's last CTA folds the ntiles partials in tile order, records
+// rms = sqrt(sum / ncell) (airfoil/airfoil_op.cpp:291) and applies the
+// stopping test (iteration cap, or rms below tol x the first iteration's)
+template <class T>
+__device__ __forceinline__ void end_of_iteration(const SolveDev<T> *d, SolveState *st,
+                                                 const Tile &t, T rms, int ntiles) {
+  __shared__ T ws[32];
+  __shared__ bool last;
+  const T b = block_fold(rms, T(0), OpSum(), ws);
+  if (threadIdx.x == 0) {  // the writer fences its partial, then takes a ticket
+    d->partials[t.local] = b;
+    __threadfence();
+    last = atomicAdd(&st[t.solve].ticket, 1u) == (unsigned)(ntiles - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  T sum = T(0);
+  for (int p = threadIdx.x; p < ntiles; p += blockDim.x) sum += __ldcg(d->partials + p);
+  sum = block_fold(sum, T(0), OpSum(), ws);
+  if (threadIdx.x == 0) {
+    SolveState &s = st[t.solve];
+    const T r = sqrt(sum / (T)d->ncell);
+    const int it = s.iter;
+    d->hist[it] = r;
+    const int done = it + 1;
+    if (done == 1) s.rms1 = (double)r;
+    const bool stop =
+        done >= s.max_iter || (done >= 2 && s.tol > 0.0 && (double)r < s.tol * s.rms1);
+    s.iter = done;
+    if (stop) s.active = 0;
+    s.ticket = 0u;
+  }
 }
 
 // save_soln + adt_calc over one tile of one solve's cells (a thread's cells
@@ -239,33 +281,57 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? (MODE == 1 ? 4 : 3)
     if (ADT) adt[c] = adt_calc(xs[0], xs[1], xs[2], xs[3], qn, K);
   }
   if (FIRST) return;
-  __shared__ T ws[32];
-  __shared__ bool last;
-  const T b = block_fold(rms, T(0), OpSum(), ws);
-  if (threadIdx.x == 0) {  // the writer fences its partial, then takes a ticket
-    d->partials[t.local] = b;
-    __threadfence();
-    last = atomicAdd(&st[t.solve].ticket, 1u) == (unsigned)(d->ntiles - 1);
-  }
+  end_of_iteration(d, st, t, rms, d->ntiles);
+}
+
+// The tiled chain over one tile of one solve's cells per CTA
+// (tile_chain.cuh): res_calc + bres_calc + update [+ adt_calc] [+ save_soln]
+// in one launch over all solves, the flux values in shared memory instead of
+// a DRAM round trip.  The fluxes read q and adt of cells in other tiles of
+// the same solve, so update and adt_calc write to the other buffer: PAR 0
+// reads (q, adt) and writes (q2, adt2), PAR 1 the reverse.  An iteration is
+// two chains (PAR 0, then PAR 1), so (q, adt) hold the state between
+// iterations.  MODE as in k_grp_fold; the rms partials are per tile of this
+// tiling (tntile of them), so the rms's summation tree differs from the
+// two-launch form's while every field is bit-identical to it.
+template <class T, int MODE, int PAR>
+__global__ void __launch_bounds__(1024, 1)
+    k_grp_chain_tiled(const Tile *__restrict__ tiles, const SolveDev<T> *__restrict__ sd,
+                      SolveState *st, AirConsts<T> K0) {
+  constexpr bool FIRST = MODE == 0, ADT = MODE != 1, SAVE = MODE == 2;
+  extern __shared__ __align__(16) unsigned char grp_tile_smem[];
+  T *fv = reinterpret_cast<T *>(grp_tile_smem);
+  const Tile t = tiles[blockIdx.x];
+  const SolveDev<T> *d = sd + t.solve;
+  const int beg = __ldg(d->toff + t.local), cnt = __ldg(d->toff + t.local + 1) - beg;
+  tile_stage<T, 1024>(d->tflux, beg, cnt, fv);  // plan data: before the wait
+  pdl_wait();
+  pdl_trigger();
+  if (!solve_active(st, t.solve)) return;  // the same for the whole CTA
+  const AirConsts<T> K = with_qinf(K0, d);
+  const T *x = d->x;
+  const T *qin = PAR ? d->q2 : d->q, *ain = PAR ? d->adt2 : d->adt;
+  T *qout = PAR ? d->q : d->q2, *aout = PAR ? d->adt : d->adt2;
+  const int2 *pbedge = reinterpret_cast<const int2 *>(d->pbedge);
+  auto bres = [&](int b, T (&r)[4]) {
+    const int2 bn = __ldg(pbedge + b);
+    const int c = __ldg(d->pbecell + b);
+    T p[2], sx[2], q1[4];
+    ld2(x + 2 * (size_t)bn.x, p);
+    ld2(x + 2 * (size_t)bn.y, sx);
+    ld4(qin + 4 * (size_t)c, q1);
+    bres_contrib(p, sx, q1, __ldg(ain + c), __ldg(d->bound + b), K, r);
+  };
   __syncthreads();
-  if (!last) return;
-  __threadfence();
-  T sum = T(0);
-  for (int p = threadIdx.x; p < d->ntiles; p += kThreads) sum += __ldcg(d->partials + p);
-  sum = block_fold(sum, T(0), OpSum(), ws);
-  if (threadIdx.x == 0) {
-    SolveState &s = st[t.solve];
-    const T r = sqrt(sum / (T)d->ncell);  // airfoil/airfoil_op.cpp:291
-    const int it = s.iter;
-    d->hist[it] = r;
-    const int done = it + 1;
-    if (done == 1) s.rms1 = (double)r;
-    const bool stop =
-        done >= s.max_iter || (done >= 2 && s.tol > 0.0 && (double)r < s.tol * s.rms1);
-    s.iter = done;
-    if (stop) s.active = 0;
-    s.ticket = 0u;
-  }
+  tile_fluxes<T, 1024>(cnt, (unsigned)d->nedge, (unsigned)d->nbedge,
+                       reinterpret_cast<const int2 *>(d->pedge),
+                       reinterpret_cast<const int2 *>(d->pecell), x, qin, ain, K, fv, bres);
+  __syncthreads();
+  const T rms = tile_cells<T, ADT, SAVE, 1024>(
+      t.start, t.start + t.count, d->tell, d->W, reinterpret_cast<const int4 *>(d->pcell), x,
+      d->qold, ain, qout, d->res, d->qold, aout, nullptr, K, fv);
+  if (FIRST) return;
+  end_of_iteration(d, st, t, rms, d->tntile);
 }
 
 // ------------------------------------------------ contribution lists ------
@@ -399,6 +465,8 @@ struct GroupBase {
   virtual int set_edge_tile(int e) = 0;
   virtual int set_block_bytes(long long bytes) = 0;
   virtual int set_streams(int n) = 0;
+  virtual int set_tiled(int on) = 0;
+  virtual int tiled_mode() = 0;
   virtual int edge_tile() = 0;
   virtual int autotune(int iters) = 0;
 };
@@ -418,6 +486,10 @@ struct Group : GroupBase {
     bool primed = false;
     long long join_epoch = 0;  // the first state mirror that includes this solve
     SolveDev<T> dev;
+    // the tiled chain's second buffers of q and adt, and tile lists
+    void *tbuf = nullptr;
+    TileLists tl;
+    size_t tbytes = 0;
   };
 
   cudaStream_t cs = nullptr, us = nullptr;  // iterations; admission
@@ -440,6 +512,13 @@ struct Group : GroupBase {
   // save_soln + adt_calc -- four launches; a solve's very first save_soln +
   // adt_calc is a priming launch of its own (pt: the unprimed solves' tiles)
   bool rotate = true;
+  // the tiled chain (op2b_group_set_tiled): one launch per update, each CTA
+  // one tile of one solve, its flux values in shared memory
+  bool tiled = false;
+  Tile *d_tt = nullptr;
+  size_t tt_cap = 0;
+  int ntt = 0;
+  size_t tsmem = 0, tsmem_set = 0;
   int etile = 2048;
   bool changed = true;
   cudaGraphExec_t exec = nullptr;
@@ -472,6 +551,7 @@ struct Group : GroupBase {
     cudaFree(d_ct);
     cudaFree(d_et);
     cudaFree(d_pt);
+    cudaFree(d_tt);
     if (h_st) cudaFreeHost(h_st);
     if (mirror_ev) cudaEventDestroy(mirror_ev);
     if (cs) cudaStreamDestroy(cs);
@@ -484,6 +564,9 @@ struct Group : GroupBase {
     if (s.removed) return;
     if (s.block) cudaFreeAsync(s.block, s.joined ? cs : us);
     if (s.ell) cudaFreeAsync(s.ell, s.joined ? cs : us);
+    if (s.tbuf) cudaFreeAsync(s.tbuf, s.joined ? cs : us);
+    free_tile_lists(&s.tl, s.joined ? cs : us);
+    s.tbuf = nullptr;
     if (s.ready) cudaEventDestroy(s.ready);
     s.block = nullptr;
     s.ell = nullptr;
@@ -517,9 +600,61 @@ struct Group : GroupBase {
     return tot;
   }
 
+  // the tiled chain's extra bytes of a solve: q2 and adt2, the rewritten
+  // lists (width about 4) and the tiles' flux indices (the edges, a share
+  // of them twice, and the boundary edges)
+  static size_t tiled_bytes(int nc, int ne, int nb) {
+    return align256(sizeof(T) * 5 * (size_t)nc) + align256(sizeof(int) * 4 * (size_t)nc) +
+           align256(sizeof(int) * (size_t)((ne + nb) * 5LL / 4 + 1024));
+  }
+
   long long solve_bytes(int nn, int nc, int ne, int nb, int max_iter) override {
     size_t off[16];
-    return (long long)(layout(nn, nc, ne, nb, max_iter, off) + align256(sizeof(int) * 4 * (size_t)nc));
+    return (long long)(layout(nn, nc, ne, nb, max_iter, off) +
+                       align256(sizeof(int) * 4 * (size_t)nc) +
+                       (tiled ? tiled_bytes(nc, ne, nb) : 0));
+  }
+
+  // cells per tile of the tiled chain: the largest of 4096, 3072, 2304, ...
+  // (FP32; half that in FP64), at least the rms tile, whose longest flux run
+  // fits one CTA's shared memory
+  bool ensure_tiled(Solve &s, cudaStream_t st) {
+    if (s.tbuf) return true;
+    const size_t budget = (size_t)rt().smem_optin - 2048;
+    void *buf = nullptr;
+    if (pool_malloc_async(&buf, sizeof(T) * 5 * (size_t)s.ncell, st) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    TileLists tl;
+    bool ok = false;
+    for (int ct = sizeof(T) == 4 ? 4096 : 2048; ct >= kCellTile; ct = ct * 3 / 4) {
+      if (!build_tile_lists(s.ell, s.ncell, s.dev.W, ct, st, &tl)) break;
+      if ((size_t)tl.maxcnt * 4 * sizeof(T) <= budget) {
+        ok = true;
+        break;
+      }
+      free_tile_lists(&tl, st);
+    }
+    if (!ok) {
+      cudaFreeAsync(buf, st);
+      return false;
+    }
+    s.tbuf = buf;
+    s.tl = tl;
+    s.tbytes = align256(sizeof(T) * 5 * (size_t)s.ncell) +
+               align256(sizeof(int) * (size_t)s.dev.W * s.ncell) +
+               align256(sizeof(int) * (size_t)(s.nedge + s.nbedge) * 5 / 4);
+    s.bytes += s.tbytes;
+    SolveDev<T> &d = s.dev;
+    d.q2 = (T *)buf;
+    d.adt2 = (T *)buf + 4 * (size_t)s.ncell;
+    d.toff = tl.toff;
+    d.tflux = tl.tflux;
+    d.tell = tl.tell;
+    d.tct = tl.ct;
+    d.tntile = tl.ntile;
+    return true;
   }
 
   int add(const op2b_mesh *m, double mach, double alpha, int max_iter, double tol) override {
@@ -601,6 +736,12 @@ struct Group : GroupBase {
     OP2B_CUDA(cudaMemsetAsync(d.adt, 0, sizeof(T) * (size_t)s.ncell, us));
     k_gl_init<T><<<grid, 256, 0, us>>>(s.ncell, d.q, d.res, d.vals + 4 * ((size_t)s.nedge + s.nbedge),
                                        d.qinf[0], d.qinf[1], d.qinf[2], d.qinf[3]);
+    if (tiled && !ensure_tiled(s, us)) {
+      cudaFreeAsync(s.ell, us);
+      cudaFreeAsync(s.block, us);
+      fail(-1, "op2b_group_add error -- no tile size fits the tiled chain's shared memory\n");
+      return -1;
+    }
     OP2B_CUDA(cudaEventCreateWithFlags(&s.ready, cudaEventDisableTiming));
     OP2B_CUDA(cudaEventRecord(s.ready, us));
     if (error_pending()) return -1;
@@ -656,7 +797,7 @@ struct Group : GroupBase {
   // whose values go out to DRAM and back.  A block holds solves in id order
   // up to block_bytes of values (a larger solve makes a block of its own).
   struct Block {
-    int ct0, nct, et0, net;
+    int ct0, nct, et0, net, tt0, ntt;
   };
   std::vector<Block> blocks;
   // default one block: measured on 64 solves (12M cells), blocks of 24, 48
@@ -666,11 +807,23 @@ struct Group : GroupBase {
   size_t block_bytes = ~(size_t)0;
 
   void rebuild() {
-    std::vector<Tile> ct, et, pt;
+    std::vector<Tile> ct, et, pt, tt;
     blocks.clear();
     nactive = 0;
     rotate = tuning("group_rotate", 1) != 0;
     size_t in_block = 0;
+    tsmem = 0;
+    if (tiled)  // tile lists of solves that joined before the tiled chain was chosen
+      for (int id = 0; id < (int)solves.size(); id++) {
+        Solve &s = solves[id];
+        if (!s.joined || s.removed || s.done || s.tbuf) continue;
+        if (!ensure_tiled(s, cs)) {
+          tiled = false;  // this solve cannot: the whole group takes the two launches
+          break;
+        }
+        OP2B_CUDA(cudaMemcpyAsync(d_sd + id, &s.dev, sizeof(SolveDev<T>), cudaMemcpyHostToDevice,
+                                  cs));
+      }
     for (int id = 0; id < (int)solves.size(); id++) {
       const Solve &s = solves[id];
       if (!s.joined || s.removed || s.done) continue;
@@ -681,7 +834,7 @@ struct Group : GroupBase {
       const int nv = s.nedge + s.nbedge;
       const size_t vbytes = sizeof(T) * 4 * (size_t)nv;
       if (blocks.empty() || (in_block > 0 && in_block + vbytes > block_bytes)) {
-        blocks.push_back(Block{(int)ct.size(), 0, (int)et.size(), 0});
+        blocks.push_back(Block{(int)ct.size(), 0, (int)et.size(), 0, (int)tt.size(), 0});
         in_block = 0;
       }
       in_block += vbytes;
@@ -689,15 +842,30 @@ struct Group : GroupBase {
         ct.push_back(Tile{id, a, std::min(kCellTile, s.ncell - a), l});
       for (int a = 0, l = 0; a < nv; a += etile, l++)
         et.push_back(Tile{id, a, std::min(etile, nv - a), l});
+      if (tiled) {
+        for (int a = 0, l = 0; a < s.ncell; a += s.tl.ct, l++)
+          tt.push_back(Tile{id, a, std::min(s.tl.ct, s.ncell - a), l});
+        tsmem = std::max(tsmem, (size_t)s.tl.maxcnt * 4 * sizeof(T));
+      }
       blocks.back().nct = (int)ct.size() - blocks.back().ct0;
       blocks.back().net = (int)et.size() - blocks.back().et0;
+      blocks.back().ntt = (int)tt.size() - blocks.back().tt0;
     }
     upload_tiles(d_ct, ct_cap, ct);
     upload_tiles(d_et, et_cap, et);
     upload_tiles(d_pt, pt_cap, pt);
+    upload_tiles(d_tt, tt_cap, tt);
     nct = (int)ct.size();
     net = (int)et.size();
     npt = (int)pt.size();
+    ntt = (int)tt.size();
+    if (tiled && tsmem > tsmem_set) {
+      for (const void *k : {(const void *)k_grp_chain_tiled<T, 0, 0>,
+                            (const void *)k_grp_chain_tiled<T, 1, 1>,
+                            (const void *)k_grp_chain_tiled<T, 2, 1>})
+        OP2B_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem));
+      tsmem_set = tsmem;
+    }
     if (exec) {
       cudaGraphExecDestroy(exec);
       exec = nullptr;
@@ -740,6 +908,18 @@ struct Group : GroupBase {
     if (!rotate)
       launch_pdl(k_grp_save_adt<T>, b.nct, kThreads, 0, cs, ct, (const SolveDev<T> *)d_sd,
                  (const SolveState *)d_st, K);
+    if (tiled) {  // (q, adt) -> (q2, adt2) -> (q, adt)
+      const Tile *tt = d_tt + b.tt0;
+      launch_pdl(k_grp_chain_tiled<T, 0, 0>, b.ntt, 1024, tsmem, cs, tt,
+                 (const SolveDev<T> *)d_sd, d_st, K);
+      if (rotate)
+        launch_pdl(k_grp_chain_tiled<T, 2, 1>, b.ntt, 1024, tsmem, cs, tt,
+                   (const SolveDev<T> *)d_sd, d_st, K);
+      else
+        launch_pdl(k_grp_chain_tiled<T, 1, 1>, b.ntt, 1024, tsmem, cs, tt,
+                   (const SolveDev<T> *)d_sd, d_st, K);
+      return;
+    }
     launch_pdl(k_grp_flux<T>, b.net, kThreads, 0, cs, et, (const SolveDev<T> *)d_sd,
                (const SolveState *)d_st, K);
     launch_pdl(k_grp_fold<T, 0>, b.nct, kThreads, 0, cs, ct, (const SolveDev<T> *)d_sd, d_st, K);
@@ -886,7 +1066,7 @@ struct Group : GroupBase {
     for (auto &s : solves)
       if (!s.removed) b += (long long)s.bytes;
     return b + (long long)cap * (sizeof(SolveDev<T>) + sizeof(SolveState)) +
-           (long long)(ct_cap + et_cap) * sizeof(Tile);
+           (long long)(ct_cap + et_cap + tt_cap) * sizeof(Tile);
   }
 
   int active() override { return nactive; }
@@ -897,6 +1077,13 @@ struct Group : GroupBase {
     block_bytes = b;
     return 0;
   }
+
+  int set_tiled(int on) override {
+    if ((on != 0) != tiled) changed = true;
+    tiled = on != 0;
+    return 0;
+  }
+  int tiled_mode() override { return tiled ? 1 : 0; }
 
   int set_streams(int n) override {
     if (n < 1 || n > 8) {
@@ -1080,6 +1267,8 @@ int op2b_group_set_block_bytes(op2b_group g, long long bytes) {
 }
 int op2b_group_edge_tile(op2b_group g) { GROUP_CALL(edge_tile()); }
 int op2b_group_set_streams(op2b_group g, int n) { GROUP_CALL(set_streams(n)); }
+int op2b_group_set_tiled(op2b_group g, int on) { GROUP_CALL(set_tiled(on)); }
+int op2b_group_tiled(op2b_group g) { GROUP_CALL(tiled_mode()); }
 int op2b_group_autotune(op2b_group g, int iters) { GROUP_CALL(autotune(iters)); }
 
 }  // extern "C"

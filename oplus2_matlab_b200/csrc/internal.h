@@ -173,6 +173,15 @@ int live_graphs();   // captured graphs not yet destroyed (graph.cu)
 void tile_capture_begin();  // graph capture: count the tiled chain's buffer swaps
 void tile_capture_end();    // ... and undo an odd count inside the graph
 void release_tile_alts();   // op_exit: free the tiled chain's second buffers
+// The tiled res_calc chain's lists (airfoil.cu): for tiles of ct consecutive
+// cells, each tile's distinct list indices ascending (tflux, tile t's run at
+// toff[t]) and each list entry as (slot in its tile's run << 1 | side)
+struct TileLists {
+  int ct = 0, ntile = 0, maxcnt = 0;  // cells per tile, tiles, the longest run
+  int *toff = nullptr, *tflux = nullptr, *tell = nullptr;
+};
+bool build_tile_lists(const int *ell, int ncell, int W, int ct, cudaStream_t s, TileLists *out);
+void free_tile_lists(TileLists *tl, cudaStream_t s);
 // sorts the m 64-bit keys at a (m a power of two) ascending on stream s
 bool sort_keys_u64(unsigned long long *a, long long m, cudaStream_t s);
 

@@ -193,6 +193,11 @@ class Group:
     def set_streams(self, n):
         self._check(self.lib.op2b_group_set_streams(self.h, int(n)), "op2b_group_set_streams")
 
+    def set_tiled(self, on=True):
+        """One launch per update over all solves, flux values in shared
+        memory (op2b_group_set_tiled); fields unchanged."""
+        self._check(self.lib.op2b_group_set_tiled(self.h, 1 if on else 0), "op2b_group_set_tiled")
+
     def set_block_bytes(self, nbytes):
         self._check(self.lib.op2b_group_set_block_bytes(self.h, int(nbytes)),
                     "op2b_group_set_block_bytes")
