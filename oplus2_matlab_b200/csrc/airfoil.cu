@@ -1397,7 +1397,7 @@ static void update_t(char const *name, op_set set, const op_arg *args) {
     else launch(k_update<T, 4>);
     if (seq) {
       T init = *(const T *)args[4].data;
-      k_seq_sum<T><<<1, 32, 0, s>>>(seqbuf, 4LL * n, init, result);
+      k_seq_sum<T><<<1, 32, 0, s>>>(seqbuf, 4LL * n, init, result, perm_old2new_dev(set), 4);
     }
   }
   red_finish({GblRequest{args[4].data, slot, OP_INC, sizeof(T) == 8 ? GBL_F64 : GBL_F32, seq}});
@@ -1976,7 +1976,8 @@ static bool persist_chain(const std::string &name, SlotPlan *sp, const op_arg *r
   }
   if (seq) {
     T init = *(const T *)ua[4].data;
-    k_seq_sum<T><<<1, 32, 0, s>>>(seqbuf, 4LL * ncell, init, result);
+    k_seq_sum<T><<<1, 32, 0, s>>>(seqbuf, 4LL * ncell, init, result,
+                                  perm_old2new_dev(ra[6].dat->set), 4);
   }
   return true;
 }
@@ -2369,7 +2370,8 @@ static bool tiled_chain(const std::string &name, SlotPlan *sp, const op_arg *ra,
   if (flip_adt) flip(adt, capturing);
   if (seq) {
     T init = *(const T *)ua[4].data;
-    k_seq_sum<T><<<1, 32, 0, s>>>(seqbuf, 4LL * ncell, init, result);
+    k_seq_sum<T><<<1, 32, 0, s>>>(seqbuf, 4LL * ncell, init, result,
+                                  perm_old2new_dev(ra[6].dat->set), 4);
   }
   return true;
 }
@@ -2485,7 +2487,8 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
       }
       if (seq) {
         T init = *(const T *)ua[4].data;
-        k_seq_sum<T><<<1, 32, 0, s>>>(seqbuf, 4LL * ncell, init, result);
+        k_seq_sum<T><<<1, 32, 0, s>>>(seqbuf, 4LL * ncell, init, result,
+                                  perm_old2new_dev(ra[6].dat->set), 4);
       }
     }
     }

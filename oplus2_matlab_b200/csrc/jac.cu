@@ -305,7 +305,9 @@ static void jac_update_t(char const *name, op_set set, const op_arg *args,
     launch_pdl(k_jac_update<V>, grid, threads, 0, s, n, (const float *)args[0].dat->data_d,
                (float *)args[1].dat->data_d, (float *)args[2].dat->data_d, alpha, seqbuf, ss, sm,
                red_ticket());
-    if (seq) k_seq_sum<float><<<1, 32, 0, s>>>(seqbuf, n, *(const float *)args[3].data, r_sum);
+    if (seq)
+      k_seq_sum<float><<<1, 32, 0, s>>>(seqbuf, n, *(const float *)args[3].data, r_sum,
+                                        perm_old2new_dev(set), 1);
   }
   std::vector<GblRequest> rq{GblRequest{args[3].data, slot_sum, OP_INC, GBL_F32, seq},
                              GblRequest{args[4].data, slot_max, OP_MAX, GBL_F32, false}};

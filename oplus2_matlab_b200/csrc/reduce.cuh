@@ -99,19 +99,25 @@ __device__ __forceinline__ void grid_finish(const T (&v)[N], const T (&identity)
 // warp: the lanes stage 32-element tiles in shared memory (double buffered),
 // lane 0 folds them.
 template <class T>
-__global__ void k_seq_sum(const T *__restrict__ v, long long n, T init, T *out) {
+__global__ void k_seq_sum(const T *__restrict__ v, long long n, T init, T *out,
+                          const int *__restrict__ order = nullptr, int w = 1) {
   __shared__ T tile[2][1024];
   const int lane = threadIdx.x;
   T acc = init;
   long long base = 0;
   int buf = 0;
-  for (int i = lane; i < 1024; i += 32) tile[0][i] = (i < n) ? v[i] : T(0);
+  // value j of the sum: v[j], or, for a renumbered set, component j % w of
+  // the element the app numbers j / w, stored at order[j / w]
+  auto at = [&](long long j) {
+    return order ? v[(long long)w * order[j / w] + j % w] : v[j];
+  };
+  for (int i = lane; i < 1024; i += 32) tile[0][i] = (i < n) ? at(i) : T(0);
   __syncwarp();
   while (base < n) {
     long long next = base + 1024;
     for (int i = lane; i < 1024; i += 32) {
       long long j = next + i;
-      tile[buf ^ 1][i] = (j < n) ? v[j] : T(0);
+      tile[buf ^ 1][i] = (j < n) ? at(j) : T(0);
     }
     if (lane == 0) {
       long long m = n - base < 1024 ? n - base : 1024;
