@@ -114,6 +114,11 @@ int op2b_group_edge_tile(op2b_group g);
  * current active solves, putting their state back after each trial; keeps
  * the fastest of each and returns the edge tile. */
 int op2b_group_autotune(op2b_group g, int iters);
+/* The same candidates, each timed on `iters` REAL iterations of the active
+ * solves (their state advances; launch shapes do not change results);
+ * keeps the fastest of each and returns the iterations run (11 x iters), or
+ * -1.  Tuning then costs only the graph rebuilds.  Synchronises. */
+int op2b_group_autotune_run(op2b_group g, int iters);
 
 #ifdef __cplusplus
 }

@@ -229,6 +229,7 @@ PROTOTYPES = [
     ("op2b_group_tiled", C.c_int, [_P]),
     ("op2b_group_edge_tile", C.c_int, [_P]),
     ("op2b_group_autotune", C.c_int, [_P, C.c_int]),
+    ("op2b_group_autotune_run", C.c_int, [_P, C.c_int]),
 ]
 
 # data symbols of op_lib.h

@@ -469,6 +469,7 @@ struct GroupBase {
   virtual int tiled_mode() = 0;
   virtual int edge_tile() = 0;
   virtual int autotune(int iters) = 0;
+  virtual int autotune_run(int iters) = 0;
 };
 
 template <class T>
@@ -1194,6 +1195,101 @@ struct Group : GroupBase {
     OP2B_CUDA(cudaStreamSynchronize(cs));
     return error_pending() ? -1 : best;
   }
+
+  // The same candidates timed on real iterations: each candidate runs
+  // `iters` iterations of the active solves, which count (nothing is put
+  // back).  The candidates' graphs are built while the previous candidates'
+  // iterations run (one synchronisation at the end; a graph is destroyed
+  // only then), so tuning costs little beyond the iterations themselves.
+  // Launch shapes do not change results, so a solve ends bit-identical to
+  // an untuned run of the same length.  Returns the iterations run (every
+  // active solve advanced by that many, or stopped).
+  int autotune_run(int iters) override {
+    if (!ok || iters < 1) return -1;
+    join_pending();
+    if (changed) rebuild();
+    if (nactive == 0) return 0;
+    prime();
+    struct Trial {
+      int etile;
+      size_t block_bytes;
+      int nstreams;
+      cudaEvent_t e0 = nullptr, e1 = nullptr;
+    };
+    std::vector<Trial> trials;
+    for (int c : {512, 1024, 2048, 4096, 8192}) trials.push_back(Trial{c, ~(size_t)0, 1});
+    const std::pair<size_t, int> blk[] = {{96u << 20, 1}, {48u << 20, 1}, {48u << 20, 2},
+                                          {24u << 20, 2}, {24u << 20, 3}, {12u << 20, 4}};
+    for (const auto &bb : blk) trials.push_back(Trial{-1, bb.first, bb.second});
+    std::vector<cudaGraphExec_t> retired;  // destroyed after the final synchronisation
+    int ran = 0;
+    auto enqueue = [&](Trial &t) {
+      if (exec) {
+        retired.push_back(exec);
+        exec = nullptr;
+      }
+      rebuild();
+      OP2B_CUDA(cudaEventCreate(&t.e0));
+      OP2B_CUDA(cudaEventCreate(&t.e1));
+      OP2B_CUDA(cudaEventRecord(t.e0, cs));
+      if (exec)
+        for (int i = 0; i < iters; i++) OP2B_CUDA(cudaGraphLaunch(exec, cs));
+      OP2B_CUDA(cudaEventRecord(t.e1, cs));
+      ran += iters;
+    };
+    auto elapsed = [&](Trial &t) {
+      float ms = 1e30f;
+      OP2B_CUDA(cudaEventSynchronize(t.e1));
+      if (cudaEventElapsedTime(&ms, t.e0, t.e1) != cudaSuccess) ms = 1e30f;
+      cudaEventDestroy(t.e0);
+      cudaEventDestroy(t.e1);
+      return ms;
+    };
+    // edge tiles (one block, one stream), then blocks x streams at the best tile
+    const size_t bb0 = block_bytes;
+    const int ns0 = nstreams;
+    for (int k = 0; k < 5; k++) {
+      etile = trials[k].etile;
+      block_bytes = ~(size_t)0;
+      nstreams = 1;
+      enqueue(trials[k]);
+    }
+    int best = 0;
+    float best_ms = 1e30f;
+    for (int k = 0; k < 5; k++) {
+      const float ms = elapsed(trials[k]);
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = k;
+      }
+    }
+    etile = trials[best].etile;
+    std::pair<size_t, int> best_blk{~(size_t)0, 1};
+    for (size_t k = 5; k < trials.size(); k++) {
+      block_bytes = trials[k].block_bytes;
+      nstreams = trials[k].nstreams;
+      enqueue(trials[k]);
+    }
+    for (size_t k = 5; k < trials.size(); k++) {
+      const float ms = elapsed(trials[k]);
+      if (ms < best_ms) {
+        best_ms = ms;
+        best_blk = {trials[k].block_bytes, trials[k].nstreams};
+      }
+    }
+    (void)bb0;
+    (void)ns0;
+    block_bytes = best_blk.first;
+    nstreams = best_blk.second;
+    if (exec) {
+      retired.push_back(exec);
+      exec = nullptr;
+    }
+    rebuild();
+    OP2B_CUDA(cudaStreamSynchronize(cs));
+    for (cudaGraphExec_t e : retired) cudaGraphExecDestroy(e);
+    return error_pending() ? -1 : ran;
+  }
 };
 
 }  // namespace
@@ -1270,5 +1366,6 @@ int op2b_group_set_streams(op2b_group g, int n) { GROUP_CALL(set_streams(n)); }
 int op2b_group_set_tiled(op2b_group g, int on) { GROUP_CALL(set_tiled(on)); }
 int op2b_group_tiled(op2b_group g) { GROUP_CALL(tiled_mode()); }
 int op2b_group_autotune(op2b_group g, int iters) { GROUP_CALL(autotune(iters)); }
+int op2b_group_autotune_run(op2b_group g, int iters) { GROUP_CALL(autotune_run(iters)); }
 
 }  // extern "C"

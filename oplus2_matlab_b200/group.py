@@ -204,3 +204,8 @@ class Group:
 
     def autotune(self, iters=5):
         return self._check(self.lib.op2b_group_autotune(self.h, int(iters)), "op2b_group_autotune")
+
+    def autotune_run(self, iters=1):
+        """Tune on real iterations (they count); returns the iterations run."""
+        return self._check(self.lib.op2b_group_autotune_run(self.h, int(iters)),
+                           "op2b_group_autotune_run")

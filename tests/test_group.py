@@ -261,3 +261,27 @@ def test_tiled_group_solve_alone_equals_in_mix_and_late_switch(op2):
     sw.run(niter - 4)
     assert sw.fetch_q(c).tobytes() == qr.tobytes()
     sw.close()
+
+
+@pytest.mark.gpu
+def test_autotune_on_real_iterations_counts_them(op2):
+    """op2b_group_autotune_run times each launch shape on real iterations of
+    the active solves: after it and the remaining iterations, every solve
+    (one of them stopping during the trials) is bit-identical, q and rms
+    history, to an untuned run of the same length."""
+    niter = 30
+    specs = [((40, 60), 0.45, -1.0, niter), ((30, 45), 0.6, 2.0, niter),
+             ((20, 30), 0.35, 5.0, 5)]
+    ref = G.Group()
+    ids = [ref.add(mesh(*ij), m, a, n) for ij, m, a, n in specs]
+    ref.run(niter)
+    want = [(ref.fetch_q(i).tobytes(), ref.history(i).tobytes()) for i in ids]
+    ref.close()
+    g = G.Group()
+    ids = [g.add(mesh(*ij), m, a, n) for ij, m, a, n in specs]
+    ran = g.autotune_run(2)
+    assert ran == 22  # 11 launch shapes x 2 iterations
+    g.run(niter - ran)
+    got = [(g.fetch_q(i).tobytes(), g.history(i).tobytes()) for i in ids]
+    g.close()
+    assert got == want
