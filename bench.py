@@ -282,6 +282,18 @@ def chain_bytes(m, name, s=4):
     return b
 
 
+def chain_loop_bytes(m, name, s=4):
+    """The chain's loops' compulsory bytes each counted as if the loop ran
+    alone (the per-loop definition: bytes moved per loop), summed."""
+    loops = name.split("+")
+    per = {"res_calc": res_calc_bytes(m, s),
+           "bres_calc": 16 * m.nbedge + (2 * s + 4 * s + s + 8 * s) * m.nbedge,
+           "update": 17 * s * m.ncell,
+           "adt_calc": 16 * m.ncell + 2 * s * m.nnode + 4 * s * m.ncell + s * m.ncell,
+           "save_soln": 8 * s * m.ncell}
+    return float(sum(per[l] for l in loops if l in per))
+
+
 def iteration_bytes(m, s=4):
     save = 8 * s * m.ncell
     adt = 16 * m.ncell + 2 * s * m.nnode + 4 * s * m.ncell + s * m.ncell
@@ -605,7 +617,13 @@ def impl_ours(args, dist):
                      "algorithmic_bytes_per_launch": algo, "avg_launch_us": res_launch_s * 1e6,
                      "timing": "%s, CUDA events, mean of %d launches" % (chain_method, nchain),
                      "profiled_graph_us": profiled_launch_s * 1e6,
-                     "kernels_us": phases},
+                     "kernels_us": phases,
+                     # the per-loop definition (each loop's compulsory bytes as
+                     # if it ran alone, summed over the chain's loops) over
+                     # the same launch time
+                     "per_loop_bytes_per_launch": chain_loop_bytes(mesh, res_key, s),
+                     "frac_per_loop_bytes": chain_loop_bytes(mesh, res_key, s) / res_launch_s
+                                            / 1e9 / peak},
         "iteration_roofline": {"algorithmic_bytes": iter_bytes,
                                "achieved_gbs": iter_bytes * value / dist.world / 1e9,
                                "frac": iter_bytes * value / dist.world / 1e9 / peak},
