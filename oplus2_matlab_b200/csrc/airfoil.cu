@@ -2207,13 +2207,13 @@ static std::vector<void *> g_alt;
 static std::vector<int> g_alt_flips;
 static unsigned long long g_tiled_launches = 0;  // tiled chain launches queued or captured
 
-static void *alt_of(op_dat d) {
+void *alt_of(op_dat d) {
   if (g_alt.size() <= (size_t)d->index) g_alt.resize(d->index + 1, nullptr);
   if (!g_alt[d->index]) g_alt[d->index] = dev_alloc((size_t)d->size * d->set->size);
   return g_alt[d->index];
 }
 
-static void flip(op_dat d, bool capturing) {
+void flip(op_dat d, bool capturing) {
   std::swap(d->data_d, reinterpret_cast<char *&>(g_alt[d->index]));
   if (capturing) {
     if (g_alt_flips.size() <= (size_t)d->index) g_alt_flips.resize(d->index + 1, 0);

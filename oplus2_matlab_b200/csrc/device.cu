@@ -22,6 +22,7 @@ namespace op2b {
 
 void release_fused_plans();  // airfoil.cu
 void release_jac_pairs();    // jac.cu
+void release_jac_steps();    // jac.cu
 
 void ensure_cuda() {
   Runtime &R = rt();
@@ -180,6 +181,7 @@ const int *map_dev(op_map m) {
 void release_plans_and_maps() {
   ::op2b_release_plans();
   release_fused_plans();
+  release_jac_steps();
   release_jac_pairs();
   for (auto &m : rt().maps) {
     dev_free(m.d);
@@ -408,6 +410,7 @@ void op_exit(void) {
   }
   op2b_release_plans();
   release_fused_plans();
+  release_jac_steps();
   release_jac_pairs();
   renumber_reset();
   checkpoint_reset();

@@ -170,6 +170,11 @@ void ahead_drop();   // discard what was run ahead (constants, capture, restore)
 void ahead_reset();  // op_exit: also free the spare buffers
 void noalloc_reset();  // op_exit: forget op2b_update_noalloc's cached scratch addresses
 int live_graphs();   // captured graphs not yet destroyed (graph.cu)
+// A dataset's second device buffer (allocated on first use) and the swap
+// of the two, for loops that write a dataset other elements of the same
+// launch still read (airfoil.cu); swaps made while capturing are counted
+void *alt_of(op_dat d);
+void flip(op_dat d, bool capturing);
 void tile_capture_begin();  // graph capture: count the tiled chain's buffer swaps
 void tile_capture_end();    // ... and undo an odd count inside the graph
 void release_tile_alts();   // op_exit: free the tiled chain's second buffers

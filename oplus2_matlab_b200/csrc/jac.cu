@@ -321,4 +321,252 @@ void run_jac_update(char const *name, op_set set, const op_arg *args, int varian
   else jac_update_t<1>(name, set, args, held);
 }
 
+// ------------------------------------------------- fused jac1 step ------
+// update (iteration k) and the res that follows it (iteration k + 1) as ONE
+// launch.  The nodes are cut into tiles of consecutive nodes, and a CTA takes
+// a tile.  Phase 1: u after update, u + (du + alpha*r), of every node the
+// tile's res contributions read (its own nodes and the neighbours across the
+// tile's edges: recomputed by each tile that reads them, with the same
+// arithmetic) into shared memory.  Phase 2, per node of the tile: update's
+// new u (to the second buffer of u, with the sum and max reductions) and
+// res's new du, 0 + beta*A*u' over its contributions in op_seq.h's order (to
+// the second buffer of du: update leaves du zero, and res adds to that).
+// Other tiles read this tile's old u and du, hence the second buffers, which
+// become the datasets' after the launch.  Per element the arithmetic is that
+// of k_jac_update and k_jac_res_pairs, so u and du are bit-identical to the
+// two launches; only the TREE order of u_sum follows the tiles.
+
+// ELL of the res contributions from the gather plan (every node a target):
+// entry j of node i is its j-th (A element, u element) pair, as
+// (u element << 1) and the A element, or -1 past the node's count
+__global__ void k_jac_ell(int n, int W, const int *__restrict__ row,
+                          const int2 *__restrict__ pairs, int *ell_u, int *ell_a) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)n * W;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int node = (int)(i / W), j = (int)(i % W);
+    const int k = row[node] + j;
+    if (k < row[node + 1]) {
+      const int2 p = pairs[k];
+      ell_u[i] = p.y << 1;
+      ell_a[i] = p.x;
+    } else {
+      ell_u[i] = -1;
+      ell_a[i] = 0;
+    }
+  }
+}
+
+constexpr int kJacStepW = 8;  // the longest contribution list the fused step takes
+
+template <int BS>
+__global__ void __launch_bounds__(BS)
+    k_jac_step(int n, int ntile, int ct, int W, const int *__restrict__ toff,
+               const int *__restrict__ tflux, const int *__restrict__ tell,
+               const int *__restrict__ ell_a, const float *__restrict__ A,
+               const float *__restrict__ r, const float *__restrict__ du,
+               const float *__restrict__ u, float alpha, float beta, float *__restrict__ u_out,
+               float *__restrict__ du_out, float *seq, RedSlot<float> s_sum,
+               RedSlot<float> s_max, unsigned *ticket) {
+  extern __shared__ float us[];
+  constexpr int QA = 4;  // phase-1 elements per thread per pass, loads issued together
+  float sum = 0.0f, mx = -INFINITY;
+  bool waited = false;
+  for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
+    const int beg = __ldg(toff + t), cnt = __ldg(toff + t + 1) - beg;
+    // plan data (read-only, before the wait on the first tile): this
+    // thread's first phase-1 indices
+    int j[QA];
+#pragma unroll
+    for (int q = 0; q < QA; q++) {
+      const int i = threadIdx.x + q * BS;
+      j[q] = i < cnt ? __ldg(tflux + beg + i) : -1;
+    }
+    if (!waited) {
+      pdl_wait();
+      pdl_trigger();
+      waited = true;
+    }
+    // phase 1: u after update of every node the tile's res reads
+    for (int i0 = threadIdx.x; i0 < cnt; i0 += QA * BS) {
+      float uu[QA], dd[QA], rr[QA];
+#pragma unroll
+      for (int q = 0; q < QA; q++)
+        if (j[q] >= 0) {
+          uu[q] = u[j[q]];
+          dd[q] = du[j[q]];
+          rr[q] = __ldg(r + j[q]);
+        }
+      int jn[QA];
+#pragma unroll
+      for (int q = 0; q < QA; q++) {
+        const int i = i0 + (QA + q) * BS;
+        jn[q] = i < cnt ? __ldg(tflux + beg + i) : -1;
+      }
+#pragma unroll
+      for (int q = 0; q < QA; q++)
+        if (j[q] >= 0) us[i0 + q * BS] = uu[q] + (dd[q] + alpha * rr[q]);  // jac1/update.h:2
+#pragma unroll
+      for (int q = 0; q < QA; q++) j[q] = jn[q];
+    }
+    __syncthreads();
+    // phase 2: each node's update and res; its own streams and list entries
+    // first, then the A values they point to
+    const int c1 = min(n, (t + 1) * ct);
+    for (int c = t * ct + threadIdx.x; c < c1; c += BS) {
+      const float u0 = u[c], d0 = du[c], r0 = __ldg(r + c);
+      int kk[kJacStepW], ka[kJacStepW];
+#pragma unroll
+      for (int m = 0; m < kJacStepW; m++) {
+        kk[m] = m < W ? __ldg(tell + (size_t)c * W + m) : -1;
+        ka[m] = m < W ? __ldg(ell_a + (size_t)c * W + m) : 0;
+      }
+      float av[kJacStepW];
+#pragma unroll
+      for (int m = 0; m < kJacStepW; m++) av[m] = kk[m] >= 0 ? __ldg(A + ka[m]) : 0.0f;
+      const float uu = u0 + (d0 + alpha * r0);
+      u_out[c] = uu;
+      const float sq = uu * uu;
+      sum += sq;
+      mx = (mx > uu) ? mx : uu;
+      if (seq) seq[c] = sq;
+      float d = 0.0f;  // update's du = 0, then res adds in list order
+#pragma unroll
+      for (int m = 0; m < kJacStepW; m++)
+        if (kk[m] >= 0) d = jac_inc<1>(d, beta, av[m], us[kk[m] >> 1]);
+      du_out[c] = d;
+    }
+    __syncthreads();  // the next tile reuses the shared u
+  }
+  if (!waited) {
+    pdl_wait();
+    pdl_trigger();
+  }
+  const float v[2] = {sum, mx}, id[2] = {0.0f, -INFINITY};
+  RedSlot<float> sl[2] = {s_sum, s_max};
+  grid_finish<float, OpSum, OpMax, 2>(v, id, OpSum(), OpMax(), sl, ticket);
+}
+
+// the step's plan, by gather plan and the maps of the pairs
+struct JacStep {
+  const GatherPlan *g;
+  op_map mA, mu;
+  int iA, iu, ct;
+  int W = 0;
+  int *ell_a = nullptr;
+  TileLists tl;
+};
+static std::vector<JacStep> g_jac_steps;
+
+void release_jac_steps() {
+  for (auto &p : g_jac_steps) {
+    if (p.ell_a) cudaFreeAsync(p.ell_a, rt().stream);
+    free_tile_lists(&p.tl, rt().stream);
+  }
+  g_jac_steps.clear();
+}
+
+static JacStep *jac_step_plan(const GatherPlan *g, const op_arg *ra, int2 *pairs, int ct,
+                              cudaStream_t s) {
+  for (auto &p : g_jac_steps)
+    if (p.g == g && p.mA == ra[0].map && p.mu == ra[1].map && p.iA == ra[0].idx &&
+        p.iu == ra[1].idx && p.ct == ct)
+      return &p;
+  const int n = g->ntarget, W = g->max_row;
+  if (W < 1 || W > kJacStepW || (long long)n * W >= (1LL << 31)) return nullptr;
+  JacStep p{g, ra[0].map, ra[1].map, ra[0].idx, ra[1].idx, ct};
+  p.W = W;
+  int *ell_u = nullptr;
+  if (pool_malloc_async((void **)&ell_u, sizeof(int) * (size_t)n * W, s) != cudaSuccess ||
+      pool_malloc_async((void **)&p.ell_a, sizeof(int) * (size_t)n * W, s) != cudaSuccess) {
+    cudaGetLastError();
+    if (ell_u) cudaFreeAsync(ell_u, s);
+    if (p.ell_a) cudaFreeAsync(p.ell_a, s);
+    return nullptr;
+  }
+  k_jac_ell<<<rt().num_sms * 8, 256, 0, s>>>(n, W, g->d_row, pairs, ell_u, p.ell_a);
+  const bool ok = build_tile_lists(ell_u, n, W, ct, s, &p.tl);
+  cudaFreeAsync(ell_u, s);
+  if (!ok) {
+    cudaFreeAsync(p.ell_a, s);
+    return nullptr;
+  }
+  g_jac_steps.push_back(p);
+  return &g_jac_steps.back();
+}
+
+// jac1's update `ua` (r, du, u, u_sum, u_max) followed by its res `ra`
+// (A, u through the map, du incremented through the map, beta) as one
+// launch; false when the shapes do not suit it (the caller runs both)
+bool run_jac_step(char const *uname, op_set uset, const op_arg *ua, char const *rname,
+                  op_set rset, const op_arg *ra) {
+  if (!tuning("jac_step", 1) || effective_strategy(rname) == OP2B_STRATEGY_COLOURED) return false;
+  op_dat r = ua[0].dat, du = ua[1].dat, u = ua[2].dat;
+  if (ra[1].dat != u || ra[2].dat != du || ra[0].dat == u || ra[0].dat == du ||
+      r == u || r == du || !ra[1].map || !ra[2].map || ra[0].map)
+    return false;
+  cudaStream_t s = rt().stream;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  OP2B_CUDA(cudaStreamIsCapturing(s, &cap));
+  const bool capturing = cap != cudaStreamCaptureStatusNone;
+  if (!capturing && live_graphs() > 0) return false;  // graphs hold the buffers they captured
+  GatherPlan *g = get_gather_plan(rset, ra, {2});
+  if (!g || g->nactive != uset->size || g->d_active || uset != du->set) return false;
+  int2 *pairs = jac_pairs(g, ra, s);
+  if (!pairs) return false;
+  const int n = uset->size;
+  const int ct = std::max(64, tuning("jac_tile_nodes", 1024));
+  JacStep *p = nullptr;
+  for (auto &q : g_jac_steps)
+    if (q.g == g && q.mA == ra[0].map && q.mu == ra[1].map && q.iA == ra[0].idx &&
+        q.iu == ra[1].idx && q.ct == ct)
+      p = &q;
+  if (!p) {
+    if (capturing) return false;  // plans are built before a capture
+    p = jac_step_plan(g, ra, pairs, ct, s);
+    if (!p) return false;
+  }
+  const size_t smem = sizeof(float) * (size_t)std::max(1, p->tl.maxcnt);
+  if (smem > (size_t)rt().smem_optin - 1024) return false;
+  float alpha = 0.f;
+  if (const_get_f32("alpha", &alpha, 1) < 1) return false;
+  const float beta = *(const float *)ra[3].data;
+  float *u_out = (float *)alt_of(u), *du_out = (float *)alt_of(du);
+  if (!u_out || !du_out || error_pending()) return false;
+  // threads per CTA (knob jac_step_threads: 512, 1024 or 256)
+  const int BS = tuning("jac_step_threads", 512) == 1024 ? 1024
+                 : tuning("jac_step_threads", 512) == 256 ? 256 : 512;
+  auto kern = BS == 1024 ? k_jac_step<1024> : BS == 256 ? k_jac_step<256> : k_jac_step<512>;
+  static size_t sized[3] = {0, 0, 0};
+  size_t &have = sized[BS == 1024 ? 2 : BS == 256 ? 0 : 1];
+  if (smem > 48 * 1024 && smem > have) {
+    OP2B_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    have = smem;
+  }
+  const bool seq = rt().reduction == OP2B_REDUCE_SEQ;
+  int slot_sum = red_new_slot(), slot_max = red_new_slot();
+  float *r_sum = (float *)red_slot_ptr(slot_sum), *r_max = (float *)red_slot_ptr(slot_max);
+  {
+    std::string name = std::string(uname) + "+" + rname;
+    LoopScope ls(name.c_str(),
+                 compulsory_bytes(uset, 5, ua) + compulsory_bytes(rset, 4, ra), 0);
+    float *seqbuf = seq ? (float *)red_seq_buffer(sizeof(float) * (size_t)n) : nullptr;
+    const int grid = std::min(p->tl.ntile, kMaxRedBlocks);
+    RedSlot<float> ss{(float *)red_partials(0), r_sum}, sm{(float *)red_partials(1), r_max};
+    launch_pdl(kern, grid, BS, smem, s, n, p->tl.ntile, p->tl.ct, p->W,
+               (const int *)p->tl.toff, (const int *)p->tl.tflux, (const int *)p->tl.tell,
+               (const int *)p->ell_a, (const float *)ra[0].dat->data_d,
+               (const float *)r->data_d, (const float *)du->data_d, (const float *)u->data_d,
+               alpha, beta, u_out, du_out, seqbuf, ss, sm, red_ticket());
+    if (seq)
+      k_seq_sum<float><<<1, 32, 0, s>>>(seqbuf, n, *(const float *)ua[3].data, r_sum,
+                                        perm_old2new_dev(uset), 1);
+  }
+  if (error_pending()) return true;
+  flip(u, capturing);
+  flip(du, capturing);
+  red_finish({GblRequest{ua[3].data, slot_sum, OP_INC, GBL_F32, seq},
+              GblRequest{ua[4].data, slot_max, OP_MAX, GBL_F32, false}});
+  return true;
+}
+
 }  // namespace op2b

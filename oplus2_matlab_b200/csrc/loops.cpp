@@ -445,6 +445,16 @@ bool extend_chain(Kind k, char const *name, op_set set, int nargs, const op_arg 
   const Held &h0 = g_chain[0];
   const op_arg *pa = h0.args.data();
   const size_t n = g_chain.size();
+  if (n == 1 && h0.kind == K_JUPDATE && k == K_JRES && nargs == 4) {
+    // jac1: the held update, then this res, as one launch
+    std::vector<Held> ch;
+    std::swap(ch, g_chain);
+    if (jac_res_variant(nargs, a) == 1 &&
+        run_jac_step(ch[0].name.c_str(), ch[0].set, ch[0].args.data(), name, set, a))
+      return true;
+    run_chain(ch, nullptr);  // the update alone; the caller runs the res
+    return false;
+  }
   if (n == 1 && h0.kind == K_SAVE && k == K_ADT && set == h0.set) {
     // save_soln(q -> qold), adt_calc(x, q' -> adt)
     op_dat q = pa[0].dat, qold = pa[1].dat;
@@ -499,9 +509,12 @@ bool extend_chain(Kind k, char const *name, op_set set, int nargs, const op_arg 
 }
 
 // loops that may start a chain
-bool holdable(Kind k) {
+bool holdable(Kind k, int variant = 0) {
   if (!tuning("fuse", 1)) return false;
   if (k == K_SAVE) return true;
+  // jac1's update waits for the next res (one launch for both) when its
+  // reductions need not reach the host before its call returns
+  if (k == K_JUPDATE) return variant == 1 && rt().gbl_deferred && tuning("jac_step", 1);
   if (k == K_RES) return res_holdable();
   if (k == K_AUPDATE) return update_holdable();
   return false;
@@ -689,7 +702,7 @@ void par_loop_run(char const *name, op_set set, int nargs, const op_arg *args) {
     if (extend_chain(k, name, set, nargs, args)) return;
     flush_pending();
   }
-  if (holdable(k)) {
+  if (holdable(k, v)) {
     g_chain.push_back(make_held(k, name, set, nargs, args));
     if (k == K_RES) g_chain.back().flux_done = res_flux_done;
     return;

@@ -71,6 +71,10 @@ void run_jac_update(char const *name, op_set set, const op_arg *args, int varian
                     std::vector<GblRequest> *held = nullptr);
 // jac1's res into du_out (a spare buffer of du's size) instead of du, ahead
 // of its call; false when not applicable (nothing launched)
+// jac1's update followed by its res as one launch (jac.cu); false when the
+// shapes do not suit it
+bool run_jac_step(char const *uname, op_set uset, const op_arg *ua, char const *rname,
+                  op_set rset, const op_arg *ra);
 bool run_jac_res_ahead(char const *name, op_set set, const op_arg *args, int variant,
                        void *du_out);
 // whether run_jac_res_ahead would launch for these arguments (GATHER, jac1,
