@@ -514,7 +514,16 @@ bool run_jac_step(char const *uname, op_set uset, const op_arg *ua, char const *
   int2 *pairs = jac_pairs(g, ra, s);
   if (!pairs) return false;
   const int n = uset->size;
-  const int ct = std::max(64, tuning("jac_tile_nodes", 1024));
+  // threads per CTA (knob jac_step_threads: 512, 1024 or 256) and nodes per
+  // tile (knob jac_tile_nodes; 0: one tile per resident CTA -- two CTAs of
+  // 512 per SM at the kernel's 63 registers -- so that every SM gets the
+  // same share)
+  const int BS = tuning("jac_step_threads", 512) == 1024 ? 1024
+                 : tuning("jac_step_threads", 512) == 256 ? 256 : 512;
+  const long long slots = (long long)rt().num_sms * std::max(1, 1024 / BS);
+  const int ct = tuning("jac_tile_nodes", 0) > 0
+                     ? std::max(64, tuning("jac_tile_nodes", 0))
+                     : (int)std::max(64LL, (n + slots - 1) / slots);
   JacStep *p = nullptr;
   for (auto &q : g_jac_steps)
     if (q.g == g && q.mA == ra[0].map && q.mu == ra[1].map && q.iA == ra[0].idx &&
@@ -532,9 +541,6 @@ bool run_jac_step(char const *uname, op_set uset, const op_arg *ua, char const *
   const float beta = *(const float *)ra[3].data;
   float *u_out = (float *)alt_of(u), *du_out = (float *)alt_of(du);
   if (!u_out || !du_out || error_pending()) return false;
-  // threads per CTA (knob jac_step_threads: 512, 1024 or 256)
-  const int BS = tuning("jac_step_threads", 512) == 1024 ? 1024
-                 : tuning("jac_step_threads", 512) == 256 ? 256 : 512;
   auto kern = BS == 1024 ? k_jac_step<1024> : BS == 256 ? k_jac_step<256> : k_jac_step<512>;
   static size_t sized[3] = {0, 0, 0};
   size_t &have = sized[BS == 1024 ? 2 : BS == 256 ? 0 : 1];

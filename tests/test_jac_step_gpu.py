@@ -50,7 +50,7 @@ def test_deferred_jac1_step_matches_reference(op2, knobs):
     finally:
         api.set_gbl_deferred(0)
         for k in knobs:
-            lib.op2b_set_tuning(k.encode(), {"jac_tile_nodes": 1024, "jac_step_threads": 512}[k])
+            lib.op2b_set_tuning(k.encode(), {"jac_tile_nodes": 0, "jac_step_threads": 512}[k])
     assert op2.last_error() == ""
     assert sha(u) == g["u_sha256"]
     gm, grms = g["u_max_rms"][-1]
@@ -93,7 +93,7 @@ def test_jac1_step_graph_is_one_launch(op2):
 
 
 def test_jac1_step_larger_grid_tree(op2):
-    """NN=256 (tiles of 1024 nodes, four rows each): u bit-identical to the
+    """NN=256 (tiles of a few rows): u bit-identical to the
     two-launch form; the TREE sum within summation order."""
     jm = M.jac(256, 1)
     op2.set_strategy(op2.STRATEGY_GATHER)
