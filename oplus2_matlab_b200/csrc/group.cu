@@ -1246,8 +1246,6 @@ struct Group : GroupBase {
       return ms;
     };
     // edge tiles (one block, one stream), then blocks x streams at the best tile
-    const size_t bb0 = block_bytes;
-    const int ns0 = nstreams;
     for (int k = 0; k < 5; k++) {
       etile = trials[k].etile;
       block_bytes = ~(size_t)0;
@@ -1277,8 +1275,6 @@ struct Group : GroupBase {
         best_blk = {trials[k].block_bytes, trials[k].nstreams};
       }
     }
-    (void)bb0;
-    (void)ns0;
     block_bytes = best_blk.first;
     nstreams = best_blk.second;
     if (exec) {
