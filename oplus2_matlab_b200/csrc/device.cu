@@ -12,12 +12,7 @@
 #include <stdlib.h>
 #include <string.h>
 
-#include <algorithm>
-#include <condition_variable>
-#include <mutex>
-#include <thread>
 #include <unordered_set>
-#include <vector>
 
 #include "internal.h"
 
@@ -161,121 +156,6 @@ void dev_free(void *p) {
   cudaFree(p);
 }
 
-// Host -> device copies of the caller's arrays.  From pinned memory the copy
-// engine reads the array itself.  A pageable array of 256 KB or more would be
-// staged by the driver through its own buffer at a few GB/s with the host
-// waiting; instead it is copied here, 8 MB at a time, by several host
-// threads into one of two pinned stages while the previous stage's DMA
-// runs, and the caller's array is free again when staged_upload returns
-// (the last DMA may still be running; the library stream orders it before
-// any use of dst).
-namespace {
-// host threads copying slices of one buffer: started on first use, kept
-// (and left running) for the life of the process
-class CopyPool {
- public:
-  CopyPool() {
-    const unsigned hw = std::thread::hardware_concurrency();
-    const int k = (int)std::min(8u, std::max(1u, hw / 2));
-    for (int i = 0; i < k - 1; i++) workers_.emplace_back([this] { loop(); });
-  }
-  void copy(void *dst, const void *src, size_t n) {
-    if (workers_.empty() || n < (2u << 20)) {
-      memcpy(dst, src, n);
-      return;
-    }
-    {
-      std::lock_guard<std::mutex> g(m_);
-      dst_ = (char *)dst;
-      src_ = (const char *)src;
-      n_ = n;
-      slice_ = std::max<size_t>(1u << 20, (n + workers_.size()) / (workers_.size() + 1));
-      nslices_ = (int)((n + slice_ - 1) / slice_);
-      next_ = 0;
-      left_ = nslices_;
-      gen_++;
-    }
-    cv_.notify_all();
-    run_slices();
-    std::unique_lock<std::mutex> lk(m_);
-    done_.wait(lk, [this] { return left_ == 0; });
-  }
-
- private:
-  void run_slices() {
-    for (;;) {
-      int i;
-      {
-        std::lock_guard<std::mutex> g(m_);
-        if (next_ >= nslices_) return;
-        i = next_++;
-      }
-      const size_t a = (size_t)i * slice_, b = std::min(n_, a + slice_);
-      memcpy(dst_ + a, src_ + a, b - a);
-      std::lock_guard<std::mutex> g(m_);
-      if (--left_ == 0) done_.notify_all();
-    }
-  }
-  void loop() {
-    unsigned long long seen = 0;
-    for (;;) {
-      {
-        std::unique_lock<std::mutex> lk(m_);
-        cv_.wait(lk, [&] { return gen_ != seen; });
-        seen = gen_;
-      }
-      run_slices();
-    }
-  }
-  std::vector<std::thread> workers_;
-  std::mutex m_;
-  std::condition_variable cv_, done_;
-  char *dst_ = nullptr;
-  const char *src_ = nullptr;
-  size_t n_ = 0, slice_ = 0;
-  int nslices_ = 0, next_ = 0, left_ = 0;
-  unsigned long long gen_ = 0;
-};
-
-CopyPool &copy_pool() {
-  static CopyPool *p = new CopyPool();  // never destroyed: its threads wait for work
-  return *p;
-}
-
-constexpr size_t kStageBytes = 8u << 20;
-char *g_stage[2] = {nullptr, nullptr};
-cudaEvent_t g_stage_done[2] = {nullptr, nullptr};
-
-// true when it took the copy (pageable src of 256 KB or more)
-bool staged_upload(void *dst, const void *src, size_t bytes, cudaStream_t s) {
-  if (bytes < (256u << 10)) return false;
-  cudaPointerAttributes pa;
-  if (cudaPointerGetAttributes(&pa, src) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  if (pa.type != cudaMemoryTypeUnregistered) return false;
-  if (!g_stage[0]) {
-    for (int b = 0; b < 2; b++) {
-      if (cudaMallocHost((void **)&g_stage[b], kStageBytes) != cudaSuccess ||
-          cudaEventCreateWithFlags(&g_stage_done[b], cudaEventDisableTiming) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-      }
-    }
-  }
-  int b = 0;
-  for (size_t off = 0; off < bytes; off += kStageBytes, b ^= 1) {
-    const size_t n = std::min(kStageBytes, bytes - off);
-    OP2B_CUDA(cudaEventSynchronize(g_stage_done[b]));  // its previous DMA is done
-    copy_pool().copy(g_stage[b], (const char *)src + off, n);
-    OP2B_CUDA(cudaMemcpyAsync((char *)dst + off, g_stage[b], n, cudaMemcpyHostToDevice, s));
-    OP2B_CUDA(cudaEventRecord(g_stage_done[b], s));
-  }
-  return true;
-}
-}  // namespace
-
 const int *map_dev(op_map m) {
   Runtime &R = rt();
   if (!m) return nullptr;
@@ -286,9 +166,8 @@ const int *map_dev(op_map m) {
     size_t bytes = sizeof(int) * (size_t)m->dim * m->from->size;
     md.d = (int *)dev_alloc(bytes);
     if (md.d) {
-      if (!staged_upload(md.d, m->map, bytes, R.stream))
-        OP2B_CUDA(cudaMemcpyAsync(md.d, (const int *)m->map, bytes, cudaMemcpyHostToDevice,
-                                  R.stream));
+      OP2B_CUDA(cudaMemcpyAsync(md.d, (const int *)m->map, bytes, cudaMemcpyHostToDevice,
+                                R.stream));
       OP2B_CUDA(cudaStreamSynchronize(R.stream));
       // renumbered sets: rows in the from-set's new order, values in the
       // to-set's new numbering, rewritten on the device
@@ -451,8 +330,8 @@ void op_init(int argc, char **argv, int diags) {
   printf("\n Using CUDA device: %s\n", rt().device_name.c_str());
 }
 
-// common/op_lib.cu:145-153: registry entry + device copy (the caller may
-// reuse its array on return: a copy from it has finished, or it was staged)
+// common/op_lib.cu:145-153: registry entry + device copy (synchronous, so
+// the caller may reuse its array on return)
 op_dat op_decl_dat_char(op_set set, int dim, char const *type, int size, char *data,
                         char const *name) {
   op_dat dat = op_decl_dat_core(set, dim, type, size, data, name);
@@ -464,14 +343,9 @@ op_dat op_decl_dat_char(op_set set, int dim, char const *type, int size, char *d
   R.dats[dat->index].bytes = bytes;
   dat->data_d = (char *)dev_alloc(bytes);
   if (!dat->data_d) return dat;
-  if (!data) {
-    OP2B_CUDA(cudaMemsetAsync(dat->data_d, 0, bytes, R.stream));
-  } else if (!staged_upload(dat->data_d, data, bytes, R.stream)) {
-    // pinned (or small) arrays: the copy reads the caller's array, so wait
-    // for it before the caller may reuse the array
-    OP2B_CUDA(cudaMemcpyAsync(dat->data_d, data, bytes, cudaMemcpyHostToDevice, R.stream));
-    OP2B_CUDA(cudaStreamSynchronize(R.stream));
-  }
+  if (data) OP2B_CUDA(cudaMemcpyAsync(dat->data_d, data, bytes, cudaMemcpyHostToDevice, R.stream));
+  else OP2B_CUDA(cudaMemsetAsync(dat->data_d, 0, bytes, R.stream));
+  OP2B_CUDA(cudaStreamSynchronize(R.stream));
   permute_dat_in_place(dat);  // when its set has been renumbered
   return dat;
 }
