@@ -54,6 +54,10 @@ enum { OP2B_REDUCE_TREE = 0, OP2B_REDUCE_SEQ = 1 };
  *                   computes its tile's fluxes into shared memory and
  *                   updates the tile's cells ("tile_threads" 1024 or 512
  *                   per CTA, "tile_cells" the tile size, 0 automatic)
+ *   "jac_step"      1 (default): with reductions deferred, jac1's update and
+ *                   the res that follows it as one launch ("jac_tile_nodes"
+ *                   the tile size, 0 automatic; "jac_step_threads" 512,
+ *                   1024 or 256 per CTA); 0: two launches
  * Every setting leaves the fields bit-identical. */
 int op2b_set_tuning(const char *key, int value);
 /* The value of a tuning knob, or `def` when it is unset. */
