@@ -53,3 +53,41 @@ def test_jac_tree_reduction_close(op2):
         # u bit-identical; u_sum differs only by the summation order of
         # op_seq.h's one-at-a-time float sum of 16,129 squares
         assert abs(us - os_) <= 1e-4 * os_
+
+
+def test_jac1_c_app_matches_reference(op2):
+    """The C++ jac1 main over the C API (apps/jac_app.cpp, the end-to-end
+    path of the bench) reproduces the reference: u bit-identical, and with
+    REDUCE_SEQ every u_max and rms of the history."""
+    import ctypes as C
+    import os
+    g = load_golden("jac1_nn64")
+    jm = M.jac(g["NN"], 1)
+    op2.set_strategy(op2.STRATEGY_GATHER)
+    op2.set_reduction(op2.REDUCE_SEQ)
+    op2.op_exit()  # the app opens its own session
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    app = C.CDLL(os.path.join(root, "oplus2_matlab_b200", "lib", "libop2b200_apps.so"))
+
+    class Timing(C.Structure):
+        _fields_ = [("t_declare", C.c_double), ("t_iterate", C.c_double),
+                    ("t_fetch", C.c_double), ("t_total", C.c_double),
+                    ("h2d_bytes", C.c_longlong), ("d2h_bytes", C.c_longlong)]
+    app.op2b_jac1_app.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.POINTER(Timing)]
+    pp = np.ascontiguousarray(jm.pp, np.int32)
+    A = np.ascontiguousarray(jm.A.reshape(-1), np.float32)
+    r = np.ascontiguousarray(jm.r.reshape(-1), np.float32)
+    u = np.zeros(jm.nnode, np.float32)
+    n = g["niter"]
+    umax, urms = np.zeros(n), np.zeros(n)
+    t = Timing()
+    rc = app.op2b_jac1_app(jm.nnode, jm.nedge, pp.ctypes.data, A.ctypes.data, r.ctypes.data, n,
+                           u.ctypes.data, umax.ctypes.data, urms.ctypes.data, C.byref(t))
+    op2.op_init([], 0)  # for the fixture's op_exit
+    assert rc == 0
+    assert sha(u) == g["u_sha256"]
+    for k, (gm, grms) in enumerate(g["u_max_rms"]):
+        assert np.float32(umax[k]) == np.float32(gm)
+        assert np.float32(urms[k]) == np.float32(grms)

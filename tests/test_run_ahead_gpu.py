@@ -109,11 +109,11 @@ JAC_SEQUENCES = {
 }
 
 
-def run_jac(op2, seq, ahead, variant):
+def run_jac(op2, seq, ahead, variant, reduction=None):
     lib = _lib.load()
     lib.op2b_set_tuning(b"run_ahead", 1 if ahead else 0)
     op2.set_strategy(op2.STRATEGY_GATHER)
-    op2.set_reduction(op2.REDUCE_TREE)
+    op2.set_reduction(op2.REDUCE_TREE if reduction is None else reduction)
     J = apps.Jac(M.jac(40, variant), variant)
     out, snaps = [], []
 
@@ -146,11 +146,17 @@ def run_jac(op2, seq, ahead, variant):
 
 @pytest.mark.parametrize("variant", [1, 2])
 @pytest.mark.parametrize("seq", sorted(JAC_SEQUENCES))
-def test_jac_same_results_with_and_without_run_ahead(op2, seq, variant):
-    a_out, a_snaps = run_jac(op2, JAC_SEQUENCES[seq], True, variant)
+@pytest.mark.parametrize("reduction", ["tree", "seq"])
+def test_jac_same_results_with_and_without_run_ahead(op2, seq, variant, reduction):
+    """u and du bit-identical at every snapshot, u_max and u_sum exact, in
+    TREE and in SEQ mode."""
+    red = op2.REDUCE_TREE if reduction == "tree" else op2.REDUCE_SEQ
+    a_out, a_snaps = run_jac(op2, JAC_SEQUENCES[seq], True, variant, red)
     api.op_exit()
     api.op_init([], 0)
-    b_out, b_snaps = run_jac(op2, JAC_SEQUENCES[seq], False, variant)
-    assert a_out == b_out
+    b_out, b_snaps = run_jac(op2, JAC_SEQUENCES[seq], False, variant, red)
+    assert len(a_out) == len(b_out)
+    for (sa, ma), (sb, mb) in zip(a_out, b_out):
+        assert ma == mb and sa == sb
     for (ua, dua), (ub, dub) in zip(a_snaps, b_snaps):
         assert np.array_equal(ua, ub) and np.array_equal(dua, dub)
