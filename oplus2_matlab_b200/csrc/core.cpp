@@ -194,12 +194,16 @@ op_map op_decl_map(op_set from, op_set to, int dim, int *imap, char const *name)
   // bad entry for the message
   const size_t nent = (size_t)dim * from->size;
   const unsigned lim = (unsigned)to->size;
+  // the device copy (when the GPU is up) is queued first and runs during
+  // the check
+  void *dcopy = map_upload_begin(imap, sizeof(int) * nent);
   unsigned bad = range_check(imap, nent, lim);
   if (bad)
     for (int d = 0; d < dim; d++)
       for (int n = 0; n < from->size; n++) {
         int v = imap[d + (size_t)n * dim];
         if (v < 0 || v >= to->size) {
+          map_upload_abort(dcopy);
           fail(-1,
                "op_decl_map error -- invalid data for map %s\n"
                "element = %d, dimension = %d, map = %d\n",
@@ -208,6 +212,7 @@ op_map op_decl_map(op_set from, op_set to, int dim, int *imap, char const *name)
         }
       }
   if (!grow(&OP_map_list, OP_map_index, &OP_map_max)) {
+    map_upload_abort(dcopy);
     fail(-1, " op_decl_map error -- error reallocating memory\n");
     return nullptr;
   }
@@ -219,8 +224,10 @@ op_map op_decl_map(op_set from, op_set to, int dim, int *imap, char const *name)
   map->map = imap;
   map->name = name;
   OP_map_list[OP_map_index++] = map;
-  // the device copy is made on first use by a loop (map_dev), so declaring
-  // maps needs no GPU, as in the reference
+  // without a GPU (or with renumbering on) the device copy is made on first
+  // use by a loop (map_dev), so declaring maps needs no GPU, as in the
+  // reference
+  map_upload_attach(map, dcopy);
   return map;
 }
 

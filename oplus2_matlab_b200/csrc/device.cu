@@ -156,6 +156,46 @@ void dev_free(void *p) {
   cudaFree(p);
 }
 
+// A map's device copy started at its declaration, so the copy runs while
+// the host checks the map's entries and declares the rest: the upload is
+// queued on the library stream (pool memory, no host wait), and a loop's
+// first use of the map finds it there.  Not while renumbering is on (the
+// copy would be rewritten anyway) or before CUDA is up.
+void *map_upload_begin(const int *imap, size_t bytes) {
+  Runtime &R = rt();
+  if (!R.cuda_ready || renumber_enabled() || error_pending() || !imap || bytes == 0)
+    return nullptr;
+  if (stream_capturing()) return nullptr;
+  void *d = nullptr;
+  if (pool_malloc_async(&d, bytes, R.stream) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  if (cudaMemcpyAsync(d, imap, bytes, cudaMemcpyHostToDevice, R.stream) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFreeAsync(d, R.stream);
+    return nullptr;
+  }
+  return d;
+}
+
+void map_upload_attach(op_map m, void *d) {
+  if (!d) return;
+  Runtime &R = rt();
+  if (R.maps.size() <= (size_t)m->index) R.maps.resize(m->index + 1);
+  MapDev &md = R.maps[m->index];
+  if (md.d) {  // cannot happen for a new map; keep the existing copy
+    cudaFreeAsync(d, R.stream);
+    return;
+  }
+  md.d = (int *)d;
+  g_pooled.insert(d);  // freed with dev_free like the other pool buffers
+}
+
+void map_upload_abort(void *d) {
+  if (d) cudaFreeAsync(d, rt().stream);
+}
+
 const int *map_dev(op_map m) {
   Runtime &R = rt();
   if (!m) return nullptr;

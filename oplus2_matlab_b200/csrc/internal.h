@@ -135,6 +135,12 @@ void *dev_alloc(size_t bytes);
 void dev_free(void *p);
 // stream-ordered scratch from the library's pool; free with cudaFreeAsync
 cudaError_t pool_malloc_async(void **p, size_t bytes, cudaStream_t s);
+// a map's device copy queued at its declaration (nullptr: none, the first
+// loop that uses the map makes it), handed to the map once it is valid,
+// or dropped when the declaration fails
+void *map_upload_begin(const int *imap, size_t bytes);
+void map_upload_attach(op_map m, void *d);
+void map_upload_abort(void *d);
 void ensure_cuda();  // op_init's device part, also run lazily
 
 // timing around one loop call
