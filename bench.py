@@ -875,16 +875,22 @@ def measure_batched(args, dist, instances, n):
     t_tune = time.perf_counter() - tt
     tile = g.lib.op2b_group_edge_tile(g.h)
     ti = time.perf_counter()
+    # each solve's q is copied out as soon as it has stopped, while the
+    # others iterate
     stopped = 0
+    q_of = dict(zip(ids, mine))
     while stopped < len(ids):
         g.run(50)
         graph_launches += 50
-        stopped += len(g.poll())
+        done = g.poll()
+        stopped += len(done)
+        for sid in done:
+            g.fetch_q_async(sid, qbuf[q_of[sid]])
     g.sync()
     t_iter = time.perf_counter() - ti
     tf = time.perf_counter()
     hist = [g.history(s) for s in ids]
-    qg = [g.fetch_q(s, out=qbuf[i]) for s, i in zip(ids, mine)]
+    qg = [qbuf[i] for i in mine]
     t_fetch = time.perf_counter() - tf
     t_group = dist.max(time.perf_counter() - t0)
     gbytes = g.device_bytes()

@@ -71,6 +71,10 @@ int op2b_group_sync(op2b_group g);
 int op2b_group_iterations(op2b_group g, int id);
 int op2b_group_history(op2b_group g, int id, double *rms, int max); /* returns count */
 int op2b_group_fetch_q(op2b_group g, int id, void *q);              /* ncell*4 reals */
+/* The same for a solve op2b_group_poll has reported stopped, queued while
+ * the other solves iterate (into pinned memory for an overlapped copy): q is
+ * valid after op2b_group_sync.  Any other solve: as op2b_group_fetch_q. */
+int op2b_group_fetch_q_async(op2b_group g, int id, void *q);
 
 /* Release a solve's device memory; it leaves the group. */
 int op2b_group_remove(op2b_group g, int id);

@@ -218,6 +218,7 @@ PROTOTYPES = [
     ("op2b_group_iterations", C.c_int, [_P, C.c_int]),
     ("op2b_group_history", C.c_int, [_P, C.c_int, C.POINTER(C.c_double), C.c_int]),
     ("op2b_group_fetch_q", C.c_int, [_P, C.c_int, _P]),
+    ("op2b_group_fetch_q_async", C.c_int, [_P, C.c_int, _P]),
     ("op2b_group_remove", C.c_int, [_P, C.c_int]),
     ("op2b_group_solve_bytes", C.c_longlong, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
     ("op2b_group_device_bytes", C.c_longlong, [_P]),

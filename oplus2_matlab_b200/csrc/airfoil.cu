@@ -2055,6 +2055,26 @@ __global__ void k_tile_place(const unsigned long long *__restrict__ key,
   }
 }
 
+// toff[0..ntile] = the number of distinct keys (pos and flag of the last key)
+__global__ void k_tile_total(const int *__restrict__ flag, const int *__restrict__ pos, int n,
+                             int ntile, int *toff) {
+  const int total = pos[n - 1] + flag[n - 1];
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t <= ntile; t += gridDim.x * blockDim.x)
+    toff[t] = total;
+}
+
+// *out = the longest tile run (one CTA)
+__global__ void k_tile_longest(const int *__restrict__ toff, int ntile, int *out) {
+  __shared__ int best;
+  if (threadIdx.x == 0) best = 0;
+  __syncthreads();
+  int m = 0;
+  for (int t = threadIdx.x; t < ntile; t += blockDim.x) m = max(m, toff[t + 1] - toff[t]);
+  atomicMax(&best, m);
+  __syncthreads();
+  if (threadIdx.x == 0) *out = best;
+}
+
 // each list entry as its slot in the tile's flux run (binary search)
 __global__ void k_tile_lists(const int *__restrict__ ell, int W, int ncell, int ct,
                              const int *__restrict__ toff, const int *__restrict__ tflux,
@@ -2137,8 +2157,68 @@ bool build_tile_lists(const int *ell, int ncell, int W, int ct, cudaStream_t s, 
   return false;
 }
 
+// The same lists queued on stream s with no host wait: the flux runs get
+// room for every list entry, and the longest run is left in tl->d_longest
+// (read it with tile_lists_longest once s has run them).  False when the
+// memory cannot be had.
+bool build_tile_lists_async(const int *ell, int ncell, int W, int ct, cudaStream_t s,
+                            TileLists *out) {
+  *out = TileLists();
+  const long long n = (long long)ncell * W;
+  if (ncell < 1 || W < 1 || ct < 1 || n >= (1LL << 30)) return false;
+  const int ntile = (ncell + ct - 1) / ct;
+  long long m = 1;
+  while (m < n) m <<= 1;
+  unsigned long long *key = nullptr;
+  int *flag = nullptr, *pos = nullptr;
+  TileLists tl;
+  tl.ct = ct;
+  tl.ntile = ntile;
+  tl.maxcnt = -1;  // in d_longest
+  bool ok = pool_malloc_async((void **)&key, sizeof(unsigned long long) * m, s) == cudaSuccess &&
+            pool_malloc_async((void **)&flag, sizeof(int) * n, s) == cudaSuccess &&
+            pool_malloc_async((void **)&pos, sizeof(int) * n, s) == cudaSuccess &&
+            pool_malloc_async((void **)&tl.toff, sizeof(int) * (ntile + 1), s) == cudaSuccess &&
+            pool_malloc_async((void **)&tl.tell, sizeof(int) * n, s) == cudaSuccess &&
+            pool_malloc_async((void **)&tl.tflux, sizeof(int) * n, s) == cudaSuccess &&
+            pool_malloc_async((void **)&tl.d_longest, sizeof(int), s) == cudaSuccess;
+  if (!ok) cudaGetLastError();
+  const int g = rt().num_sms * 8;
+  if (ok) {
+    k_tile_keys<<<g, 256, 0, s>>>(ell, W, ncell, ct, m, key);
+    ok = sort_keys_u64(key, m, s);
+  }
+  if (ok) {
+    k_tile_first<<<g, 256, 0, s>>>(key, (int)n, flag);
+    exclusive_scan_nosync(flag, pos, (int)n, s);
+    k_tile_total<<<std::max(1, (ntile + 256) / 256), 256, 0, s>>>(flag, pos, (int)n, ntile, tl.toff);
+    k_tile_place<<<g, 256, 0, s>>>(key, flag, pos, (int)n, tl.tflux, tl.toff);
+    k_tile_lists<<<g, 256, 0, s>>>(ell, W, ncell, ct, tl.toff, tl.tflux, tl.tell);
+    k_tile_longest<<<1, 1024, 0, s>>>(tl.toff, ntile, tl.d_longest);
+  }
+  for (void *p : {(void *)key, (void *)flag, (void *)pos})
+    if (p) cudaFreeAsync(p, s);
+  if (ok && !error_pending()) {
+    *out = tl;
+    return true;
+  }
+  free_tile_lists(&tl, s);
+  return false;
+}
+
+// the longest run of lists built by build_tile_lists_async (waits for s)
+int tile_lists_longest(TileLists *tl, cudaStream_t s) {
+  if (tl->maxcnt < 0 && tl->d_longest) {
+    int v = 0;
+    OP2B_CUDA(cudaMemcpyAsync(&v, tl->d_longest, sizeof(int), cudaMemcpyDeviceToHost, s));
+    OP2B_CUDA(cudaStreamSynchronize(s));
+    tl->maxcnt = v;
+  }
+  return tl->maxcnt;
+}
+
 void free_tile_lists(TileLists *tl, cudaStream_t s) {
-  for (void *p : {(void *)tl->toff, (void *)tl->tflux, (void *)tl->tell})
+  for (void *p : {(void *)tl->toff, (void *)tl->tflux, (void *)tl->tell, (void *)tl->d_longest})
     if (p) cudaFreeAsync(p, s);
   *tl = TileLists();
 }

@@ -458,6 +458,7 @@ struct GroupBase {
   virtual int iterations(int id) = 0;
   virtual int history(int id, double *out, int max) = 0;
   virtual int fetch_q(int id, void *q) = 0;
+  virtual int fetch_q_async(int id, void *q) = 0;
   virtual int remove(int id) = 0;
   virtual long long solve_bytes(int nn, int nc, int ne, int nb, int max_iter) = 0;
   virtual long long device_bytes() = 0;
@@ -487,6 +488,8 @@ struct Group : GroupBase {
     bool primed = false;
     long long join_epoch = 0;  // the first state mirror that includes this solve
     SolveDev<T> dev;
+    cudaEvent_t fetched = nullptr;  // after an asynchronous copy of q out
+    cudaStream_t tl_stream = nullptr;  // where the tile lists were queued
     // the tiled chain's second buffers of q and adt, and tile lists
     void *tbuf = nullptr;
     TileLists tl;
@@ -516,6 +519,7 @@ struct Group : GroupBase {
   // the tiled chain (op2b_group_set_tiled): one launch per update, each CTA
   // one tile of one solve, its flux values in shared memory
   bool tiled = false;
+  long long graph_cells = 0, stopped_cells = 0;  // cells in the captured iteration; stopped since
   Tile *d_tt = nullptr;
   size_t tt_cap = 0;
   int ntt = 0;
@@ -563,6 +567,11 @@ struct Group : GroupBase {
 
   void release(Solve &s) {
     if (s.removed) return;
+    if (s.fetched) {  // an asynchronous copy of q out reads the solve's memory
+      OP2B_CUDA(cudaStreamWaitEvent(s.joined ? cs : us, s.fetched, 0));
+      cudaEventDestroy(s.fetched);
+      s.fetched = nullptr;
+    }
     if (s.block) cudaFreeAsync(s.block, s.joined ? cs : us);
     if (s.ell) cudaFreeAsync(s.ell, s.joined ? cs : us);
     if (s.tbuf) cudaFreeAsync(s.tbuf, s.joined ? cs : us);
@@ -616,46 +625,64 @@ struct Group : GroupBase {
                        (tiled ? tiled_bytes(nc, ne, nb) : 0));
   }
 
-  // cells per tile of the tiled chain: the largest of 4096, 3072, 2304, ...
-  // (FP32; half that in FP64), at least the rms tile, whose longest flux run
-  // fits one CTA's shared memory
+  // The tiled chain's lists of a solve, queued on stream st with no host
+  // wait (tiles of 4096 cells in FP32, 2048 in FP64); whether the longest
+  // tile's values fit a CTA's shared memory is checked at the next rebuild
+  // (fit_tiled), which makes smaller tiles if not.
   bool ensure_tiled(Solve &s, cudaStream_t st) {
     if (s.tbuf) return true;
-    const size_t budget = (size_t)rt().smem_optin - 2048;
     void *buf = nullptr;
     if (pool_malloc_async(&buf, sizeof(T) * 5 * (size_t)s.ncell, st) != cudaSuccess) {
       cudaGetLastError();
       return false;
     }
     TileLists tl;
-    bool ok = false;
-    for (int ct = sizeof(T) == 4 ? 4096 : 2048; ct >= kCellTile; ct = ct * 3 / 4) {
-      if (!build_tile_lists(s.ell, s.ncell, s.dev.W, ct, st, &tl)) break;
-      if ((size_t)tl.maxcnt * 4 * sizeof(T) <= budget) {
-        ok = true;
-        break;
-      }
-      free_tile_lists(&tl, st);
-    }
-    if (!ok) {
+    const int ct = std::max(kCellTile, sizeof(T) == 4 ? 4096 : 2048);
+    if (!build_tile_lists_async(s.ell, s.ncell, s.dev.W, ct, st, &tl)) {
       cudaFreeAsync(buf, st);
       return false;
     }
     s.tbuf = buf;
-    s.tl = tl;
+    s.tl_stream = st;
+    set_tiled_view(s, tl);
     s.tbytes = align256(sizeof(T) * 5 * (size_t)s.ncell) +
-               align256(sizeof(int) * (size_t)s.dev.W * s.ncell) +
-               align256(sizeof(int) * (size_t)(s.nedge + s.nbedge) * 5 / 4);
+               align256(sizeof(int) * (size_t)s.dev.W * s.ncell) * 2;
     s.bytes += s.tbytes;
     SolveDev<T> &d = s.dev;
     d.q2 = (T *)buf;
     d.adt2 = (T *)buf + 4 * (size_t)s.ncell;
-    d.toff = tl.toff;
-    d.tflux = tl.tflux;
-    d.tell = tl.tell;
-    d.tct = tl.ct;
-    d.tntile = tl.ntile;
     return true;
+  }
+
+  void set_tiled_view(Solve &s, const TileLists &tl) {
+    s.tl = tl;
+    s.dev.toff = tl.toff;
+    s.dev.tflux = tl.tflux;
+    s.dev.tell = tl.tell;
+    s.dev.tct = tl.ct;
+    s.dev.tntile = tl.ntile;
+  }
+
+  // true when the solve's longest tile fits shared memory, after making
+  // smaller tiles (at least the rms tile) if it did not; the solve's view
+  // on the device is refreshed then
+  bool fit_tiled(int id) {
+    Solve &s = solves[id];
+    const size_t budget = (size_t)rt().smem_optin - 2048;
+    if ((size_t)tile_lists_longest(&s.tl, s.tl_stream) * 4 * sizeof(T) <= budget) return true;
+    for (int ct = s.tl.ct * 3 / 4; ct >= kCellTile; ct = ct * 3 / 4) {
+      TileLists tl;
+      if (!build_tile_lists(s.ell, s.ncell, s.dev.W, ct, cs, &tl)) return false;
+      if ((size_t)tl.maxcnt * 4 * sizeof(T) <= budget) {
+        free_tile_lists(&s.tl, cs);
+        set_tiled_view(s, tl);
+        OP2B_CUDA(cudaMemcpyAsync(d_sd + id, &s.dev, sizeof(SolveDev<T>), cudaMemcpyHostToDevice,
+                                  cs));
+        return true;
+      }
+      free_tile_lists(&tl, cs);
+    }
+    return false;
   }
 
   int add(const op2b_mesh *m, double mach, double alpha, int max_iter, double tol) override {
@@ -740,7 +767,7 @@ struct Group : GroupBase {
     if (tiled && !ensure_tiled(s, us)) {
       cudaFreeAsync(s.ell, us);
       cudaFreeAsync(s.block, us);
-      fail(-1, "op2b_group_add error -- no tile size fits the tiled chain's shared memory\n");
+      fail(-1, "op2b_group_add error -- out of device memory for the tiled chain\n");
       return -1;
     }
     OP2B_CUDA(cudaEventCreateWithFlags(&s.ready, cudaEventDisableTiming));
@@ -811,6 +838,7 @@ struct Group : GroupBase {
     std::vector<Tile> ct, et, pt, tt;
     blocks.clear();
     nactive = 0;
+    graph_cells = stopped_cells = 0;
     rotate = tuning("group_rotate", 1) != 0;
     size_t in_block = 0;
     tsmem = 0;
@@ -825,10 +853,16 @@ struct Group : GroupBase {
         OP2B_CUDA(cudaMemcpyAsync(d_sd + id, &s.dev, sizeof(SolveDev<T>), cudaMemcpyHostToDevice,
                                   cs));
       }
+    if (tiled)
+      for (int id = 0; id < (int)solves.size() && tiled; id++) {
+        const Solve &s = solves[id];
+        if (s.joined && !s.removed && !s.done && !fit_tiled(id)) tiled = false;
+      }
     for (int id = 0; id < (int)solves.size(); id++) {
       const Solve &s = solves[id];
       if (!s.joined || s.removed || s.done) continue;
       nactive++;
+      graph_cells += s.ncell;
       if (rotate && !s.primed)
         for (int a = 0, l = 0; a < s.ncell; a += kCellTile, l++)
           pt.push_back(Tile{id, a, std::min(kCellTile, s.ncell - a), l});
@@ -1006,8 +1040,14 @@ struct Group : GroupBase {
       Solve &s = solves[id];
       if (!s.joined || s.removed || s.reported || s.join_epoch > mirror_epoch || h_st[id].active)
         continue;
-      s.done = true;
-      changed = true;
+      if (!s.done) {
+        s.done = true;
+        // a stopped solve's CTAs return at once, so the captured iteration is
+        // rebuilt without it only when the stopped cells are a quarter of
+        // those it holds (knob group_lazy_retire 0: at every stop)
+        stopped_cells += s.ncell;
+        if (!tuning("group_lazy_retire", 1) || 4 * stopped_cells > graph_cells) changed = true;
+      }
       if (n < max && ids) {
         ids[n++] = id;
         s.reported = true;
@@ -1054,6 +1094,21 @@ struct Group : GroupBase {
     return error_pending() ? -1 : 0;
   }
 
+  // q of a solve that poll has reported stopped: its device q is final (the
+  // launches after its stop return before writing it), so the copy is
+  // queued on the admission stream while the other solves iterate; q is
+  // valid after op2b_group_sync.  Other solves: the synchronous fetch_q.
+  int fetch_q_async(int id, void *q) override {
+    Solve *s = get(id);
+    if (!s) return -1;
+    if (!s->done || !s->reported) return fetch_q(id, q);
+    OP2B_CUDA(cudaMemcpyAsync(q, s->dev.q, sizeof(T) * 4 * (size_t)s->ncell,
+                              cudaMemcpyDeviceToHost, us));
+    if (!s->fetched) OP2B_CUDA(cudaEventCreateWithFlags(&s->fetched, cudaEventDisableTiming));
+    OP2B_CUDA(cudaEventRecord(s->fetched, us));
+    return error_pending() ? -1 : 0;
+  }
+
   int remove(int id) override {
     Solve *s = get(id);
     if (!s) return -1;
@@ -1070,7 +1125,11 @@ struct Group : GroupBase {
            (long long)(ct_cap + et_cap + tt_cap) * sizeof(Tile);
   }
 
-  int active() override { return nactive; }
+  int active() override {  // joined and not stopped (stopped ones may still be in the graph)
+    int n = 0;
+    for (const auto &s : solves) n += s.joined && !s.removed && !s.done;
+    return n;
+  }
 
   int set_block_bytes(long long bytes) override {
     const size_t b = bytes <= 0 ? ~(size_t)0 : (size_t)bytes;  // <= 0: one block
@@ -1346,6 +1405,7 @@ int op2b_group_history(op2b_group g, int id, double *rms, int max) {
   GROUP_CALL(history(id, rms, max));
 }
 int op2b_group_fetch_q(op2b_group g, int id, void *q) { GROUP_CALL(fetch_q(id, q)); }
+int op2b_group_fetch_q_async(op2b_group g, int id, void *q) { GROUP_CALL(fetch_q_async(id, q)); }
 int op2b_group_remove(op2b_group g, int id) { GROUP_CALL(remove(id)); }
 long long op2b_group_solve_bytes(op2b_group g, int nnode, int ncell, int nedge, int nbedge,
                                  int max_iter) {

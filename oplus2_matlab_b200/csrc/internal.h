@@ -188,10 +188,14 @@ void release_tile_alts();   // op_exit: free the tiled chain's second buffers
 // cells, each tile's distinct list indices ascending (tflux, tile t's run at
 // toff[t]) and each list entry as (slot in its tile's run << 1 | side)
 struct TileLists {
-  int ct = 0, ntile = 0, maxcnt = 0;  // cells per tile, tiles, the longest run
+  int ct = 0, ntile = 0, maxcnt = 0;  // cells per tile, tiles, the longest run (-1: on the device)
   int *toff = nullptr, *tflux = nullptr, *tell = nullptr;
+  int *d_longest = nullptr;  // the longest run, when built asynchronously
 };
 bool build_tile_lists(const int *ell, int ncell, int W, int ct, cudaStream_t s, TileLists *out);
+bool build_tile_lists_async(const int *ell, int ncell, int W, int ct, cudaStream_t s,
+                            TileLists *out);
+int tile_lists_longest(TileLists *tl, cudaStream_t s);
 void free_tile_lists(TileLists *tl, cudaStream_t s);
 // sorts the m 64-bit keys at a (m a power of two) ascending on stream s
 bool sort_keys_u64(unsigned long long *a, long long m, cudaStream_t s);

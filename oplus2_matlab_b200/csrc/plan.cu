@@ -474,6 +474,20 @@ __global__ void k_scan_add(int *out, int n, const int *offs, int chunk) {
   }
 }
 
+void exclusive_scan_nosync(const int *d_in, int *d_out, int n, cudaStream_t s) {
+  const int chunk = 8192;
+  const int nch = (n + chunk - 1) / chunk;
+  if (n <= 0) return;
+  int *sums = nullptr;
+  OP2B_CUDA(pool_malloc_async((void **)&sums, sizeof(int) * (nch + 1), s));
+  k_scan_chunks<<<nch, 1024, 0, s>>>(d_in, d_out, n, sums, chunk);
+  if (nch > 1) {
+    exclusive_scan_nosync(sums, sums, nch, s);
+    k_scan_add<<<nch, 1024, 0, s>>>(d_out, n, sums, chunk);
+  }
+  OP2B_CUDA(cudaFreeAsync(sums, s));
+}
+
 long long exclusive_scan(const int *d_in, int *d_out, int n, cudaStream_t s) {
   const int chunk = 8192;
   int nch = (n + chunk - 1) / chunk;

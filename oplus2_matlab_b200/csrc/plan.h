@@ -118,5 +118,7 @@ long validate_plan(const DevPlan &p);
 
 // device-wide exclusive scan of n ints (in place allowed); returns the total
 long long exclusive_scan(const int *d_in, int *d_out, int n, cudaStream_t s);
+// the same, queued only (no total, no host wait)
+void exclusive_scan_nosync(const int *d_in, int *d_out, int n, cudaStream_t s);
 
 }  // namespace op2b

@@ -169,6 +169,13 @@ class Group:
         self._check(self.lib.op2b_group_fetch_q(self.h, sid, q.ctypes.data), "op2b_group_fetch_q")
         return q
 
+    def fetch_q_async(self, sid, out):
+        """q of a solve poll() has reported stopped, copied while the others
+        iterate; `out` (pinned for an overlapped copy) is valid after sync()."""
+        self._check(self.lib.op2b_group_fetch_q_async(self.h, sid, out.ctypes.data),
+                    "op2b_group_fetch_q_async")
+        return out
+
     def remove(self, sid):
         self._check(self.lib.op2b_group_remove(self.h, sid), "op2b_group_remove")
 

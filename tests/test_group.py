@@ -285,3 +285,39 @@ def test_autotune_on_real_iterations_counts_them(op2):
     got = [(g.fetch_q(i).tobytes(), g.history(i).tobytes()) for i in ids]
     g.close()
     assert got == want
+
+
+@pytest.mark.gpu
+def test_lazy_retire_and_async_fetch_keep_results(op2):
+    """Stopped solves stay in the captured iteration until a quarter of its
+    cells have stopped (their CTAs return at once), and their q can be
+    copied out while the others iterate: every solve ends bit-identical to
+    the same solves run with a rebuild at every stop and synchronous
+    fetches."""
+    niter = 24
+    specs = [((40, 60), 0.45, -1.0, niter), ((30, 45), 0.6, 2.0, 6),
+             ((20, 30), 0.35, 5.0, 9), ((40, 60), 0.5, 0.0, 15), ((30, 45), 0.7, 3.0, niter)]
+
+    def run(lazy):
+        from oplus2_matlab_b200 import api
+        api.lib().op2b_set_tuning(b"group_lazy_retire", 1 if lazy else 0)
+        try:
+            g = G.Group()
+            ids = [g.add(mesh(*ij), m, a, n) for ij, m, a, n in specs]
+            out = {}
+            stopped = 0
+            while stopped < len(ids):
+                g.run(4)
+                done = g.poll()
+                stopped += len(done)
+                for sid in done:
+                    buf = np.zeros((g.ncell[sid], 4), np.float32)
+                    out[sid] = g.fetch_q_async(sid, buf) if lazy else g.fetch_q(sid, buf)
+            g.sync()
+            res = [(out[i].tobytes(), g.history(i).tobytes(), g.iterations(i)) for i in ids]
+            g.close()
+            return res
+        finally:
+            api.lib().op2b_set_tuning(b"group_lazy_retire", 1)
+
+    assert run(True) == run(False)
