@@ -55,7 +55,7 @@ constexpr int kMaxWidth = 8;                           // longest contribution l
 template <class T>
 struct SolveDev {  // device view of one solve; written by the host only
   const T *x;
-  T *q, *qold, *adt, *res, *vals, *partials, *hist;
+  T *q, *qold, *adt, *vals, *partials, *hist;
   const int *pedge, *pecell, *pbedge, *pbecell, *bound, *pcell, *ell;
   int ncell, nedge, nbedge, W, ntiles, pad;
   T qinf[4];
@@ -206,7 +206,11 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 8 : 4)
 }
 
 // the cell pass: fold each cell's listed values onto res in list order, then
-// update (airfoil/update.h:1-12).  MODE 0 (the iteration's first update):
+// update (airfoil/update.h:1-12).  A solve's res is +0.0 on every cell when
+// each fold starts (zero at admission, zeroed by every update, written by
+// nothing else), so the fold starts its sums from +0.0 in registers and the
+// group keeps no res array: the same values as reading it, 32 bytes per cell
+// less traffic per update.  MODE 0 (the iteration's first update):
 // then adt_calc on the new q, no rms.  MODE 1 (its second): the rms partial,
 // and the solve's last CTA ends the iteration.  MODE 2: MODE 1 plus the next
 // iteration's save_soln and adt_calc on the new q (qold = q, then adt), so
@@ -235,13 +239,12 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? (MODE == 1 ? 4 : 3)
   const bool live = solve_active(st, t.solve);  // the same for the whole CTA
   if (!live) return;
   const T *x = d->x, *qold = d->qold, *vals = d->vals;
-  T *q = d->q, *res = d->res, *adt = d->adt;
+  T *q = d->q, *adt = d->adt;
   T rms = T(0);
 #pragma unroll 1
   for (int i = threadIdx.x; i < t.count; i += kThreads) {
     const int c = t.start + i;
-    T r[4], qo[4], f[4][4], xs[4][2];
-    ldw4(res + 4 * (size_t)c, r);
+    T r[4] = {T(0), T(0), T(0), T(0)}, qo[4], f[4][4], xs[4][2];
     if (SAVE) ldw4(qold + 4 * (size_t)c, qo);
     else ld4(qold + 4 * (size_t)c, qo);
     const T ad = adt[c];
@@ -276,8 +279,6 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? (MODE == 1 ? 4 : 3)
     }
     st4(q + 4 * (size_t)c, qn);
     if (SAVE) st4(d->qold + 4 * (size_t)c, qn);  // airfoil/save_soln.h:1-3
-    const T z[4] = {T(0), T(0), T(0), T(0)};
-    st4(res + 4 * (size_t)c, z);
     if (ADT) adt[c] = adt_calc(xs[0], xs[1], xs[2], xs[3], qn, K);
   }
   if (FIRST) return;
@@ -329,7 +330,7 @@ __global__ void __launch_bounds__(1024, 1)
   __syncthreads();
   const T rms = tile_cells<T, ADT, SAVE, 1024>(
       t.start, t.start + t.count, d->tell, d->W, reinterpret_cast<const int4 *>(d->pcell), x,
-      d->qold, ain, qout, d->res, d->qold, aout, nullptr, K, fv);
+      d->qold, ain, qout, nullptr, d->qold, aout, nullptr, K, fv);
   if (FIRST) return;
   end_of_iteration(d, st, t, rms, d->tntile);
 }
@@ -387,13 +388,12 @@ __global__ void k_gl_sort(int ncell, int W, int *ell) {
   }
 }
 
-// q = qinf and res = 0 on every cell; the padding value -0.0
+// q = qinf on every cell; the padding value -0.0
 template <class T>
-__global__ void k_gl_init(int ncell, T *q, T *res, T *vals_pad, T q0, T q1, T q2, T q3) {
+__global__ void k_gl_init(int ncell, T *q, T *vals_pad, T q0, T q1, T q2, T q3) {
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
-    const T v[4] = {q0, q1, q2, q3}, z[4] = {T(0), T(0), T(0), T(0)};
+    const T v[4] = {q0, q1, q2, q3};
     st4(q + 4 * (size_t)c, v);
-    st4(res + 4 * (size_t)c, z);
   }
   if (blockIdx.x == 0 && threadIdx.x < 4) vals_pad[threadIdx.x] = T(-0.0);
 }
@@ -590,7 +590,7 @@ struct Group : GroupBase {
                            sizeof(T) * 4 * (size_t)nc,                 // q
                            sizeof(T) * 4 * (size_t)nc,                 // qold
                            sizeof(T) * (size_t)nc,                     // adt
-                           sizeof(T) * 4 * (size_t)nc,                 // res
+                           0,                                          // (res: none)
                            sizeof(T) * 4 * ((size_t)ne + nb + 1),      // vals
                            sizeof(T) * (size_t)std::max(ntiles, 1),    // partials
                            sizeof(T) * (size_t)std::max(max_iter, 1),  // hist
@@ -712,7 +712,7 @@ struct Group : GroupBase {
     memset(&d, 0, sizeof d);
     d.x = (const T *)(b + off[0]);
     d.q = (T *)(b + off[1]); d.qold = (T *)(b + off[2]); d.adt = (T *)(b + off[3]);
-    d.res = (T *)(b + off[4]); d.vals = (T *)(b + off[5]); d.partials = (T *)(b + off[6]);
+    d.vals = (T *)(b + off[5]); d.partials = (T *)(b + off[6]);
     d.hist = (T *)(b + off[7]);
     d.pedge = (const int *)(b + off[8]); d.pecell = (const int *)(b + off[9]);
     d.pbedge = (const int *)(b + off[10]); d.pbecell = (const int *)(b + off[11]);
@@ -762,7 +762,7 @@ struct Group : GroupBase {
     k_gl_sort<<<grid, 256, 0, us>>>(s.ncell, W, s.ell);
     OP2B_CUDA(cudaMemsetAsync(d.qold, 0, sizeof(T) * 4 * (size_t)s.ncell, us));
     OP2B_CUDA(cudaMemsetAsync(d.adt, 0, sizeof(T) * (size_t)s.ncell, us));
-    k_gl_init<T><<<grid, 256, 0, us>>>(s.ncell, d.q, d.res, d.vals + 4 * ((size_t)s.nedge + s.nbedge),
+    k_gl_init<T><<<grid, 256, 0, us>>>(s.ncell, d.q, d.vals + 4 * ((size_t)s.nedge + s.nbedge),
                                        d.qinf[0], d.qinf[1], d.qinf[2], d.qinf[3]);
     if (tiled && !ensure_tiled(s, us)) {
       cudaFreeAsync(s.ell, us);
@@ -1182,7 +1182,6 @@ struct Group : GroupBase {
       regions.push_back({s.dev.q, sizeof(T) * 4 * (size_t)s.ncell});
       regions.push_back({s.dev.qold, sizeof(T) * 4 * (size_t)s.ncell});
       regions.push_back({s.dev.adt, sizeof(T) * (size_t)s.ncell});
-      regions.push_back({s.dev.res, sizeof(T) * 4 * (size_t)s.ncell});
     }
     regions.push_back({d_st, sizeof(SolveState) * (size_t)solves.size()});
     size_t tot = 0;

@@ -81,7 +81,10 @@ __device__ __forceinline__ void tile_fluxes(int cnt, unsigned n_e, unsigned n_b,
 // cell's list, nodes and own streams fetched while this one works.  update
 // reads qold and adt at the cell and writes the new q to qout (and, SAVE, to
 // qsave), res = 0, del^2 to seq (when not null); ADT: adt_calc on the new q
-// into adt_out.  Returns the thread's sum of del^2 in cell order.
+// into adt_out.  res null: res is known to hold +0.0 everywhere (update
+// zeroed it and nothing wrote it since), so it is neither read nor
+// rewritten; the sums start from the same +0.0.  Returns the thread's sum
+// of del^2 in cell order.
 template <class T, bool ADT, bool SAVE, int BS>
 __device__ __forceinline__ T tile_cells(int c0, int c1, const int *__restrict__ tell, int W,
                                         const int4 *__restrict__ pcell,
@@ -96,7 +99,8 @@ __device__ __forceinline__ T tile_cells(int c0, int c1, const int *__restrict__ 
       const int4 v = __ldg(pcell + c);
       nd[0] = v.x; nd[1] = v.y; nd[2] = v.z; nd[3] = v.w;
     }
-    ldw4(res + 4 * (size_t)c, r);
+    if (res) ldw4(res + 4 * (size_t)c, r);
+    else r[0] = r[1] = r[2] = r[3] = T(0);
     if (SAVE) ldw4(qold + 4 * (size_t)c, qo);  // qsave may be qold itself
     else ld4(qold + 4 * (size_t)c, qo);
     ad = __ldg(adt + c);
@@ -140,7 +144,7 @@ __device__ __forceinline__ T tile_cells(int c0, int c1, const int *__restrict__ 
     st4(qout + 4 * (size_t)c, qn);
     if (SAVE) st4(qsave + 4 * (size_t)c, qn);  // airfoil/save_soln.h:1-3
     const T z[4] = {T(0), T(0), T(0), T(0)};
-    st4(res + 4 * (size_t)c, z);
+    if (res) st4(res + 4 * (size_t)c, z);
     if (seq) st4(seq + 4 * (size_t)c, sq);
     if (ADT) adt_out[c] = adt_calc(xs[0], xs[1], xs[2], xs[3], qn, K);
     if (cn < c1) {
