@@ -58,6 +58,9 @@ enum { OP2B_REDUCE_TREE = 0, OP2B_REDUCE_SEQ = 1 };
  *                   the res that follows it as one launch ("jac_tile_nodes"
  *                   the tile size, 0 automatic; "jac_step_threads" 512,
  *                   1024 or 256 per CTA); 0: two launches
+ *   "known_zero"    1 (default): the res_calc chain neither reads nor
+ *                   rewrites res when res is known to hold zeros
+ *                   (op2b_res_skips); 0: it always reads res
  * Every setting leaves the fields bit-identical. */
 int op2b_set_tuning(const char *key, int value);
 /* The value of a tuning knob, or `def` when it is unset. */
@@ -225,6 +228,16 @@ unsigned op2b_wait_timeouts(int reset);
  * captured since the last reset; reset != 0 clears the count.  No
  * counterpart in the reference. */
 unsigned long long op2b_tiled_launches(int reset);
+
+/* Launches of the res_calc chain (res_calc + bres_calc + update, fused) that
+ * neither read nor rewrote res because res held +0.0 in every element when
+ * res_calc was called -- as the previous update leaves it and nothing else
+ * wrote it since -- queued or captured since the last reset; reset != 0
+ * clears the count.  The fold's sums start from the same +0.0 in registers,
+ * so every value is the same as when res is read.  A graph captured while
+ * res was known zero is set, at each launch, to read res when res may hold
+ * other values then.  No counterpart in the reference. */
+unsigned long long op2b_res_skips(int reset);
 
 /* The airfoil update loop (q = qold - res/adt, res = 0, *rms += sum of
  * del^2) for callers that must not allocate device memory: code that cannot

@@ -551,7 +551,8 @@ __global__ void __launch_bounds__(256, MINB)
     for (int u = 0; u < U; u++) {
       const int c = base + u * stride;
       if (c >= n) continue;
-      ldw4(res + 4 * (size_t)c, r[u]);
+      if (res) ldw4(res + 4 * (size_t)c, r[u]);
+      else r[u][0] = r[u][1] = r[u][2] = r[u][3] = T(0);
       if (SAVE) ldw4(qold + 4 * (size_t)c, qo[u]);
       else ld4(qold + 4 * (size_t)c, qo[u]);
       ad[u] = adt[c];
@@ -590,7 +591,7 @@ __global__ void __launch_bounds__(256, MINB)
       st4(q + 4 * (size_t)c, qn);
       if (SAVE) st4(qsave + 4 * (size_t)c, qn);  // airfoil/save_soln.h:1-3
       const T z[4] = {T(0), T(0), T(0), T(0)};
-      st4(res + 4 * (size_t)c, z);
+      if (res) st4(res + 4 * (size_t)c, z);
       if (seq) st4(seq + 4 * (size_t)c, sq);
       if (ADT) (adt_out ? adt_out : adt)[c] = adt_calc(xs[u][0], xs[u][1], xs[u][2], xs[u][3], qn, K);
     }
@@ -639,7 +640,8 @@ __global__ void __launch_bounds__(256, MINB)
     }
   };
   auto streams = [&](int c, T (&r)[4], T (&qo)[4], T &ad) {
-    ldw4(res + 4 * (size_t)c, r);
+    if (res) ldw4(res + 4 * (size_t)c, r);
+    else r[0] = r[1] = r[2] = r[3] = T(0);
     if (SAVE) ldw4(qold + 4 * (size_t)c, qo);
     else ld4(qold + 4 * (size_t)c, qo);
     ad = adt[c];
@@ -689,7 +691,7 @@ __global__ void __launch_bounds__(256, MINB)
     st4(q + 4 * (size_t)c, qn);
     if (SAVE) st4(qsave + 4 * (size_t)c, qn);  // airfoil/save_soln.h:1-3
     const T z[4] = {T(0), T(0), T(0), T(0)};
-    st4(res + 4 * (size_t)c, z);
+    if (res) st4(res + 4 * (size_t)c, z);
     if (seq) st4(seq + 4 * (size_t)c, sq);
     if (ADT) (adt_out ? adt_out : adt)[c] = adt_calc(xs[0], xs[1], xs[2], xs[3], qn, K);
     if (cn < n) {
@@ -2287,6 +2289,7 @@ __global__ void __launch_bounds__(BS, 1024 / BS)
 static std::vector<void *> g_alt;
 static std::vector<int> g_alt_flips;
 static unsigned long long g_tiled_launches = 0;  // tiled chain launches queued or captured
+static unsigned long long g_res_skips = 0;  // chain launches that skipped reading res
 
 void *alt_of(op_dat d) {
   if (g_alt.size() <= (size_t)d->index) g_alt.resize(d->index + 1, nullptr);
@@ -2323,12 +2326,19 @@ void release_tile_alts() {
 
 // res_calc + bres_calc + update [+ adt_calc] [+ save_soln] as one tiled
 // launch; false when it does not apply (the caller runs the two passes)
+// a kernel just launched skipped reading d, known zero; inside a capture,
+// when the zeros come from before it, the graph records the kernel
+static void zero_entry(op_dat d, int arg, int nparams) {
+  g_res_skips++;
+  if (known_zero_from_before_capture(d)) capture_zero_entry(d, arg, nparams, d->data_d);
+}
+
 template <class T>
 static bool tiled_chain(const std::string &name, SlotPlan *sp, const op_arg *ra,
                         const op_arg *ba, const ResEdges<T> &E, const BresEdges<T> &B,
                         const op_arg *ua, const op_arg *aa, const op_arg *sa, void *adt_out,
                         void *save_out, const AirConsts<T> &K, bool seq, int rslot_id,
-                        cudaStream_t s) {
+                        cudaStream_t s, bool skip_res) {
   const size_t nval = (size_t)sp->na + sp->nb + 1;
   if (!tuning("chain_tiled", 0) || !flux_pair_shape(ra, nval) || sp->tile_unsuited) return false;
   // CTAs of 1024 threads (one per SM) or 512 (two per SM, each on its own tile)
@@ -2432,8 +2442,10 @@ static bool tiled_chain(const std::string &name, SlotPlan *sp, const op_arg *ra,
       launch_pdl(kernel, grid, threads, smem, s, P, E.n,
                  reinterpret_cast<const int2 *>(map_dev(ra[0].map)),
                  reinterpret_cast<const int2 *>(map_dev(ra[2].map)), E.xa, E.qa, E.adta, B,
-                 ncell, (const T *)ua[0].dat->data_d, (T *)qout, (T *)ua[2].dat->data_d, pcell,
-                 xc, K, seqbuf, rslot, red_ticket(), qsave, (T *)adt_to);
+                 ncell, (const T *)ua[0].dat->data_d, (T *)qout,
+                 skip_res ? (T *)nullptr : (T *)ua[2].dat->data_d, pcell, xc, K, seqbuf, rslot,
+                 red_ticket(), qsave, (T *)adt_to);
+      if (skip_res) zero_entry(ua[2].dat, 11, kernel_nparams(kernel));
     };
     if (threads == 512) {
       if (sa) go(k_chain_tiled<T, true, true, 512>);
@@ -2461,7 +2473,7 @@ template <class T>
 static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op_set bset,
                         const op_arg *ba, const op_arg *ua, const op_arg *aa, const op_arg *sa,
                         void *adt_out, void *save_out, bool flux_done,
-                        std::vector<GblRequest> *held) {
+                        std::vector<GblRequest> *held, bool res_zero) {
   // save_soln rides on the one-cell-per-thread fold + update + adt_calc forms
   const int fvar = tuning("fold_variant", 0);
   if (sa && (!ua || !aa || (fvar != 0 && fvar != 4 && fvar != 5))) return false;
@@ -2483,6 +2495,9 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
   if (sa) name += "+save_soln", bytes += compulsory_bytes(ra[6].dat->set, 2, sa);
   if (aa) name += "+adt_calc", bytes += compulsory_bytes(ra[6].dat->set, 6, aa);
   const bool seq = ua && rt().reduction == OP2B_REDUCE_SEQ;
+  // res held +0.0 everywhere when res_calc was called: the fold's sums start
+  // from +0.0 in registers, and res is neither read nor rewritten
+  const bool skip_res = res_zero && ua && ua[2].dat == ra[6].dat && tuning("known_zero", 1);
   int rslot_id = ua ? red_new_slot() : -1;
   {
     LoopScope ls(name.c_str(), bytes, 0);
@@ -2490,7 +2505,7 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
     BresEdges<T> B = bres_edges<T>(bset, ba);
     if (ua && !flux_done && ua[2].dat == ra[6].dat &&
         tiled_chain<T>(name, sp, ra, ba, E, B, ua, aa, sa, adt_out, save_out, K, seq, rslot_id,
-                       s))
+                       s, skip_res))
       goto chained;
     if (ua && !flux_done && ua[2].dat == ra[6].dat &&
         persist_chain<T>(name, sp, ra, E, B, ua, aa, sa, adt_out, save_out, K, seq, rslot_id, s))
@@ -2543,8 +2558,9 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
       auto launch = [&](auto kernel) {
         launch_pdl(kernel, grid_of((const void *)kernel), 256, 0, s, ncell,
                    (const int *)sp->d_ell, W, (const T *)vals,
-                   qold, q, res, adt, N, xs[0], xs[1], xs[2], xs[3], K, seqbuf, rslot,
-                   red_ticket(), qsave, adt_to);
+                   qold, q, skip_res ? (T *)nullptr : res, adt, N, xs[0], xs[1], xs[2], xs[3],
+                   K, seqbuf, rslot, red_ticket(), qsave, adt_to);
+        if (skip_res) zero_entry(ra[6].dat, 6, kernel_nparams(kernel));
       };
       const int fv = fvar;
       if (sa) {
@@ -2575,6 +2591,8 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
     }
   chained:;
   }
+  // every update zeroes res, whichever form ran
+  if (ua && ua[2].dat == ra[6].dat && !error_pending()) dat_set_known_zero(ra[6].dat, true);
   if (ua) {
     GblRequest rq{ua[4].data, rslot_id, OP_INC, sizeof(T) == 8 ? GBL_F64 : GBL_F32, seq};
     if (held) held->push_back(rq);  // the caller delivers it
@@ -2598,16 +2616,22 @@ unsigned wait_timeouts(bool reset) {
 bool run_res_chain(char const *name, op_set rset, const op_arg *ra, op_set bset,
                    const op_arg *ba, const op_arg *ua, const op_arg *aa, const op_arg *sa,
                    void *adt_out, void *save_out, bool flux_done,
-                   std::vector<GblRequest> *held) {
+                   std::vector<GblRequest> *held, bool res_zero) {
   return is_double(ra[0]) ? res_chain_t<double>(name, rset, ra, bset, ba, ua, aa, sa, adt_out,
-                                                save_out, flux_done, held)
+                                                save_out, flux_done, held, res_zero)
                           : res_chain_t<float>(name, rset, ra, bset, ba, ua, aa, sa, adt_out,
-                                               save_out, flux_done, held);
+                                               save_out, flux_done, held, res_zero);
 }
 
 }  // namespace op2b
 
 extern "C" unsigned op2b_wait_timeouts(int reset) { return op2b::wait_timeouts(reset != 0); }
+
+extern "C" unsigned long long op2b_res_skips(int reset) {
+  const unsigned long long n = op2b::g_res_skips;
+  if (reset) op2b::g_res_skips = 0;
+  return n;
+}
 
 extern "C" unsigned long long op2b_tiled_launches(int reset) {
   const unsigned long long n = op2b::g_tiled_launches;

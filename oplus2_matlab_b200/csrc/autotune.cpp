@@ -250,6 +250,10 @@ extern "C" int op2b_autotune(const char *cache_path, int iters, int allow_reorde
     return -1;
   }
   ahead_drop();  // nothing run ahead is swapped in after the trials
+  // the trials leave the datasets as they found them, not as their flags say
+  struct ForgetZeros {
+    ~ForgetZeros() { known_zero_forget(); }
+  } forget_zeros;
   alignas(16) static char gbl_scratch[16];  // the update's rms: never the caller's variable
   c.ua[4].data = gbl_scratch;
   const std::string key = cache_key(c);

@@ -116,6 +116,7 @@ bool load(const std::string &path, Ckpt &c) {
 // restore every dataset recorded in the file (matched by name and shape)
 void restore(Ckpt &c) {
   ahead_drop();  // the datasets change under anything run ahead
+  known_zero_forget();
   if (renumber_enabled()) renumber_apply();
   int found = 0;
   for (const DatRecord &r : c.ff_dats)

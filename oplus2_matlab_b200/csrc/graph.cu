@@ -14,18 +14,89 @@
 
 namespace op2b {
 
+// A captured kernel that skips reading a dataset because the dataset held
+// zeros when the capture began (res after airfoil's update).  A launch at a
+// time the dataset may hold other values sets the kernel's parameter to the
+// dataset's buffer, so that the kernel reads it (and writes its zeros); a
+// later launch with the zeros known again sets it back.
+struct ZeroEntry {
+  op_dat dat = nullptr;
+  cudaGraphNode_t node = nullptr;  // nullptr: the node could not be identified
+  int arg = 0, nparams = 0;
+  void *buf = nullptr;
+  bool skipping = true;  // the form the instantiated graph has now
+};
+
 struct Graph {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int nkernels = 0;
   std::vector<Runtime::CapturedLoop> loops;
   std::vector<GblRequest> reductions;  // deferred results each launch refreshes
+  std::vector<ZeroEntry> zero_entries;
+  std::vector<std::pair<int, unsigned char>> zero_effects;  // on the known-zero flags
 };
 
 static bool g_prev_deferred = false;
 static int g_live_graphs = 0;
+static std::vector<ZeroEntry> g_capture_zero_entries;
 
 int live_graphs() { return g_live_graphs; }
+
+void capture_zero_entry(op_dat d, int arg, int nparams, void *buf) {
+  ZeroEntry z;
+  z.dat = d;
+  z.arg = arg;
+  z.nparams = nparams;
+  z.buf = buf;
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  const cudaGraphNode_t *deps = nullptr;
+  const cudaGraphEdgeData *edges = nullptr;
+  size_t n = 0;
+  if (cudaStreamGetCaptureInfo_v3(rt().stream, &st, nullptr, nullptr, &deps, &edges, &n) ==
+          cudaSuccess &&
+      st == cudaStreamCaptureStatusActive && n == 1) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(deps[0], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+      z.node = deps[0];
+  }
+  cudaGetLastError();
+  g_capture_zero_entries.push_back(z);
+}
+
+// set each recorded kernel to skip or read its dataset as the dataset's
+// known-zero flag says now; false (with the error set) when a kernel that
+// must read cannot be changed
+static bool zero_entries_match(Graph *g) {
+  for (ZeroEntry &z : g->zero_entries) {
+    const bool zero = dat_known_zero(z.dat);
+    if (zero == z.skipping) continue;
+    if (!z.node || z.nparams <= z.arg) {
+      fail(-1, "op2b error: graph launch: dataset \"%s\" held zeros when the graph was "
+               "captured and may not now; capture the graph again\n",
+           z.dat->name ? z.dat->name : "");
+      return false;
+    }
+    cudaKernelNodeParams kp;
+    cudaError_t e = cudaGraphKernelNodeGetParams(z.node, &kp);
+    std::vector<void *> args;
+    void *ptr = zero ? nullptr : z.buf;
+    if (e == cudaSuccess) {
+      args.assign(kp.kernelParams, kp.kernelParams + z.nparams);
+      args[z.arg] = &ptr;
+      kp.kernelParams = args.data();
+      kp.extra = nullptr;
+      e = cudaGraphExecKernelNodeSetParams(g->exec, z.node, &kp);
+    }
+    if (e != cudaSuccess) {
+      fail(-1, "op2b error: graph launch: cannot update a kernel for dataset \"%s\": %s\n",
+           z.dat->name ? z.dat->name : "", cudaGetErrorString(e));
+      return false;
+    }
+    z.skipping = zero;
+  }
+  return true;
+}
 
 }  // namespace op2b
 
@@ -42,6 +113,8 @@ int op2b_capture_begin(int profile) {
   flush_pending();  // loops held back before the capture run outside the graph
   ahead_drop();     // a graph bakes dataset pointers: nothing may be swapped in later
   tile_capture_begin();
+  known_zero_capture_begin();
+  g_capture_zero_entries.clear();
   deliver_deferred();
   g_pending_mark = red_pending_count();
   R.capture_events.clear();
@@ -52,6 +125,7 @@ int op2b_capture_begin(int profile) {
   if (e != cudaSuccess) {
     R.gbl_deferred = g_prev_deferred;
     R.capture_profile = false;
+    known_zero_capture_end();
     fail(-1, "op2b error: cannot start graph capture: %s\n", cudaGetErrorString(e));
     return 0;
   }
@@ -63,6 +137,8 @@ void *op2b_capture_end(void) {
   tile_capture_end();  // the graph leaves every dataset in the buffer it found
   Runtime &R = rt();
   Graph *g = new Graph();
+  g->zero_effects = known_zero_capture_end();
+  g->zero_entries.swap(g_capture_zero_entries);
   cudaError_t e = cudaStreamEndCapture(R.stream, &g->graph);
   R.capture_profile = false;
   R.gbl_deferred = g_prev_deferred;
@@ -97,8 +173,11 @@ void *op2b_capture_end(void) {
 int op2b_graph_launch(void *h) {
   Graph *g = (Graph *)h;
   if (!g) return (int)cudaErrorInvalidValue;
+  if (!zero_entries_match(g)) return -1;
   red_replace_pending(g->reductions);
-  return (int)cudaGraphLaunch(g->exec, rt().stream);
+  const cudaError_t e = cudaGraphLaunch(g->exec, rt().stream);
+  if (e == cudaSuccess) known_zero_apply(g->zero_effects);
+  return (int)e;
 }
 
 int op2b_graph_nloops(void *h) { return h ? (int)((Graph *)h)->loops.size() : -1; }

@@ -181,6 +181,26 @@ int live_graphs();   // captured graphs not yet destroyed (graph.cu)
 // launch still read (airfoil.cu); swaps made while capturing are counted
 void *alt_of(op_dat d);
 void flip(op_dat d, bool capturing);
+// Datasets known to hold +0.0 in every element of their device buffer
+// (loops.cpp): set when a res chain whose update zeroes res is enqueued,
+// cleared by every loop call that writes the dataset
+bool dat_known_zero(op_dat d);
+void dat_set_known_zero(op_dat d, bool zero);
+void known_zero_forget();  // any dataset may have changed (restore, renumbering, op_exit)
+// a capture runs nothing: the flags are saved at its start and put back at
+// its end, which returns the capture's effect on them (dataset index, flag)
+// for each launch of the graph to apply
+void known_zero_capture_begin();
+std::vector<std::pair<int, unsigned char>> known_zero_capture_end();
+void known_zero_apply(const std::vector<std::pair<int, unsigned char>> &effects);
+// capturing, and no captured work has set d's flag: a kernel that relies on
+// d's zeros (seen when its loop was called) relies on the state before the
+// capture
+bool known_zero_from_before_capture(op_dat d);
+// graph.cu: the kernel just captured skips reading d (its kernel parameter
+// `arg` of `nparams`) because d was zero when the capture began; a launch of
+// the graph when d may hold other values hands the kernel d's buffer instead
+void capture_zero_entry(op_dat d, int arg, int nparams, void *buf);
 void tile_capture_begin();  // graph capture: count the tiled chain's buffer swaps
 void tile_capture_end();    // ... and undo an odd count inside the graph
 void release_tile_alts();   // op_exit: free the tiled chain's second buffers

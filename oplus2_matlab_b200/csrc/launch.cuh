@@ -30,6 +30,12 @@ __device__ __forceinline__ void pdl_trigger() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// number of parameters of a kernel
+template <class... KArgs>
+constexpr int kernel_nparams(void (*)(KArgs...)) {
+  return (int)sizeof...(KArgs);
+}
+
 // kernel<<<grid, block, smem, s>>>(args...), with PDL unless "pdl" is 0;
 // only for kernels that call pdl_wait() before touching any dataset
 template <typename... KArgs, typename... Args>

@@ -104,11 +104,13 @@ bool run_res_bres(op_set res_set, const op_arg *res_args, op_set bres_set,
 // flux_done: the flux pass already ran for exactly these arguments (run
 // ahead, run_res_flux_ahead).  held: the update's reduction is appended
 // there for the caller to deliver, instead of being delivered here.
+// res_zero: res held +0.0 in every element when res_calc was called (then,
+// with update, res is neither read nor rewritten).
 bool run_res_chain(char const *name, op_set res_set, const op_arg *res_args, op_set bres_set,
                    const op_arg *bres_args, const op_arg *update_args, const op_arg *adt_args,
                    const op_arg *save_args = nullptr, void *adt_out = nullptr,
                    void *save_out = nullptr, bool flux_done = false,
-                   std::vector<GblRequest> *held = nullptr);
+                   std::vector<GblRequest> *held = nullptr, bool res_zero = false);
 // the flux pass of a res_calc + bres_calc chain before its calls, adt read
 // from adt_now instead of adt's buffer; false when not applicable
 bool run_res_flux_ahead(op_set res_set, const op_arg *res_args, op_set bres_set,

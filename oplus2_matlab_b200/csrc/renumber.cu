@@ -838,6 +838,7 @@ void renumber_apply() {
   g_applied = true;
   release_plans_and_maps();  // device copies of maps and plans follow the new order
   for (int k = 0; k < OP_dat_index; k++) permute_dat_in_place(OP_dat_list[k]);
+  known_zero_forget();
   OP2B_CUDA(cudaStreamSynchronize(rt().stream));
   g_order_seconds =
       std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
