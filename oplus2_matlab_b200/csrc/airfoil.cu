@@ -20,6 +20,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "airfoil_math.cuh"
 #include "tile_chain.cuh"
@@ -507,8 +508,10 @@ struct CellNodes {  // adt_calc's four x arguments through pcell
 // new q is also stored to qsave -- usually qold itself, which update read at
 // the same cell first, hence the plain (coherent) load of qold.  adt_out,
 // when not null, receives adt_calc's values instead of adt (update still
-// reads adt): the loops run ahead of their calls into spare buffers
-template <class T, bool ADT, int U, int MINB, bool SAVE = false>
+// reads adt): the loops run ahead of their calls into spare buffers.  NORES:
+// res is known to hold +0.0 everywhere, so the sums start from +0.0 and res
+// is neither read nor rewritten
+template <class T, bool ADT, int U, int MINB, bool SAVE = false, bool NORES = false>
 __global__ void __launch_bounds__(256, MINB)
     k_fold_update(int n, const int *__restrict__ ell, int W, const T *__restrict__ vals,
                   const T *qold, T *__restrict__ q, T *__restrict__ res,
@@ -551,7 +554,7 @@ __global__ void __launch_bounds__(256, MINB)
     for (int u = 0; u < U; u++) {
       const int c = base + u * stride;
       if (c >= n) continue;
-      if (res) ldw4(res + 4 * (size_t)c, r[u]);
+      if (!NORES) ldw4(res + 4 * (size_t)c, r[u]);
       else r[u][0] = r[u][1] = r[u][2] = r[u][3] = T(0);
       if (SAVE) ldw4(qold + 4 * (size_t)c, qo[u]);
       else ld4(qold + 4 * (size_t)c, qo[u]);
@@ -591,7 +594,7 @@ __global__ void __launch_bounds__(256, MINB)
       st4(q + 4 * (size_t)c, qn);
       if (SAVE) st4(qsave + 4 * (size_t)c, qn);  // airfoil/save_soln.h:1-3
       const T z[4] = {T(0), T(0), T(0), T(0)};
-      if (res) st4(res + 4 * (size_t)c, z);
+      if (!NORES) st4(res + 4 * (size_t)c, z);
       if (seq) st4(seq + 4 * (size_t)c, sq);
       if (ADT) (adt_out ? adt_out : adt)[c] = adt_calc(xs[u][0], xs[u][1], xs[u][2], xs[u][3], qn, K);
     }
@@ -616,7 +619,7 @@ __global__ void __launch_bounds__(256, MINB)
 // arithmetic and its order are k_fold_update's.  Reading the next cell's
 // res/qold/adt before this cell's stores is safe: every cell belongs to one
 // thread.
-template <class T, bool ADT, int MINB, bool SAVE>
+template <class T, bool ADT, int MINB, bool SAVE, bool NORES = false>
 __global__ void __launch_bounds__(256, MINB)
     k_fold_update_pf(int n, const int *__restrict__ ell, int W, const T *__restrict__ vals,
                      const T *qold, T *__restrict__ q, T *__restrict__ res, T *__restrict__ adt,
@@ -640,7 +643,7 @@ __global__ void __launch_bounds__(256, MINB)
     }
   };
   auto streams = [&](int c, T (&r)[4], T (&qo)[4], T &ad) {
-    if (res) ldw4(res + 4 * (size_t)c, r);
+    if (!NORES) ldw4(res + 4 * (size_t)c, r);
     else r[0] = r[1] = r[2] = r[3] = T(0);
     if (SAVE) ldw4(qold + 4 * (size_t)c, qo);
     else ld4(qold + 4 * (size_t)c, qo);
@@ -691,7 +694,7 @@ __global__ void __launch_bounds__(256, MINB)
     st4(q + 4 * (size_t)c, qn);
     if (SAVE) st4(qsave + 4 * (size_t)c, qn);  // airfoil/save_soln.h:1-3
     const T z[4] = {T(0), T(0), T(0), T(0)};
-    if (res) st4(res + 4 * (size_t)c, z);
+    if (!NORES) st4(res + 4 * (size_t)c, z);
     if (seq) st4(seq + 4 * (size_t)c, sq);
     if (ADT) (adt_out ? adt_out : adt)[c] = adt_calc(xs[0], xs[1], xs[2], xs[3], qn, K);
     if (cn < n) {
@@ -2328,9 +2331,13 @@ void release_tile_alts() {
 // launch; false when it does not apply (the caller runs the two passes)
 // a kernel just launched skipped reading d, known zero; inside a capture,
 // when the zeros come from before it, the graph records the kernel
-static void zero_entry(op_dat d, int arg, int nparams) {
+// (read_kernel, read_grid: the kernel and grid that read d instead, or
+// nullptr when the kernel itself reads d when given its buffer)
+static void zero_entry(op_dat d, int arg, int nparams, const void *read_kernel = nullptr,
+                       int read_grid = 0) {
   g_res_skips++;
-  if (known_zero_from_before_capture(d)) capture_zero_entry(d, arg, nparams, d->data_d);
+  if (known_zero_from_before_capture(d))
+    capture_zero_entry(d, arg, nparams, d->data_d, read_kernel, read_grid);
 }
 
 template <class T>
@@ -2555,33 +2562,44 @@ static bool res_chain_t(char const *loop_name, op_set rset, const op_arg *ra, op
       // cell's own streams fetched a cell ahead
       T *qsave = sa ? (T *)(save_out ? save_out : sa[1].dat->data_d) : nullptr;
       T *adt_to = aa ? (T *)adt_out : nullptr;
-      auto launch = [&](auto kernel) {
+      // kr reads res; ks, the same kernel for res known zero, neither reads
+      // nor rewrites it (no branch per cell).  A graph captured with ks
+      // also records kr, for launches at which res may not be zero
+      auto launch = [&](auto kr, auto ks) {
+        const bool skip = skip_res;
+        auto kernel = skip ? ks : kr;
         launch_pdl(kernel, grid_of((const void *)kernel), 256, 0, s, ncell,
                    (const int *)sp->d_ell, W, (const T *)vals,
-                   qold, q, skip_res ? (T *)nullptr : res, adt, N, xs[0], xs[1], xs[2], xs[3],
+                   qold, q, skip ? (T *)nullptr : res, adt, N, xs[0], xs[1], xs[2], xs[3],
                    K, seqbuf, rslot, red_ticket(), qsave, adt_to);
-        if (skip_res) zero_entry(ra[6].dat, 6, kernel_nparams(kernel));
+        if (skip)
+          zero_entry(ra[6].dat, 6, kernel_nparams(kernel), (const void *)kr,
+                     grid_of((const void *)kr));
       };
       const int fv = fvar;
+#define OP2B_FOLD(...) launch(k_fold_update<__VA_ARGS__>, k_fold_update<__VA_ARGS__, true>)
+#define OP2B_FOLD_PF(...) launch(k_fold_update_pf<__VA_ARGS__>, k_fold_update_pf<__VA_ARGS__, true>)
       if (sa) {
-        if (fv == 4) launch(k_fold_update<T, true, 1, 3, true>);
-        else if (fv == 5) launch(k_fold_update_pf<T, true, sizeof(T) == 4 ? 3 : 2, true>);
-        else launch(k_fold_update<T, true, 1, sizeof(T) == 4 ? 4 : 2, true>);
+        if (fv == 4) OP2B_FOLD(T, true, 1, 3, true);
+        else if (fv == 5) OP2B_FOLD_PF(T, true, sizeof(T) == 4 ? 3 : 2, true);
+        else OP2B_FOLD(T, true, 1, sizeof(T) == 4 ? 4 : 2, true);
       } else if (aa) {
-        if (fv == 1) launch(k_fold_update<T, true, 1, 6>);
-        else if (fv == 2) launch(k_fold_update<T, true, 2, 1>);
-        else if (fv == 3) launch(k_fold_update<T, true, 2, 3>);
-        else if (fv == 4) launch(k_fold_update<T, true, 1, 3>);
-        else if (fv == 5) launch(k_fold_update_pf<T, true, sizeof(T) == 4 ? 3 : 2, false>);
-        else launch(k_fold_update<T, true, 1, sizeof(T) == 4 ? 4 : 2>);
+        if (fv == 1) OP2B_FOLD(T, true, 1, 6, false);
+        else if (fv == 2) OP2B_FOLD(T, true, 2, 1, false);
+        else if (fv == 3) OP2B_FOLD(T, true, 2, 3, false);
+        else if (fv == 4) OP2B_FOLD(T, true, 1, 3, false);
+        else if (fv == 5) OP2B_FOLD_PF(T, true, sizeof(T) == 4 ? 3 : 2, false);
+        else OP2B_FOLD(T, true, 1, sizeof(T) == 4 ? 4 : 2, false);
       } else {
-        if (fv == 1) launch(k_fold_update<T, false, 1, 6>);
-        else if (fv == 2) launch(k_fold_update<T, false, 2, 1>);
-        else if (fv == 3) launch(k_fold_update<T, false, 2, 3>);
-        else if (fv == 4) launch(k_fold_update<T, false, 1, sizeof(T) == 4 ? 4 : 3>);
-        else if (fv == 5) launch(k_fold_update_pf<T, false, sizeof(T) == 4 ? 4 : 2, false>);
-        else launch(k_fold_update<T, false, 1, sizeof(T) == 4 ? 5 : 2>);
+        if (fv == 1) OP2B_FOLD(T, false, 1, 6, false);
+        else if (fv == 2) OP2B_FOLD(T, false, 2, 1, false);
+        else if (fv == 3) OP2B_FOLD(T, false, 2, 3, false);
+        else if (fv == 4) OP2B_FOLD(T, false, 1, sizeof(T) == 4 ? 4 : 3, false);
+        else if (fv == 5) OP2B_FOLD_PF(T, false, sizeof(T) == 4 ? 4 : 2, false);
+        else OP2B_FOLD(T, false, 1, sizeof(T) == 4 ? 5 : 2, false);
       }
+#undef OP2B_FOLD
+#undef OP2B_FOLD_PF
       if (seq) {
         T init = *(const T *)ua[4].data;
         k_seq_sum<T><<<1, 32, 0, s>>>(seqbuf, 4LL * ncell, init, result,

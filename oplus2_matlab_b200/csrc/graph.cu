@@ -17,13 +17,16 @@ namespace op2b {
 // A captured kernel that skips reading a dataset because the dataset held
 // zeros when the capture began (res after airfoil's update).  A launch at a
 // time the dataset may hold other values sets the kernel's parameter to the
-// dataset's buffer, so that the kernel reads it (and writes its zeros); a
-// later launch with the zeros known again sets it back.
+// dataset's buffer and, where the skipping kernel is a variant that ignores
+// it, the variant that reads it (and writes its zeros) in its place; a later
+// launch with the zeros known again puts the captured kernel back.
 struct ZeroEntry {
   op_dat dat = nullptr;
   cudaGraphNode_t node = nullptr;  // nullptr: the node could not be identified
   int arg = 0, nparams = 0;
   void *buf = nullptr;
+  const void *read_kernel = nullptr;  // nullptr: the captured kernel reads the buffer
+  int read_grid = 0;
   bool skipping = true;  // the form the instantiated graph has now
 };
 
@@ -43,12 +46,15 @@ static std::vector<ZeroEntry> g_capture_zero_entries;
 
 int live_graphs() { return g_live_graphs; }
 
-void capture_zero_entry(op_dat d, int arg, int nparams, void *buf) {
+void capture_zero_entry(op_dat d, int arg, int nparams, void *buf, const void *read_kernel,
+                        int read_grid) {
   ZeroEntry z;
   z.dat = d;
   z.arg = arg;
   z.nparams = nparams;
   z.buf = buf;
+  z.read_kernel = read_kernel;
+  z.read_grid = read_grid;
   cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
   const cudaGraphNode_t *deps = nullptr;
   const cudaGraphEdgeData *edges = nullptr;
@@ -77,17 +83,22 @@ static bool zero_entries_match(Graph *g) {
            z.dat->name ? z.dat->name : "");
       return false;
     }
+    // the graph's own node holds the captured (skipping) form
     cudaKernelNodeParams kp;
     cudaError_t e = cudaGraphKernelNodeGetParams(z.node, &kp);
     std::vector<void *> args;
-    void *ptr = zero ? nullptr : z.buf;
-    if (e == cudaSuccess) {
+    void *ptr = z.buf;
+    if (e == cudaSuccess && !zero) {
       args.assign(kp.kernelParams, kp.kernelParams + z.nparams);
       args[z.arg] = &ptr;
       kp.kernelParams = args.data();
       kp.extra = nullptr;
-      e = cudaGraphExecKernelNodeSetParams(g->exec, z.node, &kp);
+      if (z.read_kernel) {
+        kp.func = const_cast<void *>(z.read_kernel);
+        kp.gridDim = dim3((unsigned)z.read_grid);
+      }
     }
+    if (e == cudaSuccess) e = cudaGraphExecKernelNodeSetParams(g->exec, z.node, &kp);
     if (e != cudaSuccess) {
       fail(-1, "op2b error: graph launch: cannot update a kernel for dataset \"%s\": %s\n",
            z.dat->name ? z.dat->name : "", cudaGetErrorString(e));

@@ -200,7 +200,10 @@ bool known_zero_from_before_capture(op_dat d);
 // graph.cu: the kernel just captured skips reading d (its kernel parameter
 // `arg` of `nparams`) because d was zero when the capture began; a launch of
 // the graph when d may hold other values hands the kernel d's buffer instead
-void capture_zero_entry(op_dat d, int arg, int nparams, void *buf);
+// and, when read_kernel is not null, runs read_kernel (the same parameters)
+// on read_grid CTAs in its place
+void capture_zero_entry(op_dat d, int arg, int nparams, void *buf, const void *read_kernel,
+                        int read_grid);
 void tile_capture_begin();  // graph capture: count the tiled chain's buffer swaps
 void tile_capture_end();    // ... and undo an odd count inside the graph
 void release_tile_alts();   // op_exit: free the tiled chain's second buffers
