@@ -86,6 +86,9 @@ def parse():
     ap.add_argument("--admit-ms", type=float, default=10.0,
                     help="batched: device milliseconds of iterations enqueued after each "
                          "admitted chunk (sized from the admitted cells)")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="batched: skip the plain back-to-back leg (no speed-up, no parity; "
+                         "for profiling the group alone)")
     ap.add_argument("--group-tiled", action="store_true",
                     help="batched and served forms: the tiled chain (op2b_group_set_tiled)")
     ap.add_argument("--no-forms", action="store_true",
@@ -896,15 +899,19 @@ def measure_batched(args, dist, instances, n):
     gbytes = g.device_bytes()
     g.close()
 
-    dist.barrier()
-    t0 = time.perf_counter()
-    plain = [G.plain_solve(meshes[inst[i][:2]], inst[i][2], inst[i][3], n, dt,
-                           q_out=qbuf_plain[i]) for i in mine]
-    t_plain = dist.max(time.perf_counter() - t0)
+    plain, t_plain = None, None
+    if not args.no_plain:
+        dist.barrier()
+        t0 = time.perf_counter()
+        plain = [G.plain_solve(meshes[inst[i][:2]], inst[i][2], inst[i][3], n, dt,
+                               q_out=qbuf_plain[i]) for i in mine]
+        t_plain = dist.max(time.perf_counter() - t0)
     clk = clocks.stop()
 
-    exact = sum(int(a.tobytes() == p[0].astype(dt).tobytes()) for a, p in zip(qg, plain))
-    rel = max(float(np.max(np.abs(h - p[1]) / np.abs(p[1]))) for h, p in zip(hist, plain))
+    exact = rel = None
+    if plain:
+        exact = sum(int(a.tobytes() == p[0].astype(dt).tobytes()) for a, p in zip(qg, plain))
+        rel = max(float(np.max(np.abs(h - p[1]) / np.abs(p[1]))) for h, p in zip(hist, plain))
     s = 8 if args.fp64 else 4
     my_bytes = sum(iteration_bytes(meshes[inst[i][:2]], s) for i in mine) * n
     del meshes
@@ -934,12 +941,13 @@ def measure_batched(args, dist, instances, n):
                   "device_bytes_rank0": gbytes,
                   "autotuned": "edge tile and L2 block size, on real iterations",
                   "iteration_gbs_rank0": my_bytes / (t_group - t_fetch) / 1e9},
-        "plain_back_to_back": {"seconds": t_plain, "solves_per_s": total / t_plain,
-                               "path": "op2b_airfoil_app_flow per instance (op_par_loop, "
-                                       "rms to the host after every update)"},
-        "speedup_vs_plain": t_plain / t_group,
-        "parity_rank0": {"q_bit_identical": "%d/%d" % (exact, len(mine)),
-                         "max_rms_rel_diff": rel},
+        "plain_back_to_back": None if plain is None else {
+            "seconds": t_plain, "solves_per_s": total / t_plain,
+            "path": "op2b_airfoil_app_flow per instance (op_par_loop, rms to the host after "
+                    "every update)"},
+        "speedup_vs_plain": None if plain is None else t_plain / t_group,
+        "parity_rank0": None if plain is None else {
+            "q_bit_identical": "%d/%d" % (exact, len(mine)), "max_rms_rel_diff": rel},
         # graph launches (iterations: 4 kernels each, 2 with the tiled chain;
         # more when the tuned blocks split the solves), priming save_soln +
         # adt_calc launches, list building at admission (6 per solve)
