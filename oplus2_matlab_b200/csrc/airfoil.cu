@@ -545,11 +545,13 @@ __global__ void __launch_bounds__(256, MINB)
     }
   };
   const int base0 = blockIdx.x * blockDim.x + threadIdx.x;
-  indices(base0, k, nd);  // before the previous kernel has finished
-  pdl_wait();
-  pdl_trigger();
-  for (int base = base0; base < n; base += stride * U) {
-    T r[U][4], qo[U][4], ad[U], xs[U][4][2], f[U][4][4];
+  // the cells' own streams and node coordinates (res, qold, adt, x): the
+  // flux pass this kernel follows does not write them, and the launches
+  // that did had completed before the flux pass could let this kernel
+  // start, so the first pass fetches them before the wait too; only the
+  // flux values wait
+  T r[U][4], qo[U][4], ad[U], xs[U][4][2];
+  auto streams = [&](int base) {
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const int c = base + u * stride;
@@ -559,15 +561,28 @@ __global__ void __launch_bounds__(256, MINB)
       if (SAVE) ldw4(qold + 4 * (size_t)c, qo[u]);
       else ld4(qold + 4 * (size_t)c, qo[u]);
       ad[u] = adt[c];
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-        if (k[u][j] >= 0) ld4(vals + 4 * (size_t)(k[u][j] >> 1), f[u][j]);
       if (ADT) {
         ld2(x0 + 2 * (size_t)nd[u][0], xs[u][0]);
         ld2(x1 + 2 * (size_t)nd[u][1], xs[u][1]);
         ld2(x2 + 2 * (size_t)nd[u][2], xs[u][2]);
         ld2(x3 + 2 * (size_t)nd[u][3], xs[u][3]);
       }
+    }
+  };
+  indices(base0, k, nd);  // before the previous kernel has finished
+  streams(base0);
+  pdl_wait();
+  pdl_trigger();
+  for (int base = base0; base < n; base += stride * U) {
+    T f[U][4][4];
+    if (base != base0) streams(base);
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int c = base + u * stride;
+      if (c >= n) continue;
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (k[u][j] >= 0) ld4(vals + 4 * (size_t)(k[u][j] >> 1), f[u][j]);
     }
     indices(base + stride * U, kn, ndn);
 #pragma unroll
