@@ -239,6 +239,14 @@ unsigned long long op2b_tiled_launches(int reset);
  * other values then.  No counterpart in the reference. */
 unsigned long long op2b_res_skips(int reset);
 
+/* Bytes copied from host to device by dataset declarations and map uploads
+ * since the last reset; reset != 0 clears the count.  A dataset declared
+ * from a large (1 MiB or more) array in pageable host memory that holds only
+ * zero bytes is not copied: its device buffer is cleared instead (same
+ * bytes; knob "decl_zero_scan", 1 by default) and the dataset is known to
+ * hold zeros.  No counterpart in the reference. */
+unsigned long long op2b_h2d_bytes(int reset);
+
 /* The airfoil update loop (q = qold - res/adt, res = 0, *rms += sum of
  * del^2) for callers that must not allocate device memory: code that cannot
  * afford cudaMalloc's device synchronisation, hosts that reserve all device

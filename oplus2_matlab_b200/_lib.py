@@ -154,6 +154,7 @@ PROTOTYPES = [
     ("op2b_wait_timeouts", C.c_uint, [C.c_int]),
     ("op2b_tiled_launches", C.c_ulonglong, [C.c_int]),
     ("op2b_res_skips", C.c_ulonglong, [C.c_int]),
+    ("op2b_h2d_bytes", C.c_ulonglong, [C.c_int]),
     ("op2b_layout_ab", C.c_int, [C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, C.c_float,
                                  C.c_float, C.c_int, C.POINTER(C.c_double),
                                  C.POINTER(C.c_double)]),

@@ -42,6 +42,7 @@ extern "C" int op2b_jac1_app(int nnode, int nedge, const int *pp, const float *A
   for (int n = 0; n < nnode; n++) u[n] = 0.0f;
 
   op_init(0, nullptr, 0);
+  const unsigned long long h2d0 = op2b_h2d_bytes(0);
   op_set nodes = op_decl_set(nnode, "nodes");
   op_set edges = op_decl_set(nedge, "edges");
   op_map ppedge = op_decl_map(edges, nodes, 2, (int *)pp, "ppedge");
@@ -75,6 +76,7 @@ extern "C" int op2b_jac1_app(int nnode, int nedge, const int *pp, const float *A
   const double t2 = now();
   op_fetch_data(p_u);
   const double t3 = now();
+  const long long h2d = (long long)(op2b_h2d_bytes(0) - h2d0);
   const int err = op2b_last_error()[0] != 0;
   op_exit();
   free(du);
@@ -83,7 +85,7 @@ extern "C" int op2b_jac1_app(int nnode, int nedge, const int *pp, const float *A
     tm->t_iterate = t2 - t1;
     tm->t_fetch = t3 - t2;
     tm->t_total = t3 - t0;
-    tm->h2d_bytes = 8LL * nedge + 4LL * nedge + 4LL * 3 * nnode;
+    tm->h2d_bytes = h2d;  // what the library copied
     tm->d2h_bytes = 4LL * nnode + 8LL * niter;
   }
   return err;

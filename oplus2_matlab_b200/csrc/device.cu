@@ -12,7 +12,10 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
+#include <thread>
 #include <unordered_set>
+#include <vector>
 
 #include "internal.h"
 
@@ -23,6 +26,9 @@ namespace op2b {
 void release_fused_plans();  // airfoil.cu
 void release_jac_pairs();    // jac.cu
 void release_jac_steps();    // jac.cu
+
+// bytes copied host -> device by dataset declarations and map uploads
+static unsigned long long g_h2d_bytes = 0;
 
 void ensure_cuda() {
   Runtime &R = rt();
@@ -176,6 +182,7 @@ void *map_upload_begin(const int *imap, size_t bytes) {
     cudaFreeAsync(d, R.stream);
     return nullptr;
   }
+  g_h2d_bytes += bytes;
   return d;
 }
 
@@ -208,6 +215,7 @@ const int *map_dev(op_map m) {
     if (md.d) {
       OP2B_CUDA(cudaMemcpyAsync(md.d, (const int *)m->map, bytes, cudaMemcpyHostToDevice,
                                 R.stream));
+      g_h2d_bytes += bytes;
       OP2B_CUDA(cudaStreamSynchronize(R.stream));
       // renumbered sets: rows in the from-set's new order, values in the
       // to-set's new numbering, rewritten on the device
@@ -370,8 +378,47 @@ void op_init(int argc, char **argv, int diags) {
   printf("\n Using CUDA device: %s\n", rt().device_name.c_str());
 }
 
+// whether the host bytes [p, p + n) are all zero: the first 4 KB alone, then
+// one pass split over up to 8 host threads (a zero-filled calloc'd array
+// that was never touched maps the zero page as it is read, page by page,
+// which the threads do in parallel)
+static bool host_all_zero(const char *p, size_t n) {
+  auto part = [p](size_t a, size_t b) {
+    unsigned long long acc = 0;
+    size_t i = a;
+    for (; i < b && ((uintptr_t)(p + i) & 7); i++) acc |= (unsigned char)p[i];
+    const unsigned long long *w = reinterpret_cast<const unsigned long long *>(p + i);
+    const size_t nw = (b - i) / 8;
+    for (size_t k = 0; k < nw; k++) acc |= w[k];
+    for (i += 8 * nw; i < b; i++) acc |= (unsigned char)p[i];
+    return acc == 0;
+  };
+  const size_t head = std::min(n, (size_t)4096);
+  if (!part(0, head)) return false;
+  const unsigned hw = std::thread::hardware_concurrency();
+  const size_t nt = hw < 2 ? 1 : std::min<size_t>(8, hw);
+  const size_t chunk = (n - head + nt - 1) / nt;
+  std::vector<char> zero(nt, 1);
+  std::vector<std::thread> th;
+  for (size_t t = 1; t < nt; t++)
+    th.emplace_back([&, t] {
+      zero[t] = part(std::min(n, head + t * chunk), std::min(n, head + (t + 1) * chunk));
+    });
+  zero[0] = part(head, std::min(n, head + chunk));
+  bool all = zero[0] != 0;
+  for (size_t t = 1; t < nt; t++) {
+    th[t - 1].join();
+    all = all && zero[t] != 0;
+  }
+  return all;
+}
+
 // common/op_lib.cu:145-153: registry entry + device copy (synchronous, so
-// the caller may reuse its array on return)
+// the caller may reuse its array on return).  A large array in pageable
+// host memory that holds only zero bytes (an app's zero-initialised qold,
+// adt, res) is not copied: the device buffer is cleared instead, which
+// gives the same bytes without the pageable copy's page-by-page staging,
+// and the dataset is known to hold zeros.
 op_dat op_decl_dat_char(op_set set, int dim, char const *type, int size, char *data,
                         char const *name) {
   op_dat dat = op_decl_dat_core(set, dim, type, size, data, name);
@@ -383,10 +430,23 @@ op_dat op_decl_dat_char(op_set set, int dim, char const *type, int size, char *d
   R.dats[dat->index].bytes = bytes;
   dat->data_d = (char *)dev_alloc(bytes);
   if (!dat->data_d) return dat;
-  if (data) OP2B_CUDA(cudaMemcpyAsync(dat->data_d, data, bytes, cudaMemcpyHostToDevice, R.stream));
-  else OP2B_CUDA(cudaMemsetAsync(dat->data_d, 0, bytes, R.stream));
+  bool zero = data == nullptr;
+  if (data && bytes >= ((size_t)1 << 20) && tuning("decl_zero_scan", 1)) {
+    cudaPointerAttributes pa;
+    const bool pageable =
+        cudaPointerGetAttributes(&pa, data) == cudaSuccess && pa.type == cudaMemoryTypeUnregistered;
+    cudaGetLastError();
+    zero = pageable && host_all_zero(data, bytes);
+  }
+  if (zero) {
+    OP2B_CUDA(cudaMemsetAsync(dat->data_d, 0, bytes, R.stream));
+  } else {
+    OP2B_CUDA(cudaMemcpyAsync(dat->data_d, data, bytes, cudaMemcpyHostToDevice, R.stream));
+    g_h2d_bytes += bytes;
+  }
   OP2B_CUDA(cudaStreamSynchronize(R.stream));
   permute_dat_in_place(dat);  // when its set has been renumbered
+  if (zero && !error_pending()) dat_set_known_zero(dat, true);
   return dat;
 }
 
@@ -533,6 +593,12 @@ int op2b_l2_flush(void) {
   k_l2_sweep<<<rt().num_sms * 8, 256, 0, rt().stream>>>((const uint4 *)buf, bytes / 16,
                                                         (unsigned *)((char *)buf + bytes));
   return (int)cudaGetLastError();
+}
+
+unsigned long long op2b_h2d_bytes(int reset) {
+  const unsigned long long n = op2b::g_h2d_bytes;
+  if (reset) op2b::g_h2d_bytes = 0;
+  return n;
 }
 
 char const *op2b_version(void) {
